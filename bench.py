@@ -1,0 +1,380 @@
+#!/usr/bin/env python
+"""Benchmark of the Galerkin triple product C = R*A*P on one or more B200s.
+
+Workload: the 128^3 7-point Poisson operator with 2x2x2 aggregation and one
+damped-Jacobi smoothing step (A: 2,097,152 rows, 14.6M nonzeros; P:
+2,097,152 x 262,144; R = P^T), FP64, seeded synthetic data.  A step is one
+complete R*A*P product on the device (default: direct variant, upper-bound
+flavour), inputs resident in HBM, output allocated and freed each step.
+
+Metric: compulsory-byte throughput in GB/s -- R, A and P read once plus C
+written once, counted in the device format (int32 indices, FP64 values).  The
+inputs (~390 MB) exceed the 126 MB L2, so no flush is needed between steps.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]
+
+Multi-GPU runs (torchrun, one rank per GPU) are replicas: every rank runs
+its own product (weak scaling, no data-path collective); the time is the max
+over ranks.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+from sp3mm4amg_b200 import problems as pb  # noqa: E402
+
+PEAKS_PATH = os.path.join(ROOT, "MEASURED_PEAKS.json")
+TRAFFIC_PATH = os.path.join(ROOT, "profiles", "roofline_traffic.json")
+FALLBACK_HBM_GBS = 6650.0
+
+VARIANTS = {"pair": 0, "direct": 1, "pair_right": 2}
+FLAVOURS = {"ub": 0, "symbnum": 1}
+
+# nvidia-smi clocks_event_reasons bits.
+REASONS = {0x1: "gpu_idle", 0x2: "applications_clocks_setting", 0x4: "sw_power_cap",
+           0x8: "hw_slowdown", 0x10: "sync_boost", 0x20: "sw_thermal_slowdown",
+           0x40: "hw_thermal_slowdown", 0x80: "hw_power_brake_slowdown",
+           0x100: "display_clock_setting"}
+
+
+def parse_args():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=200)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--variant", default="direct", choices=list(VARIANTS))
+    ap.add_argument("--flavour", default="ub", choices=list(FLAVOURS))
+    ap.add_argument("--side", type=int, default=128, help="grid side of the 3D problem")
+    ap.add_argument("--e2e-steps", type=int, default=3)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--cpu-seconds", type=float, default=12.0,
+                    help="target CPU time of the cpu_baseline sample")
+    return ap.parse_args()
+
+
+def peaks():
+    try:
+        with open(PEAKS_PATH) as f:
+            p = json.load(f)
+        return float(p["hbm_gbs"]), "measured"
+    except Exception:
+        return FALLBACK_HBM_GBS, "fallback"
+
+
+def workload_name(side):
+    return f"poisson3d_{side}^3_7pt_agg2x2x2_jacobi"
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled during the timed region."""
+
+    def __init__(self, index: int):
+        self.cmd = ["nvidia-smi", f"--id={index}",
+                    "--query-gpu=clocks.sm,clocks.max.sm,clocks_event_reasons.active",
+                    "--format=csv,noheader,nounits", "-lms", "50"]
+        self.proc = None
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(self.cmd, stdout=subprocess.PIPE,
+                                         stderr=subprocess.DEVNULL, text=True)
+            time.sleep(0.3)
+        except Exception:
+            self.proc = None
+
+    def stop(self):
+        if not self.proc:
+            return None
+        time.sleep(0.1)
+        self.proc.terminate()
+        try:
+            out, _ = self.proc.communicate(timeout=5)
+        except Exception:
+            self.proc.kill()
+            out = ""
+        sm, mx, reasons = [], [], set()
+        for line in out.splitlines():
+            parts = [x.strip() for x in line.split(",")]
+            if len(parts) < 3:
+                continue
+            try:
+                sm.append(float(parts[0]))
+                mx.append(float(parts[1]))
+                bits = int(parts[2], 16)
+            except ValueError:
+                continue
+            for b, name in REASONS.items():
+                if bits & b and name != "gpu_idle":
+                    reasons.add(name)
+        if not sm:
+            return None
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": max(mx),
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def smi_index(local_rank: int) -> int:
+    vis = os.environ.get("CUDA_VISIBLE_DEVICES", "")
+    if vis:
+        ids = [x.strip() for x in vis.split(",") if x.strip()]
+        if local_rank < len(ids) and ids[local_rank].isdigit():
+            return int(ids[local_rank])
+    return local_rank
+
+
+# ---------------------------------------------------------------------------
+# CPU baseline: the reference's own OpenMP code (oracle/_ref) on a bounded
+# row sample of the same product, extrapolated to the full product.
+
+def cpu_reference_runner(prob, threads):
+    """Returns (kind, fn(rows) -> seconds, description)."""
+    os.environ["OMP_NUM_THREADS"] = str(threads)
+    import oracle
+    try:
+        ref = oracle.Reference(threads=threads)
+        ref.adapt_grid(0)
+
+        def run(rows):
+            Rs = prob.R.rows(0, rows)
+            t0 = time.perf_counter()
+            ref.sp3mm_pair("spmmRowByRow_", Rs, prob.A, prob.P, 0)
+            return time.perf_counter() - t0
+        return ("reference", run,
+                "reference sp3mmRowByRowPair_0 with spmmRowByRow_0 (upper-bound 1D, its "
+                "fastest variant here)")
+    except (FileNotFoundError, OSError):
+        orc = oracle.Oracle()
+        orc.set_threads(threads)
+
+        def run(rows):
+            Rs = prob.R.rows(0, rows)
+            t0 = time.perf_counter()
+            orc.sp3mm_pair(Rs, prob.A, prob.P)
+            return time.perf_counter() - t0
+        return "port", run, "oracle restatement (pair), reference library not built"
+
+
+def calibrated_sample(run, M, seconds):
+    rows = 64
+    t = run(rows)
+    while t < 0.5 and rows < M:
+        rows = min(M, rows * 4)
+        t = run(rows)
+    want = int(rows * seconds / max(t, 1e-6))
+    return max(1, min(M, want))
+
+
+def run_reference_arm(args, prob, nnz_c):
+    threads = os.cpu_count() or 1
+    total_bytes = prob.compulsory_bytes(nnz_c=nnz_c, idx_bytes=4)
+    kind, run, desc = cpu_reference_runner(prob, threads)
+    M = prob.R.M
+    rows = calibrated_sample(run, M, 4.0)
+    vals = []
+    for i in range(args.warmup + args.steps):
+        t = run(rows)
+        if i >= args.warmup:
+            vals.append(total_bytes / (t * M / rows) / 1e9)
+    value = statistics.median(vals)
+    sample = f"rows 0..{rows} of {M} of R per step ({desc}), time scaled by {M}/{rows}"
+    line = {
+        "impl": "reference", "metric": "rap_compulsory_GBps", "value": value, "unit": "GB/s",
+        "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": total_bytes / (value * 1e9) * 1e3, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": workload_name(args.side), "variant": "pair", "flavour": "ub"},
+        "cpu_baseline": {"value": value, "unit": "GB/s", "cores": threads, "kind": kind,
+                         "sample": sample},
+        "e2e": {"value": value, "unit": "GB/s", "h2d_bytes_per_step": 0,
+                "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+# ---------------------------------------------------------------------------
+
+def main():
+    args = parse_args()
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local_rank = int(os.environ.get("LOCAL_RANK", "0"))
+
+    if args.impl == "reference":
+        if rank != 0:
+            return
+        prob = pb.stencil_problem(3, args.side)
+        nnz_c = 8_382_712 if args.side == 128 else None
+        if nnz_c is None:
+            import oracle
+            nnz_c = oracle.Oracle().sp3mm_pair(prob.R, prob.A, prob.P).nnz
+        run_reference_arm(args, prob, nnz_c)
+        return
+
+    import torch
+    import sp3mm4amg_b200 as S
+    torch.cuda.set_device(local_rank)
+    dist = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
+                                device_id=torch.device("cuda", local_rank))
+
+    def barrier():
+        if dist is not None:
+            dist.barrier()
+
+    prob = pb.stencil_problem(3, args.side)
+    variant, flavour = VARIANTS[args.variant], FLAVOURS[args.flavour]
+    ctx = S.Context(local_rank)
+    stream = torch.cuda.ExternalStream(ctx.stream, device=torch.device("cuda", local_rank))
+    dR, dA, dP = ctx.upload(prob.R), ctx.upload(prob.A), ctx.upload(prob.P)
+
+    # Warm-up (also fixes the output size).
+    nnz_c = 0
+    for _ in range(max(args.warmup, 3)):
+        C = ctx.rap(dR, dA, dP, variant, flavour)
+        nnz_c = C.nnz
+        C.free()
+    ctx.sync()
+    total_bytes = prob.compulsory_bytes(nnz_c=nnz_c, idx_bytes=4)
+
+    clocks = ClockSampler(smi_index(local_rank))
+    clocks.start()
+    barrier()
+    torch.cuda.synchronize()
+    launches0 = ctx.launches()
+    ev0 = torch.cuda.Event(enable_timing=True)
+    ev1 = torch.cuda.Event(enable_timing=True)
+    ev0.record(stream)
+    for _ in range(args.steps):
+        C = ctx.rap(dR, dA, dP, variant, flavour)
+        C.free()
+    ev1.record(stream)
+    ev1.synchronize()
+    torch.cuda.synchronize()
+    barrier()
+    launches = ctx.launches() - launches0
+    clk = clocks.stop()
+    elapsed_ms = ev0.elapsed_time(ev1)
+    if dist is not None:
+        t = torch.tensor([elapsed_ms], device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        elapsed_ms = float(t.item())
+    ms_per_step = elapsed_ms / args.steps
+    value = world * args.steps * total_bytes / (elapsed_ms * 1e-3) / 1e9
+
+    # Per-kernel device times (separate pass with per-launch events).
+    ctx.set_profiling(True)
+    nprof = 10
+    for _ in range(nprof):
+        C = ctx.rap(dR, dA, dP, variant, flavour)
+        C.free()
+    prof = ctx.profile()
+    ctx.set_profiling(False)
+    dom_label, (dom_n, dom_total, _) = max(prof.items(), key=lambda kv: kv[1][1])
+    all_ms = sum(v[1] for v in prof.values())
+    peak, peak_kind = peaks()
+    # The dominant row kernel reads R, A and P and writes C: its algorithmic
+    # bytes per launch are the product's compulsory bytes.
+    dom_avg_ms = dom_total / nprof
+    achieved = total_bytes / (dom_avg_ms * 1e-3) / 1e9
+    traffic = None
+    try:
+        with open(TRAFFIC_PATH) as f:
+            tj = json.load(f)
+        if tj.get("kernel_label") == dom_label and tj.get("variant") == args.variant:
+            traffic = tj.get("dram_bytes_per_launch")
+    except Exception:
+        pass
+
+    # End to end through the drop-in C entry point: pinned host spmat in,
+    # malloc'd host spmat out, host<->device copies inside the timed region.
+    import ctypes
+    from sp3mm4amg_b200 import capi
+    from sp3mm4amg_b200.spmat import CONFIG, HostSpMat
+    lib = capi.load()
+    hR, hA, hP = (HostSpMat(m, 0, pinned=True) for m in (prob.R, prob.A, prob.P))
+    fname = {(1, 0): "sp3mmRowByRowMerged_0", (1, 1): "sp3mmRowByRowMerged_SymbNum_0",
+             (0, 0): "sp3mmRowByRowPair_0", (0, 1): "sp3mmRowByRowPair_SymbNum_0",
+             (2, 0): "sp3mmRowByRowPairRight_0", (2, 1): "sp3mmRowByRowPairRight_0"}[
+        (variant, flavour)]
+    fn = getattr(lib, fname)
+    cfg = CONFIG(gridRows=1, gridCols=1, symbMMRowImplID=0, threadNum=1, chunkDistrbFunc=None)
+    spmm_arg = None
+    if variant == 2 and flavour == 1:
+        spmm_arg = ctypes.cast(lib.spmmRowByRow_SymbNum_0, ctypes.c_void_p).value
+    libc = ctypes.CDLL(None)
+    libc.free.argtypes = [ctypes.c_void_p]
+    from sp3mm4amg_b200.spmat import SPMAT_P
+    e2e_times = []
+    for i in range(args.e2e_steps + 1):
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        p = fn(hR.ptr, hA.ptr, hP.ptr, ctypes.byref(cfg), spmm_arg)
+        t1 = time.perf_counter()
+        if not p:
+            raise RuntimeError("e2e call returned NULL")
+        m = ctypes.cast(p, SPMAT_P).contents
+        nz = int(m.NZ)
+        for arr in (m.AS, m.JA, m.IRP):
+            libc.free(ctypes.cast(arr, ctypes.c_void_p))
+        libc.free(p)
+        if i > 0:
+            e2e_times.append(t1 - t0)
+    e2e_t = statistics.median(e2e_times)
+    h2d = sum((mm.M + 1) * 8 + mm.nnz * 16 for mm in (prob.R, prob.A, prob.P))
+    d2h = (prob.R.M + 1) * 8 + nz * 16
+
+    line = {
+        "metric": "rap_compulsory_GBps", "value": value, "unit": "GB/s", "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_per_step,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+        "data": "synthetic",
+        "config": {"workload": workload_name(args.side), "variant": args.variant,
+                   "flavour": args.flavour, "rows_R": prob.R.M, "nnz_A": prob.A.nnz,
+                   "nnz_P": prob.P.nnz, "nnz_C": nnz_c,
+                   "bytes_per_product": total_bytes, "byte_basis": "int32 idx + f64 val",
+                   "products_per_s": world * args.steps / (elapsed_ms * 1e-3),
+                   "l2": "inputs exceed L2 (126 MB); no flush",
+                   "parallelism": f"replicas x{world}"},
+        "roofline": {"bound": "hbm", "kernel": dom_label, "achieved": achieved, "peak": peak,
+                     "peak_kind": peak_kind, "unit": "GB/s", "frac": achieved / peak,
+                     "traffic": traffic, "kernel_share": dom_total / all_ms if all_ms else None,
+                     "kernels_ms_per_product": {k: v[1] / nprof for k, v in prof.items()}},
+        "e2e": {"value": total_bytes / e2e_t / 1e9, "unit": "GB/s",
+                "seconds_per_product": e2e_t, "entry_point": fname,
+                "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
+        "gpu_launches": launches,
+        "clocks": clk,
+    }
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        threads = os.cpu_count() or 1
+        kind, run, desc = cpu_reference_runner(prob, threads)
+        rows = calibrated_sample(run, prob.R.M, args.cpu_seconds)
+        t = run(rows)
+        full = t * prob.R.M / rows
+        line["cpu_baseline"] = {
+            "value": total_bytes / full / 1e9, "unit": "GB/s", "cores": threads, "kind": kind,
+            "sample": f"rows 0..{rows} of {prob.R.M} of R ({desc}); {t:.2f} s, scaled to the "
+                      f"full product ({full:.1f} s)"}
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    ctx.close()
+    if dist is not None:
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

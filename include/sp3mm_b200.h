@@ -1,0 +1,276 @@
+/*
+ * sp3mm_b200.h -- C ABI of libsp3mm_b200.so, a B200 (sm_100a) implementation
+ * of the Sp3MM4AMG Galerkin triple product C = R*AC*P on ordered CSR.
+ *
+ * Two layers:
+ *
+ *  1. Drop-in entry points with the reference's names, signatures, structs,
+ *     ownership and error behaviour (andreadiiorio/Sp3MM4AMG; paths below are
+ *     relative to that project).  Inputs are host `spmat`s (64-bit IRP/JA,
+ *     FP64 AS), borrowed and not modified; the result is a fresh host `spmat`
+ *     whose AS/JA/IRP come from malloc/calloc so the caller's freeSpmat()
+ *     releases it.  Errors return NULL after a message on stderr.  The `_1`
+ *     variants take and return 1-based (FORTRAN) IRP/JA.
+ *
+ *  2. A device-resident layer (sp3mm_*): a context (device + CUDA stream),
+ *     CSR matrices resident in HBM with 32-bit indices, and products that
+ *     keep their operands and results on the device.  Functions return 0 on
+ *     success or a SP3MM_E* code.
+ *
+ * Every product of layer 1 and 2 runs on the GPU; there is no CPU fallback.
+ *
+ * Result semantics (both layers): row pointers and column indices equal the
+ * reference's; every value is accumulated in the reference's order with
+ * separately rounded FP64 multiplies and adds, so values are bit-identical to
+ * the reference's pair-wise functions (pair variants) and to
+ * sp3mmRowByRowMerged_ (direct variants).
+ *
+ * Limits: M, N < 2^31 and every matrix (inputs, intermediate, result) has
+ * fewer than 2^31 nonzeros; each input row's column indices must be strictly
+ * ascending (ordered CSR).  Violations return NULL / SP3MM_EINVAL.
+ */
+#ifndef SP3MM_B200_H
+#define SP3MM_B200_H
+
+#include <stdint.h>
+#include <stddef.h>
+
+#if defined(__GNUC__)
+#define SP3MM_API __attribute__((visibility("default")))
+#else
+#define SP3MM_API
+#endif
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- reference ABI types (same layout; skipped when the reference's own
+ * headers were included first) ------------------------------------------ */
+#ifndef CONFIG_H
+/* code/src/include/config.h:51 */
+typedef unsigned long idx_t;
+/* code/src/include/config.h:34-37 */
+typedef enum { RBTREE, IDXMAP } ROW_MMSYM_IMPL_MODE;
+/* code/src/include/config.h:42-49.  gridRows/gridCols/threadNum are accepted
+ * and ignored (the GPU partitions by row bins); chunkDistrbFunc, when not
+ * NULL, is called once per SpMM with (rows, matrix, cfg) as the reference
+ * does (code/src/Sp3MM_CSR_OMP_UB_Generic.c:83). */
+typedef struct {
+    unsigned short gridRows;
+    unsigned short gridCols;
+    ROW_MMSYM_IMPL_MODE symbMMRowImplID;
+    unsigned int threadNum;
+    void *chunkDistrbFunc;
+} CONFIG;
+#endif
+
+#ifndef SPARSEMATRIX
+/* code/src/include/sparseMatrix.h:41-53 (ROWLENS off). */
+typedef struct {
+    idx_t NZ, M, N;
+    double *AS;
+    idx_t *JA;
+    idx_t *IRP;
+    idx_t MAX_ROW_NZ;
+} spmat;
+#endif
+
+#ifndef SP3MM_CSR_OMP_MULTI_H
+/* code/src/include/Sp3MM_CSR_OMP_Multi.h:50-53 */
+typedef spmat *(SPMM)(spmat *, spmat *, CONFIG *);
+typedef spmat *(*SPMM_INTERF)(spmat *, spmat *, CONFIG *);
+typedef spmat *(SP3MM)(spmat *, spmat *, spmat *, CONFIG *, SPMM_INTERF);
+typedef spmat *(*SP3MM_INTERF)(spmat *, spmat *, spmat *, CONFIG *, SPMM_INTERF);
+#endif
+
+/* Timing globals of code/src/Sp3MM_CSR_OMP_Multi.c:54.  ElapsedInternal is
+ * set to the device time (seconds) of the last product's compute, without
+ * host<->device copies; Start/End bracket it in omp_get_wtime-like seconds. */
+SP3MM_API extern double Start, End, Elapsed, ElapsedInternal;
+
+/* ---- layer 1: drop-in entry points ------------------------------------- */
+
+/* Triple product as a pair of SpMMs, (R*AC)*P.
+ * Replaces code/src/Sp3MM_CSR_OMP_UB_Generic.c:456-494.  spmm == NULL selects
+ * spmmRowByRow2DBlocks_ as the reference does (:462-465).  When spmm is one
+ * of this library's SpMM entry points the intermediate stays on the device;
+ * any other function pointer is called twice on host matrices, as the
+ * reference does. */
+SP3MM_API SP3MM sp3mmRowByRowPair_0, sp3mmRowByRowPair_1;
+/* Direct row-forwarding triple product, upper-bound flavour.  Each R*AC row
+ * is forwarded into P in first-touch order.  spmm is ignored.
+ * Replaces code/src/Sp3MM_CSR_OMP_UB_Generic.c:498-573. */
+SP3MM_API SP3MM sp3mmRowByRowMerged_0, sp3mmRowByRowMerged_1;
+/* Pair-wise triple product with the symbolic-numeric SpMM; spmm == NULL
+ * selects spmmRowByRow_SymbNum_.  Declared but never defined by the
+ * reference (code/src/include/Sp3MM_CSR_OMP_Num_Generic.h:44). */
+SP3MM_API SP3MM sp3mmRowByRowPair_SymbNum_0, sp3mmRowByRowPair_SymbNum_1;
+/* Direct triple product, symbolic-numeric flavour: an exact symbolic pass
+ * sizes C, then the numeric pass writes it in place.  Same values as
+ * sp3mmRowByRowMerged_.  Declared, never defined, by the reference
+ * (code/src/include/Sp3MM_CSR_OMP_Num_Generic.h:51). */
+SP3MM_API SP3MM sp3mmRowByRowMerged_SymbNum_0, sp3mmRowByRowMerged_SymbNum_1;
+/* R*(AC*P): the right association, which the reference lacks.  spmm selects
+ * the flavour as in sp3mmRowByRowPair_ (NULL: upper bound). */
+SP3MM_API SP3MM sp3mmRowByRowPairRight_0, sp3mmRowByRowPairRight_1;
+
+/* SpMM, upper-bound flavour: per-row upper bounds, accumulation, atomic
+ * space booking and a compaction into exact CSR.  All five return the same
+ * matrix; the reference's 1D/2D OpenMP partitionings have no GPU meaning.
+ * Replace code/src/Sp3MM_CSR_OMP_UB_Generic.c:38-53 (spmmSerial_, broken in
+ * the reference), :56-124, :126-201, :205-338, :340-454. */
+SP3MM_API SPMM spmmSerial_0, spmmSerial_1;
+SP3MM_API SPMM spmmRowByRow_0, spmmRowByRow_1;
+SP3MM_API SPMM spmmRowByRow1DBlocks_0, spmmRowByRow1DBlocks_1;
+SP3MM_API SPMM spmmRowByRow2DBlocks_0, spmmRowByRow2DBlocks_1;
+SP3MM_API SPMM spmmRowByRow2DBlocksAllocated_0, spmmRowByRow2DBlocksAllocated_1;
+
+/* SpMM, symbolic-numeric flavour: exact row sizes, a scan to IRP, then the
+ * numeric pass writes sorted rows in place.
+ * Replace code/src/Sp3MM_CSR_OMP_Num_Generic.c:93-146, :147-210 and the
+ * 2D stub :211-239 (which always returns NULL in the reference). */
+SP3MM_API SPMM spmmRowByRow_SymbNum_0, spmmRowByRow_SymbNum_1;
+SP3MM_API SPMM spmmRowByRow1DBlocks_SymbNum_0, spmmRowByRow1DBlocks_SymbNum_1;
+SP3MM_API SPMM spmmRowByRow2DBlocks_SymbNum_0, spmmRowByRow2DBlocks_SymbNum_1;
+SP3MM_API SPMM spmmRowByRow2DBlocksAllocated_SymbNum_0, spmmRowByRow2DBlocksAllocated_SymbNum_1;
+
+/* Exact row sizes of a*b: malloc'd idx_t[a->M + 1], the total at [a->M].
+ * Both modes return the same counts.
+ * Replaces code/src/Sp3MM_CSR_OMP_SymbStep_Generic.c:281-412 (SpMM_Symb_). */
+SP3MM_API idx_t *SpMM_Symb___0(ROW_MMSYM_IMPL_MODE mode, spmat *a, spmat *b);
+SP3MM_API idx_t *SpMM_Symb___1(ROW_MMSYM_IMPL_MODE mode, spmat *a, spmat *b);
+
+/* Upper-bound row sizes of A*B (sum of the B row lengths selected by each A
+ * row): malloc'd idx_t[A->M + 1], the total at [A->M].
+ * Replaces code/src/include/SpMMUtilsGeneric.h:112-139. */
+SP3MM_API idx_t *spMMSizeUpperbound_0(spmat *A, spmat *B);
+SP3MM_API idx_t *spMMSizeUpperbound_1(spmat *A, spmat *B);
+
+/* Upper-bound sizes per (row of A, column partition of B):
+ * malloc'd idx_t[A->M*gridCols + 1], row-major, the total at the end.
+ * bColPartOffsets is B's column-partition offset matrix
+ * (code/src/commons/sparseUtilsGeneric.c:284-311).
+ * Replaces code/src/include/SpMMUtilsGeneric.h:146-174. */
+SP3MM_API idx_t *spMMSizeUpperboundColParts_0(spmat *A, spmat *B, unsigned short gridCols,
+                                    idx_t *bColPartOffsets);
+SP3MM_API idx_t *spMMSizeUpperboundColParts_1(spmat *A, spmat *B, unsigned short gridCols,
+                                    idx_t *bColPartOffsets);
+
+/* Dispatch tables with the reference's names and orders
+ * (code/src/include/Sp3MM_CSR_OMP_UB_Generic.h:86-95,
+ *  code/src/include/Sp3MM_CSR_OMP_Num_Generic.h:86-95), so that the
+ * reference's test driver relinks unchanged.  The SymbNum direct table gains
+ * its (new) entry. */
+#ifndef SP3MM_B200_NO_TABLES
+static SPMM_INTERF Spmm_UB_Funcs_0[] = {
+    &spmmRowByRow_0, &spmmRowByRow1DBlocks_0, &spmmRowByRow2DBlocks_0,
+    &spmmRowByRow2DBlocksAllocated_0};
+static SP3MM_INTERF Sp3mm_UB_Funcs_0[] = {&sp3mmRowByRowMerged_0};
+static SPMM_INTERF Spmm_SymbNum_Funcs_0[] = {
+    &spmmRowByRow_SymbNum_0, &spmmRowByRow1DBlocks_SymbNum_0};
+static SP3MM_INTERF Sp3mm_SymbNum_Funcs_0[] = {&sp3mmRowByRowMerged_SymbNum_0};
+static SPMM_INTERF Spmm_UB_Funcs_1[] = {
+    &spmmRowByRow_1, &spmmRowByRow1DBlocks_1, &spmmRowByRow2DBlocks_1,
+    &spmmRowByRow2DBlocksAllocated_1};
+static SP3MM_INTERF Sp3mm_UB_Funcs_1[] = {&sp3mmRowByRowMerged_1};
+static SPMM_INTERF Spmm_SymbNum_Funcs_1[] = {
+    &spmmRowByRow_SymbNum_1, &spmmRowByRow1DBlocks_SymbNum_1};
+static SP3MM_INTERF Sp3mm_SymbNum_Funcs_1[] = {&sp3mmRowByRowMerged_SymbNum_1};
+#endif
+
+/* ---- layer 2: device-resident products --------------------------------- */
+
+enum {
+    SP3MM_OK = 0,
+    SP3MM_ECUDA = 1,     /* a CUDA call failed (message on stderr) */
+    SP3MM_EINVAL = 2,    /* invalid argument or malformed CSR input */
+    SP3MM_ENOMEM = 3,    /* device allocation failed or budget exceeded */
+    SP3MM_ELIMIT = 4,    /* a size exceeds the 32-bit device index limits */
+    SP3MM_EDEVICE = 5    /* a kernel reported an internal error flag */
+};
+
+/* Flavours and variants of a product. */
+enum { SP3MM_UB = 0, SP3MM_SYMBNUM = 1 };
+enum { SP3MM_PAIR = 0, SP3MM_DIRECT = 1, SP3MM_PAIR_RIGHT = 2 };
+/* Value storage of a device matrix. */
+enum { SP3MM_F64 = 0, SP3MM_F32 = 1 };
+
+/* A CSR matrix resident in device memory: 0-based int32 row_ptr[M+1] and
+ * col[nnz] (ascending within each row), values in FP64 or FP32.  Arrays are
+ * owned by the library when created by it (free with sp3mm_dcsr_free). */
+typedef struct {
+    int32_t M, N;
+    int64_t nnz;
+    int32_t *row_ptr;
+    int32_t *col;
+    void *val;
+    int32_t val_type;   /* SP3MM_F64 or SP3MM_F32 */
+    int32_t max_row;    /* longest row, or -1 when unknown */
+} sp3mm_dcsr;
+
+typedef struct sp3mm_ctx sp3mm_ctx;
+
+/* Context on `device` with its own non-blocking stream. */
+SP3MM_API int sp3mm_ctx_create(int device, sp3mm_ctx **out);
+SP3MM_API int sp3mm_ctx_destroy(sp3mm_ctx *ctx);
+/* Run subsequent work on a caller-owned stream (cudaStream_t as void*);
+ * NULL restores the context's own stream. */
+SP3MM_API int sp3mm_ctx_set_stream(sp3mm_ctx *ctx, void *stream);
+SP3MM_API void *sp3mm_ctx_stream(sp3mm_ctx *ctx);
+/* Bytes of device memory the context may hold for workspace (0: no limit). */
+SP3MM_API int sp3mm_ctx_set_workspace_limit(sp3mm_ctx *ctx, size_t bytes);
+/* Release cached workspace. */
+SP3MM_API int sp3mm_ctx_trim(sp3mm_ctx *ctx);
+/* Last error message of this context (static storage of the context). */
+SP3MM_API const char *sp3mm_ctx_last_error(sp3mm_ctx *ctx);
+/* Kernel launches issued by this context since creation. */
+SP3MM_API uint64_t sp3mm_ctx_launches(sp3mm_ctx *ctx);
+/* Block until the context's stream is idle. */
+SP3MM_API int sp3mm_ctx_sync(sp3mm_ctx *ctx);
+/* Time every kernel launch with CUDA events on the context stream (on != 0);
+ * switching clears the records. */
+SP3MM_API int sp3mm_ctx_set_profiling(sp3mm_ctx *ctx, int on);
+/* Per-kernel totals since profiling was switched on, one line per kernel
+ * family: "<label> <launches> <total_ms> <max_ms>\n". */
+SP3MM_API int sp3mm_ctx_profile_report(sp3mm_ctx *ctx, char *buf, size_t len);
+
+/* Upload a host spmat (0- or 1-based per off_f), validating it, narrowing
+ * the indices to int32 and storing values as val_type. */
+SP3MM_API int sp3mm_dcsr_upload(sp3mm_ctx *ctx, const spmat *host, int off_f, int val_type,
+                      sp3mm_dcsr *out);
+/* Upload from plain host arrays (int64 row pointers and columns, FP64 values). */
+SP3MM_API int sp3mm_dcsr_upload_arrays(sp3mm_ctx *ctx, int64_t M, int64_t N, int64_t nnz,
+                             const int64_t *row_ptr, const int64_t *col,
+                             const double *val, int val_type, sp3mm_dcsr *out);
+/* Copy to a fresh host spmat (malloc'd arrays, indices shifted by off_f). */
+SP3MM_API int sp3mm_dcsr_download(sp3mm_ctx *ctx, const sp3mm_dcsr *m, int off_f, spmat **out);
+/* Copy into caller arrays (int64 row_ptr[M+1], int64 col[nnz], FP64 val[nnz]). */
+SP3MM_API int sp3mm_dcsr_download_arrays(sp3mm_ctx *ctx, const sp3mm_dcsr *m, int64_t *row_ptr,
+                               int64_t *col, double *val);
+SP3MM_API int sp3mm_dcsr_free(sp3mm_ctx *ctx, sp3mm_dcsr *m);
+
+/* C = A*B on the device, flavour SP3MM_UB or SP3MM_SYMBNUM; C's values are
+ * stored as out_val_type.  C is allocated by the library. */
+SP3MM_API int sp3mm_spmm(sp3mm_ctx *ctx, const sp3mm_dcsr *A, const sp3mm_dcsr *B, int flavour,
+               int out_val_type, sp3mm_dcsr *C);
+/* C = R*A*P on the device: variant SP3MM_PAIR, SP3MM_DIRECT or
+ * SP3MM_PAIR_RIGHT; flavour SP3MM_UB or SP3MM_SYMBNUM. */
+SP3MM_API int sp3mm_rap(sp3mm_ctx *ctx, const sp3mm_dcsr *R, const sp3mm_dcsr *A,
+              const sp3mm_dcsr *P, int variant, int flavour, int out_val_type,
+              sp3mm_dcsr *C);
+/* Exact row sizes / upper bounds of A*B into device int32 rows[M] (any of
+ * the pointers may be NULL); returns the totals through *total. */
+SP3MM_API int sp3mm_spmm_rowsizes(sp3mm_ctx *ctx, const sp3mm_dcsr *A, const sp3mm_dcsr *B,
+                        int exact, int32_t *rows_dev, int64_t *total);
+/* Device transpose (R = P^T), values kept in their storage type. */
+SP3MM_API int sp3mm_transpose(sp3mm_ctx *ctx, const sp3mm_dcsr *A, sp3mm_dcsr *AT);
+/* Upper bound of the device bytes a sp3mm_rap call may allocate. */
+SP3MM_API int sp3mm_rap_memory_estimate(const sp3mm_dcsr *R, const sp3mm_dcsr *A,
+                              const sp3mm_dcsr *P, int variant, int flavour,
+                              size_t *bytes);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* SP3MM_B200_H */

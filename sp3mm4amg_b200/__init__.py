@@ -1,0 +1,286 @@
+"""sp3mm4amg_b200 -- B200 (sm_100a) Galerkin triple product C = R*A*P.
+
+Python mirror of the reference's Sp3MM entry points (andreadiiorio/Sp3MM4AMG,
+code/src/include/Sp3MM_CSR_OMP_UB_Generic.h and Sp3MM_CSR_OMP_Num_Generic.h)
+over the C ABI of ``lib/libsp3mm_b200.so``, plus the device-resident layer
+(:class:`Context`, :class:`DeviceCSR`).  Every product runs on the GPU.
+
+Host API (layer 1, reference names, host CSR in and out)::
+
+    C = sp3mm(R, A, P, "sp3mmRowByRowPair_", spmm="spmmRowByRow_SymbNum_")
+    C = sp3mm(R, A, P, "sp3mmRowByRowMerged_")          # direct, upper bound
+    C = spmm(A, B, "spmmRowByRow_")                       # SpMM, upper bound
+
+Device API (layer 2, operands resident in HBM)::
+
+    with Context() as ctx:
+        dR, dA, dP = ctx.upload(R), ctx.upload(A), ctx.upload(P)
+        dC = ctx.rap(dR, dA, dP, variant=DIRECT, flavour=UB)
+        C = dC.download()
+"""
+from __future__ import annotations
+
+import ctypes
+
+import numpy as np
+
+from . import capi
+from .capi import (DIRECT, F32, F64, PAIR, PAIR_RIGHT, SYMBNUM, UB, sp3mm_dcsr)
+from .problems import CSR, Problem
+from .spmat import (CONFIG, HostSpMat, IDXMAP, RBTREE, SPMAT_P, array_from_idx_ptr,
+                    csr_from_spmat, idx_t, spmat)
+
+__all__ = [
+    "CSR", "Problem", "Context", "DeviceCSR", "Sp3mmError", "spmm", "sp3mm",
+    "symb_rowsizes", "ub_rowsizes", "ub_colparts_rowsizes", "elapsed_internal",
+    "UB", "SYMBNUM", "PAIR", "DIRECT", "PAIR_RIGHT", "F64", "F32", "RBTREE", "IDXMAP",
+]
+
+
+class Sp3mmError(RuntimeError):
+    """A library call failed (the C layer returned NULL or an error code)."""
+
+
+_libc = ctypes.CDLL(None)
+_libc.free.argtypes = [ctypes.c_void_p]
+
+
+def _free_spmat(p: int) -> None:
+    m = ctypes.cast(p, SPMAT_P).contents
+    for arr in (m.AS, m.JA, m.IRP):
+        _libc.free(ctypes.cast(arr, ctypes.c_void_p))
+    _libc.free(p)
+
+
+def _take_spmat(p, off_f: int) -> CSR:
+    if not p:
+        raise Sp3mmError("libsp3mm_b200 returned NULL (see stderr)")
+    try:
+        return csr_from_spmat(p, off_f)
+    finally:
+        _free_spmat(p)
+
+
+def _config(cfg: CONFIG | None) -> CONFIG:
+    if cfg is not None:
+        return cfg
+    return CONFIG(gridRows=20, gridCols=2, symbMMRowImplID=RBTREE, threadNum=1,
+                  chunkDistrbFunc=None)
+
+
+def spmm(A: CSR, B: CSR, name: str = "spmmRowByRow_SymbNum_", off_f: int = 0,
+         cfg: CONFIG | None = None) -> CSR:
+    """C = A*B through the reference-named SpMM entry point ``name``."""
+    lib = capi.load()
+    a, b = HostSpMat(A, off_f), HostSpMat(B, off_f)
+    c = _config(cfg)
+    f = getattr(lib, f"{name}{off_f}")
+    return _take_spmat(f(a.ptr, b.ptr, ctypes.byref(c)), off_f)
+
+
+def sp3mm(R: CSR, A: CSR, P: CSR, name: str = "sp3mmRowByRowPair_", spmm: str | None = None,
+          off_f: int = 0, cfg: CONFIG | None = None) -> CSR:
+    """C = R*A*P through the reference-named triple-product entry point.
+
+    ``spmm`` names this library's SpMM entry point handed to the driver
+    (``None`` passes NULL, the driver's default).
+    """
+    lib = capi.load()
+    r, a, p = HostSpMat(R, off_f), HostSpMat(A, off_f), HostSpMat(P, off_f)
+    c = _config(cfg)
+    fp = None
+    if spmm is not None:
+        fp = ctypes.cast(getattr(lib, f"{spmm}{off_f}"), ctypes.c_void_p).value
+    f = getattr(lib, f"{name}{off_f}")
+    return _take_spmat(f(r.ptr, a.ptr, p.ptr, ctypes.byref(c), fp), off_f)
+
+
+def _sizes(p, n: int) -> np.ndarray:
+    if not p:
+        raise Sp3mmError("libsp3mm_b200 returned NULL (see stderr)")
+    try:
+        return array_from_idx_ptr(p, n)
+    finally:
+        _libc.free(p)
+
+
+def symb_rowsizes(A: CSR, B: CSR, off_f: int = 0, mode: int = RBTREE) -> np.ndarray:
+    """Exact row sizes of A*B with the total at [M] (SpMM_Symb___)."""
+    lib = capi.load()
+    a, b = HostSpMat(A, off_f), HostSpMat(B, off_f)
+    return _sizes(getattr(lib, f"SpMM_Symb___{off_f}")(mode, a.ptr, b.ptr), A.M + 1)
+
+
+def ub_rowsizes(A: CSR, B: CSR, off_f: int = 0) -> np.ndarray:
+    """Upper-bound row sizes of A*B with the total at [M] (spMMSizeUpperbound_)."""
+    lib = capi.load()
+    a, b = HostSpMat(A, off_f), HostSpMat(B, off_f)
+    return _sizes(getattr(lib, f"spMMSizeUpperbound_{off_f}")(a.ptr, b.ptr), A.M + 1)
+
+
+def ub_colparts_rowsizes(A: CSR, B: CSR, grid_cols: int, b_col_offsets: np.ndarray,
+                         off_f: int = 0) -> np.ndarray:
+    """Upper bounds per (row, column partition) (spMMSizeUpperboundColParts_)."""
+    lib = capi.load()
+    a, b = HostSpMat(A, off_f), HostSpMat(B, off_f)
+    offs = np.ascontiguousarray(b_col_offsets, dtype=np.uint64)
+    f = getattr(lib, f"spMMSizeUpperboundColParts_{off_f}")
+    return _sizes(f(a.ptr, b.ptr, grid_cols, offs.ctypes.data_as(ctypes.POINTER(idx_t))),
+                  A.M * grid_cols + 1)
+
+
+def elapsed_internal() -> float:
+    """Device seconds of the last layer-1 product (the ElapsedInternal global)."""
+    return capi.global_double(capi.load(), "ElapsedInternal")
+
+
+# ---------------------------------------------------------------------------
+# Layer 2.
+
+class DeviceCSR:
+    """A CSR matrix resident in device memory (owned by its context)."""
+
+    def __init__(self, ctx: "Context", d: sp3mm_dcsr):
+        self.ctx = ctx
+        self.d = d
+
+    @property
+    def shape(self):
+        return (int(self.d.M), int(self.d.N))
+
+    @property
+    def nnz(self) -> int:
+        return int(self.d.nnz)
+
+    @property
+    def val_type(self) -> int:
+        return int(self.d.val_type)
+
+    @property
+    def max_row(self) -> int:
+        return int(self.d.max_row)
+
+    @property
+    def ref(self):
+        return ctypes.byref(self.d)
+
+    def download(self) -> CSR:
+        M, nnz = self.shape[0], self.nnz
+        rp = np.empty(M + 1, np.int64)
+        ci = np.empty(max(nnz, 1), np.int64)
+        v = np.empty(max(nnz, 1), np.float64)
+        self.ctx._check(self.ctx.lib.sp3mm_dcsr_download_arrays(
+            self.ctx.h, self.ref, rp.ctypes.data, ci.ctypes.data, v.ctypes.data))
+        return CSR(rp, ci[:nnz], v[:nnz], self.shape)
+
+    def free(self) -> None:
+        if self.d.row_ptr or self.d.col or self.d.val:
+            self.ctx.lib.sp3mm_dcsr_free(self.ctx.h, self.ref)
+
+    def bytes(self, idx_bytes: int = 4) -> int:
+        vb = 4 if self.val_type == F32 else 8
+        return (self.shape[0] + 1) * idx_bytes + self.nnz * (idx_bytes + vb)
+
+
+class Context:
+    """A device context: CUDA device, stream and the library's workspace."""
+
+    def __init__(self, device: int = 0, stream: int | None = None):
+        self.lib = capi.load()
+        h = ctypes.c_void_p()
+        rc = self.lib.sp3mm_ctx_create(device, ctypes.byref(h))
+        if rc:
+            raise Sp3mmError(f"sp3mm_ctx_create failed ({rc})")
+        self.h = h
+        if stream is not None:
+            self.set_stream(stream)
+
+    def _check(self, rc: int) -> None:
+        if rc:
+            msg = self.lib.sp3mm_ctx_last_error(self.h)
+            raise Sp3mmError(f"error {rc}: {msg.decode() if msg else ''}")
+
+    def set_stream(self, stream: int | None) -> None:
+        self._check(self.lib.sp3mm_ctx_set_stream(self.h, stream))
+
+    @property
+    def stream(self) -> int:
+        return int(self.lib.sp3mm_ctx_stream(self.h) or 0)
+
+    def sync(self) -> None:
+        self._check(self.lib.sp3mm_ctx_sync(self.h))
+
+    def launches(self) -> int:
+        return int(self.lib.sp3mm_ctx_launches(self.h))
+
+    def set_profiling(self, on: bool) -> None:
+        """Time every kernel launch with CUDA events on the context stream."""
+        self._check(self.lib.sp3mm_ctx_set_profiling(self.h, 1 if on else 0))
+
+    def profile(self) -> dict:
+        """{label: (launches, total_ms, max_ms)} since profiling was switched on."""
+        buf = ctypes.create_string_buffer(1 << 16)
+        self._check(self.lib.sp3mm_ctx_profile_report(self.h, buf, len(buf)))
+        out = {}
+        for line in buf.value.decode().splitlines():
+            label, n, tot, mx = line.split()
+            out[label] = (int(n), float(tot), float(mx))
+        return out
+
+    def upload(self, m: CSR, val_type: int = F64) -> DeviceCSR:
+        d = sp3mm_dcsr()
+        rp = np.ascontiguousarray(m.indptr, np.int64)
+        ci = np.ascontiguousarray(m.indices, np.int64)
+        v = np.ascontiguousarray(m.data, np.float64)
+        self._check(self.lib.sp3mm_dcsr_upload_arrays(
+            self.h, m.M, m.N, m.nnz, rp.ctypes.data, ci.ctypes.data, v.ctypes.data, val_type,
+            ctypes.byref(d)))
+        return DeviceCSR(self, d)
+
+    def spmm(self, A: DeviceCSR, B: DeviceCSR, flavour: int = SYMBNUM,
+             out_val_type: int = F64) -> DeviceCSR:
+        d = sp3mm_dcsr()
+        self._check(self.lib.sp3mm_spmm(self.h, A.ref, B.ref, flavour, out_val_type,
+                                        ctypes.byref(d)))
+        return DeviceCSR(self, d)
+
+    def rap(self, R: DeviceCSR, A: DeviceCSR, P: DeviceCSR, variant: int = DIRECT,
+            flavour: int = UB, out_val_type: int = F64) -> DeviceCSR:
+        d = sp3mm_dcsr()
+        self._check(self.lib.sp3mm_rap(self.h, R.ref, A.ref, P.ref, variant, flavour,
+                                       out_val_type, ctypes.byref(d)))
+        return DeviceCSR(self, d)
+
+    def transpose(self, A: DeviceCSR) -> DeviceCSR:
+        d = sp3mm_dcsr()
+        self._check(self.lib.sp3mm_transpose(self.h, A.ref, ctypes.byref(d)))
+        return DeviceCSR(self, d)
+
+    def rowsizes(self, A: DeviceCSR, B: DeviceCSR, exact: bool = True):
+        """(per-row sizes as int64 numpy array, total)."""
+        import torch  # device buffer for the row sizes
+        M = A.shape[0]
+        buf = torch.empty(max(M, 1), dtype=torch.int32, device="cuda")
+        tot = ctypes.c_int64()
+        self._check(self.lib.sp3mm_spmm_rowsizes(self.h, A.ref, B.ref, 1 if exact else 0,
+                                                 buf.data_ptr(), ctypes.byref(tot)))
+        self.sync()
+        return buf[:M].cpu().numpy().astype(np.int64), int(tot.value)
+
+    def rap_memory_estimate(self, R: DeviceCSR, A: DeviceCSR, P: DeviceCSR,
+                            variant: int = DIRECT, flavour: int = UB) -> int:
+        b = ctypes.c_size_t()
+        self._check(self.lib.sp3mm_rap_memory_estimate(R.ref, A.ref, P.ref, variant, flavour,
+                                                       ctypes.byref(b)))
+        return int(b.value)
+
+    def close(self) -> None:
+        if self.h:
+            self.lib.sp3mm_ctx_destroy(self.h)
+            self.h = None
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()

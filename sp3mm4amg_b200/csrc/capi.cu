@@ -1,0 +1,1224 @@
+// capi.cu -- host runtime and C ABI of libsp3mm_b200.so.
+//
+// Layer 2 (sp3mm_*): contexts, device-resident CSR, device products.
+// Layer 1 (reference names): upload host spmat -> device product -> download
+// into malloc'd host spmat, with the reference's ownership and NULL-on-error
+// behaviour (code/src/include/Sp3MM_CSR_OMP_Multi.h:50-53,
+// code/src/include/sparseMatrix.h:154-168, code/src/include/macros.h:85-86).
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <chrono>
+#include <cstdarg>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <mutex>
+#include <string>
+#include <vector>
+
+#include "kernels.cuh"
+#include "sp3mm_b200.h"
+#include "sp3mm_internal.cuh"
+
+using namespace sp3mm;
+
+double Start = 0.0, End = 0.0, Elapsed = 0.0, ElapsedInternal = 0.0;
+
+struct sp3mm_ctx {
+    int device = 0;
+    int num_sms = 148;
+    cudaStream_t own_stream = nullptr;
+    cudaStream_t stream = nullptr;
+    unsigned* d_err = nullptr;           // sticky device error word
+    size_t ws_limit = 0;
+    size_t smem_budget = 110 * 1024;
+    std::string last_error;
+    cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+    // Optional per-launch timing (events on the context stream).
+    struct ProfRec {
+        const char* label;
+        cudaEvent_t a, b;
+    };
+    bool profiling = false;
+    std::vector<ProfRec> prof;
+};
+
+namespace {
+
+void prof_clear(sp3mm_ctx* ctx) {
+    for (auto& r : ctx->prof) {
+        cudaEventDestroy(r.a);
+        cudaEventDestroy(r.b);
+    }
+    ctx->prof.clear();
+}
+
+// Run `f` (which launches kernels on ctx->stream), bracketed by events when
+// profiling is on.
+template <typename F>
+void prof(sp3mm_ctx* ctx, const char* label, F&& f) {
+    if (!ctx->profiling) {
+        f();
+        return;
+    }
+    sp3mm_ctx::ProfRec r{label, nullptr, nullptr};
+    cudaEventCreate(&r.a);
+    cudaEventCreate(&r.b);
+    cudaEventRecord(r.a, ctx->stream);
+    f();
+    cudaEventRecord(r.b, ctx->stream);
+    ctx->prof.push_back(r);
+}
+
+double wall_seconds() {
+    using namespace std::chrono;
+    return duration<double>(steady_clock::now().time_since_epoch()).count();
+}
+
+int set_error(sp3mm_ctx* ctx, int code, const char* fmt, ...) {
+    char buf[512];
+    va_list ap;
+    va_start(ap, fmt);
+    vsnprintf(buf, sizeof buf, fmt, ap);
+    va_end(ap);
+    if (ctx) ctx->last_error = buf;
+    fprintf(stderr, "sp3mm_b200: %s\n", buf);
+    return code;
+}
+
+#define CK(ctx, call)                                                                   \
+    do {                                                                                \
+        cudaError_t e_ = (call);                                                        \
+        if (e_ != cudaSuccess)                                                          \
+            return set_error((ctx), SP3MM_ECUDA, "%s failed: %s (%s:%d)", #call,        \
+                             cudaGetErrorString(e_), __FILE__, __LINE__);               \
+    } while (0)
+
+#define TRY(expr)                 \
+    do {                          \
+        int rc_ = (expr);         \
+        if (rc_ != SP3MM_OK) return rc_; \
+    } while (0)
+
+// Stream-ordered device allocation from the device's memory pool.
+struct DevBuf {
+    sp3mm_ctx* ctx = nullptr;
+    void* p = nullptr;
+    DevBuf() = default;
+    DevBuf(const DevBuf&) = delete;
+    DevBuf& operator=(const DevBuf&) = delete;
+    ~DevBuf() { release(); }
+    int alloc(sp3mm_ctx* c, size_t bytes) {
+        release();
+        ctx = c;
+        if (bytes == 0) bytes = 16;
+        cudaError_t e = cudaMallocAsync(&p, bytes, c->stream);
+        if (e != cudaSuccess) {
+            p = nullptr;
+            cudaGetLastError();
+            return set_error(c, SP3MM_ENOMEM, "device allocation of %zu bytes failed: %s", bytes,
+                             cudaGetErrorString(e));
+        }
+        return SP3MM_OK;
+    }
+    void release() {
+        if (p && ctx) cudaFreeAsync(p, ctx->stream);
+        p = nullptr;
+    }
+    void* detach() {
+        void* q = p;
+        p = nullptr;
+        return q;
+    }
+    template <typename T> T* as() const { return static_cast<T*>(p); }
+};
+
+CsrView view(const sp3mm_dcsr& m) {
+    return CsrView{m.M, m.N, m.nnz, m.row_ptr, m.col, m.val, m.val_type};
+}
+
+size_t vbytes(int vt) { return vt == SP3MM_F32 ? 4 : 8; }
+
+int check_dcsr(sp3mm_ctx* ctx, const sp3mm_dcsr* m, const char* what) {
+    if (!m) return set_error(ctx, SP3MM_EINVAL, "%s is NULL", what);
+    if (m->M < 0 || m->N < 0 || m->nnz < 0 || !m->row_ptr || (m->nnz > 0 && (!m->col || !m->val)))
+        return set_error(ctx, SP3MM_EINVAL, "%s is not a valid device CSR", what);
+    if (m->val_type != SP3MM_F64 && m->val_type != SP3MM_F32)
+        return set_error(ctx, SP3MM_EINVAL, "%s has an unknown value type", what);
+    return SP3MM_OK;
+}
+
+// Small device block of counters used by one binning pass.
+struct Counters {
+    int counts[kLevels + 1];
+    int cursors[kLevels];
+    int gmax;
+    int pad;
+    unsigned long long total;
+    unsigned err;
+    unsigned pad2;
+};
+
+// Row lists by level, built from per-row `need`.
+struct Bins {
+    int counts[kLevels + 1] = {};
+    int offsets[kLevels] = {};
+    int gmax = 0;
+    unsigned long long total = 0;
+    DevBuf level, lists;
+};
+
+int read_err(sp3mm_ctx* ctx, unsigned* out) {
+    CK(ctx, cudaMemcpyAsync(out, ctx->d_err, sizeof(unsigned), cudaMemcpyDeviceToHost,
+                            ctx->stream));
+    CK(ctx, cudaStreamSynchronize(ctx->stream));
+    return SP3MM_OK;
+}
+
+int check_device_err(sp3mm_ctx* ctx) {
+    unsigned e = 0;
+    TRY(read_err(ctx, &e));
+    if (e) {
+        CK(ctx, cudaMemsetAsync(ctx->d_err, 0, sizeof(unsigned), ctx->stream));
+        if (e & kErrInput) return set_error(ctx, SP3MM_EINVAL, "malformed CSR input (flags 0x%x)", e);
+        return set_error(ctx, SP3MM_EDEVICE, "device error flags 0x%x", e);
+    }
+    return SP3MM_OK;
+}
+
+// Bin M rows by `need`; `dcnt` receives the device counters (total is
+// accumulated there by the bounds kernel beforehand); row_cnt of empty rows
+// is zeroed.
+int bin_rows(sp3mm_ctx* ctx, int M, const int* need, Counters* dcnt, int* row_cnt, Bins& b) {
+    TRY(b.level.alloc(ctx, static_cast<size_t>(M) + 1));
+    TRY(b.lists.alloc(ctx, sizeof(int) * (static_cast<size_t>(M) + 1)));
+    prof(ctx, "bin.levels", [&] {
+        launch_bin_levels(M, need, b.level.as<signed char>(), dcnt->counts, &dcnt->gmax,
+                          row_cnt, ctx->stream);
+    });
+    Counters h{};
+    CK(ctx, cudaMemcpyAsync(&h, dcnt, sizeof h, cudaMemcpyDeviceToHost, ctx->stream));
+    CK(ctx, cudaStreamSynchronize(ctx->stream));
+    int off = 0;
+    for (int L = 0; L < kLevels; ++L) {
+        b.counts[L] = h.counts[L];
+        b.offsets[L] = off;
+        h.cursors[L] = off;
+        off += h.counts[L];
+    }
+    b.counts[kLevels] = h.counts[kLevels];
+    b.gmax = h.gmax;
+    b.total = h.total;
+    CK(ctx, cudaMemcpyAsync(dcnt->cursors, h.cursors, sizeof h.cursors, cudaMemcpyHostToDevice,
+                            ctx->stream));
+    prof(ctx, "bin.scatter", [&] {
+        launch_bin_scatter(M, b.level.as<signed char>(), dcnt->cursors, b.lists.as<int>(),
+                           ctx->stream);
+    });
+    return SP3MM_OK;
+}
+
+// Run one row kernel family over every non-empty level.
+template <typename Launch>
+int run_levels(sp3mm_ctx* ctx, const Bins& b, bool direct, int mode, int G, Launch&& launch) {
+    for (int L = 0; L < kLevels; ++L) {
+        const int n = b.counts[L];
+        if (!n) continue;
+        LevelPlan pl = plan_level(L, direct, mode, G, ctx->smem_budget);
+        RowSet rs{};
+        rs.rows = b.lists.as<int>() + b.offsets[L];
+        rs.nrows = n;
+        DevBuf gtab;
+        int grid;
+        if (L == kGlobalLevel) pl.slots = static_cast<int>(slots_for(b.gmax));
+        if (!pl.global) {
+            const int gpc = pl.groups_per_cta;
+            grid = (n + gpc - 1) / gpc;
+            const int cap = ctx->num_sms * 8;
+            if (grid > cap) grid = cap;
+        } else {
+            // Tables in global memory: one region per group; bound the number
+            // of concurrent groups by a 2 GiB scratch budget.
+            const size_t stride = static_cast<size_t>(bytes_per_slot(direct, mode)) * pl.slots;
+            size_t groups = static_cast<size_t>(n);
+            const size_t cap_groups = static_cast<size_t>(ctx->num_sms) * 8;
+            if (groups > cap_groups) groups = cap_groups;
+            const size_t budget = size_t(2) << 30;
+            while (groups > 1 && groups * stride > budget) groups >>= 1;
+            groups = (groups + pl.groups_per_cta - 1) / pl.groups_per_cta * pl.groups_per_cta;
+            TRY(gtab.alloc(ctx, groups * stride));
+            rs.gtab = gtab.as<unsigned char>();
+            rs.gtab_stride = static_cast<long long>(stride);
+            grid = static_cast<int>(groups / pl.groups_per_cta);
+        }
+        rs.slots = pl.slots;
+        rs.shift = 32 - ilog2_pow2(static_cast<unsigned>(pl.slots));
+        static const char* const kLabels[2][3] = {
+            {"pair.rows.symb", "pair.rows.num", "pair.rows.book"},
+            {"direct.rows.symb", "direct.rows.num", "direct.rows.book"}};
+        prof(ctx, kLabels[direct ? 1 : 0][mode], [&] { launch(pl, rs, grid); });
+        CK(ctx, cudaGetLastError());
+    }
+    return SP3MM_OK;
+}
+
+int alloc_matrix(sp3mm_ctx* ctx, int M, int N, long long nnz, int vt, sp3mm_dcsr* C,
+                 DevBuf& rp, DevBuf& ci, DevBuf& v) {
+    TRY(rp.alloc(ctx, sizeof(int) * (static_cast<size_t>(M) + 1)));
+    TRY(ci.alloc(ctx, sizeof(int) * static_cast<size_t>(nnz)));
+    TRY(v.alloc(ctx, vbytes(vt) * static_cast<size_t>(nnz)));
+    C->M = M;
+    C->N = N;
+    C->nnz = nnz;
+    C->row_ptr = rp.as<int>();
+    C->col = ci.as<int>();
+    C->val = v.p;
+    C->val_type = vt;
+    C->max_row = -1;
+    return SP3MM_OK;
+}
+
+int finish_matrix(sp3mm_dcsr* C, DevBuf& rp, DevBuf& ci, DevBuf& v) {
+    C->row_ptr = static_cast<int*>(rp.detach());
+    C->col = static_cast<int*>(ci.detach());
+    C->val = v.detach();
+    return SP3MM_OK;
+}
+
+// Scan row counts into a fresh C; returns the total (checks the int32 limit).
+int scan_counts(sp3mm_ctx* ctx, int M, const int* row_cnt, DevBuf& rp, long long* total) {
+    TRY(rp.alloc(ctx, sizeof(int) * (static_cast<size_t>(M) + 1)));
+    DevBuf tmp;
+    const size_t tb = scan_temp_bytes(M);
+    TRY(tmp.alloc(ctx, tb));
+    prof(ctx, "scan", [&] { launch_scan(M, row_cnt, rp.as<int>(), tmp.p, tb, ctx->stream); });
+    CK(ctx, cudaGetLastError());
+    int t = 0;
+    CK(ctx, cudaMemcpyAsync(&t, rp.as<int>() + M, sizeof(int), cudaMemcpyDeviceToHost,
+                            ctx->stream));
+    CK(ctx, cudaStreamSynchronize(ctx->stream));
+    *total = t;
+    return SP3MM_OK;
+}
+
+// ---------------------------------------------------------------------------
+// C = A*B.
+int spmm_impl(sp3mm_ctx* ctx, const sp3mm_dcsr& A, const sp3mm_dcsr& B, int flavour, int out_vt,
+              sp3mm_dcsr* C) {
+    if (A.N != B.M)
+        return set_error(ctx, SP3MM_EINVAL, "inner dimensions differ (%d vs %d)", A.N, B.M);
+    const int M = A.M;
+    const cudaStream_t st = ctx->stream;
+    const CsrView a = view(A), bv = view(B);
+    const int G = choose_group(B.M ? static_cast<double>(B.nnz) / B.M : 1.0);
+
+    DevBuf cnt_buf, need, row_cnt;
+    TRY(cnt_buf.alloc(ctx, sizeof(Counters)));
+    TRY(need.alloc(ctx, sizeof(int) * (static_cast<size_t>(M) + 1)));
+    TRY(row_cnt.alloc(ctx, sizeof(int) * (static_cast<size_t>(M) + 1)));
+    Counters* dc = cnt_buf.as<Counters>();
+    CK(ctx, cudaMemsetAsync(dc, 0, sizeof(Counters), st));
+    prof(ctx, "pair.bounds", [&] { launch_pair_bounds(a, bv, need.as<int>(), &dc->total, st); });
+    Bins bins;
+    TRY(bin_rows(ctx, M, need.as<int>(), dc, row_cnt.as<int>(), bins));
+
+    PairArgs pa{};
+    pa.A = a;
+    pa.B = bv;
+    pa.row_cnt = row_cnt.as<int>();
+    pa.err = ctx->d_err;
+    pa.c_vtype = out_vt;
+
+    DevBuf rp, ci, v;
+    long long nnz = 0;
+    if (flavour == SP3MM_SYMBNUM) {
+        TRY(run_levels(ctx, bins, false, kSymb, G, [&](const LevelPlan& pl, const RowSet& rs, int grid) {
+            launch_pair_rows(pa, kSymb, pl, rs, grid, st);
+        }));
+        TRY(scan_counts(ctx, M, row_cnt.as<int>(), rp, &nnz));
+        TRY(check_device_err(ctx));
+        if (nnz < 0 || nnz >= INT32_MAX)
+            return set_error(ctx, SP3MM_ELIMIT, "result has too many nonzeros");
+        TRY(ci.alloc(ctx, sizeof(int) * static_cast<size_t>(nnz)));
+        TRY(v.alloc(ctx, vbytes(out_vt) * static_cast<size_t>(nnz)));
+        // Re-bin by exact sizes: tighter tables for the numeric pass.
+        CK(ctx, cudaMemsetAsync(dc, 0, sizeof(Counters), st));
+        launch_need_from_counts(M, row_cnt.as<int>(), nullptr, need.as<int>(), st);
+        Bins nb;
+        TRY(bin_rows(ctx, M, need.as<int>(), dc, nullptr, nb));
+        pa.c_rp = rp.as<int>();
+        pa.c_ci = ci.as<int>();
+        pa.c_v = v.p;
+        TRY(run_levels(ctx, nb, false, kNumExact, G, [&](const LevelPlan& pl, const RowSet& rs, int grid) {
+            launch_pair_rows(pa, kNumExact, pl, rs, grid, st);
+        }));
+    } else {
+        const unsigned long long cap = bins.total;
+        DevBuf ub_ci, ub_v, row_off;
+        TRY(ub_ci.alloc(ctx, sizeof(int) * cap));
+        TRY(ub_v.alloc(ctx, vbytes(out_vt) * cap));
+        TRY(row_off.alloc(ctx, sizeof(long long) * (static_cast<size_t>(M) + 1)));
+        pa.book_cursor = &dc->total;   // reuse: reset below
+        CK(ctx, cudaMemsetAsync(&dc->total, 0, sizeof(unsigned long long), st));
+        pa.book_cap = cap;
+        pa.row_off = row_off.as<long long>();
+        pa.ub_ci = ub_ci.as<int>();
+        pa.ub_v = ub_v.p;
+        TRY(run_levels(ctx, bins, false, kNumBook, G, [&](const LevelPlan& pl, const RowSet& rs, int grid) {
+            launch_pair_rows(pa, kNumBook, pl, rs, grid, st);
+        }));
+        TRY(scan_counts(ctx, M, row_cnt.as<int>(), rp, &nnz));
+        TRY(check_device_err(ctx));
+        if (nnz < 0 || nnz >= INT32_MAX)
+            return set_error(ctx, SP3MM_ELIMIT, "result has too many nonzeros");
+        TRY(ci.alloc(ctx, sizeof(int) * static_cast<size_t>(nnz)));
+        TRY(v.alloc(ctx, vbytes(out_vt) * static_cast<size_t>(nnz)));
+        prof(ctx, "compact", [&] {
+            launch_compact(M, row_cnt.as<int>(), row_off.as<long long>(), ub_ci.as<int>(),
+                           ub_v.p, rp.as<int>(), ci.as<int>(), v.p, out_vt, st);
+        });
+    }
+    TRY(check_device_err(ctx));
+    C->M = M;
+    C->N = B.N;
+    C->nnz = nnz;
+    C->val_type = out_vt;
+    C->max_row = -1;
+    return finish_matrix(C, rp, ci, v);
+}
+
+// C = R*A*P, direct (row forwarding).
+int direct_impl(sp3mm_ctx* ctx, const sp3mm_dcsr& R, const sp3mm_dcsr& A, const sp3mm_dcsr& P,
+                int flavour, int out_vt, sp3mm_dcsr* C) {
+    if (R.N != A.M || A.N != P.M)
+        return set_error(ctx, SP3MM_EINVAL, "inner dimensions differ");
+    const int M = R.M;
+    const cudaStream_t st = ctx->stream;
+    const double mean = std::max(A.M ? static_cast<double>(A.nnz) / A.M : 1.0,
+                                 P.M ? static_cast<double>(P.nnz) / P.M : 1.0);
+    const int G = choose_group(mean);
+
+    DevBuf cnt_buf, need, row_cnt, row_cnt1;
+    TRY(cnt_buf.alloc(ctx, sizeof(Counters)));
+    TRY(need.alloc(ctx, sizeof(int) * (static_cast<size_t>(M) + 1)));
+    TRY(row_cnt.alloc(ctx, sizeof(int) * (static_cast<size_t>(M) + 1)));
+    Counters* dc = cnt_buf.as<Counters>();
+    CK(ctx, cudaMemsetAsync(dc, 0, sizeof(Counters), st));
+    prof(ctx, "direct.bounds", [&] {
+        launch_direct_bounds(view(R), view(A), view(P), need.as<int>(), &dc->total, st);
+    });
+    Bins bins;
+    TRY(bin_rows(ctx, M, need.as<int>(), dc, row_cnt.as<int>(), bins));
+
+    DirectArgs da{};
+    da.R = view(R);
+    da.A = view(A);
+    da.P = view(P);
+    da.row_cnt = row_cnt.as<int>();
+    da.err = ctx->d_err;
+    da.c_vtype = out_vt;
+
+    DevBuf rp, ci, v;
+    long long nnz = 0;
+    if (flavour == SP3MM_SYMBNUM) {
+        TRY(row_cnt1.alloc(ctx, sizeof(int) * (static_cast<size_t>(M) + 1)));
+        CK(ctx, cudaMemsetAsync(row_cnt1.p, 0, sizeof(int) * (static_cast<size_t>(M) + 1), st));
+        da.row_cnt1 = row_cnt1.as<int>();
+        TRY(run_levels(ctx, bins, true, kSymb, G, [&](const LevelPlan& pl, const RowSet& rs, int grid) {
+            launch_direct_rows(da, kSymb, pl, rs, grid, st);
+        }));
+        TRY(scan_counts(ctx, M, row_cnt.as<int>(), rp, &nnz));
+        TRY(check_device_err(ctx));
+        if (nnz < 0 || nnz >= INT32_MAX)
+            return set_error(ctx, SP3MM_ELIMIT, "result has too many nonzeros");
+        TRY(ci.alloc(ctx, sizeof(int) * static_cast<size_t>(nnz)));
+        TRY(v.alloc(ctx, vbytes(out_vt) * static_cast<size_t>(nnz)));
+        CK(ctx, cudaMemsetAsync(dc, 0, sizeof(Counters), st));
+        launch_need_from_counts(M, row_cnt.as<int>(), row_cnt1.as<int>(), need.as<int>(), st);
+        Bins nb;
+        TRY(bin_rows(ctx, M, need.as<int>(), dc, nullptr, nb));
+        da.row_cnt1 = nullptr;
+        da.c_rp = rp.as<int>();
+        da.c_ci = ci.as<int>();
+        da.c_v = v.p;
+        TRY(run_levels(ctx, nb, true, kNumExact, G, [&](const LevelPlan& pl, const RowSet& rs, int grid) {
+            launch_direct_rows(da, kNumExact, pl, rs, grid, st);
+        }));
+    } else {
+        const unsigned long long cap = bins.total;
+        DevBuf ub_ci, ub_v, row_off;
+        TRY(ub_ci.alloc(ctx, sizeof(int) * cap));
+        TRY(ub_v.alloc(ctx, vbytes(out_vt) * cap));
+        TRY(row_off.alloc(ctx, sizeof(long long) * (static_cast<size_t>(M) + 1)));
+        CK(ctx, cudaMemsetAsync(&dc->total, 0, sizeof(unsigned long long), st));
+        da.book_cursor = &dc->total;
+        da.book_cap = cap;
+        da.row_off = row_off.as<long long>();
+        da.ub_ci = ub_ci.as<int>();
+        da.ub_v = ub_v.p;
+        TRY(run_levels(ctx, bins, true, kNumBook, G, [&](const LevelPlan& pl, const RowSet& rs, int grid) {
+            launch_direct_rows(da, kNumBook, pl, rs, grid, st);
+        }));
+        TRY(scan_counts(ctx, M, row_cnt.as<int>(), rp, &nnz));
+        TRY(check_device_err(ctx));
+        if (nnz < 0 || nnz >= INT32_MAX)
+            return set_error(ctx, SP3MM_ELIMIT, "result has too many nonzeros");
+        TRY(ci.alloc(ctx, sizeof(int) * static_cast<size_t>(nnz)));
+        TRY(v.alloc(ctx, vbytes(out_vt) * static_cast<size_t>(nnz)));
+        prof(ctx, "compact", [&] {
+            launch_compact(M, row_cnt.as<int>(), row_off.as<long long>(), ub_ci.as<int>(),
+                           ub_v.p, rp.as<int>(), ci.as<int>(), v.p, out_vt, st);
+        });
+    }
+    TRY(check_device_err(ctx));
+    C->M = M;
+    C->N = P.N;
+    C->nnz = nnz;
+    C->val_type = out_vt;
+    C->max_row = -1;
+    return finish_matrix(C, rp, ci, v);
+}
+
+void free_dcsr_arrays(sp3mm_ctx* ctx, sp3mm_dcsr* m) {
+    if (!m) return;
+    if (m->row_ptr) cudaFreeAsync(m->row_ptr, ctx->stream);
+    if (m->col) cudaFreeAsync(m->col, ctx->stream);
+    if (m->val) cudaFreeAsync(m->val, ctx->stream);
+    m->row_ptr = nullptr;
+    m->col = nullptr;
+    m->val = nullptr;
+}
+
+int rap_impl(sp3mm_ctx* ctx, const sp3mm_dcsr& R, const sp3mm_dcsr& A, const sp3mm_dcsr& P,
+             int variant, int flavour, int out_vt, sp3mm_dcsr* C) {
+    if (variant == SP3MM_DIRECT) return direct_impl(ctx, R, A, P, flavour, out_vt, C);
+    sp3mm_dcsr T{};
+    int rc;
+    if (variant == SP3MM_PAIR) {
+        TRY(spmm_impl(ctx, R, A, flavour, SP3MM_F64, &T));
+        rc = spmm_impl(ctx, T, P, flavour, out_vt, C);
+    } else if (variant == SP3MM_PAIR_RIGHT) {
+        TRY(spmm_impl(ctx, A, P, flavour, SP3MM_F64, &T));
+        rc = spmm_impl(ctx, R, T, flavour, out_vt, C);
+    } else {
+        return set_error(ctx, SP3MM_EINVAL, "unknown variant %d", variant);
+    }
+    free_dcsr_arrays(ctx, &T);
+    return rc;
+}
+
+// Upload from 64-bit host arrays with index offset `off`.
+int upload_u64(sp3mm_ctx* ctx, long long M, long long N, long long nnz, const uint64_t* irp,
+               const uint64_t* ja, const double* as, int off, int vt, sp3mm_dcsr* out) {
+    if (M < 0 || N < 0 || nnz < 0) return set_error(ctx, SP3MM_EINVAL, "negative sizes");
+    if (M >= INT32_MAX || N >= INT32_MAX || nnz >= INT32_MAX)
+        return set_error(ctx, SP3MM_ELIMIT,
+                         "matrix %lldx%lld with %lld nonzeros exceeds the 32-bit device limits",
+                         M, N, nnz);
+    if (!irp || (nnz > 0 && (!ja || !as)))
+        return set_error(ctx, SP3MM_EINVAL, "NULL CSR arrays");
+    const cudaStream_t st = ctx->stream;
+    DevBuf rp, ci, v, stage, maxrow;
+    TRY(rp.alloc(ctx, sizeof(int) * (M + 1)));
+    TRY(ci.alloc(ctx, sizeof(int) * nnz));
+    TRY(v.alloc(ctx, vbytes(vt) * nnz));
+    TRY(maxrow.alloc(ctx, sizeof(int)));
+    TRY(stage.alloc(ctx, sizeof(uint64_t) * std::max(M + 1, nnz)));
+    CK(ctx, cudaMemsetAsync(maxrow.p, 0, sizeof(int), st));
+    CK(ctx, cudaMemcpyAsync(stage.p, irp, sizeof(uint64_t) * (M + 1), cudaMemcpyHostToDevice, st));
+    launch_narrow_rowptr(M, nnz, stage.as<unsigned long long>(), off, rp.as<int>(), ctx->d_err, st);
+    CK(ctx, cudaGetLastError());
+    TRY(check_device_err(ctx));
+    if (nnz > 0) {
+        CK(ctx, cudaMemcpyAsync(stage.p, ja, sizeof(uint64_t) * nnz, cudaMemcpyHostToDevice, st));
+        launch_narrow_cols(M, N, rp.as<int>(), stage.as<unsigned long long>(), off, ci.as<int>(),
+                           maxrow.as<int>(), ctx->d_err, st);
+        CK(ctx, cudaGetLastError());
+        if (vt == SP3MM_F64) {
+            CK(ctx, cudaMemcpyAsync(v.p, as, sizeof(double) * nnz, cudaMemcpyHostToDevice, st));
+        } else {
+            CK(ctx, cudaMemcpyAsync(stage.p, as, sizeof(double) * nnz, cudaMemcpyHostToDevice, st));
+            launch_convert_values(nnz, stage.p, SP3MM_F64, v.p, vt, st);
+        }
+    }
+    int mr = 0;
+    CK(ctx, cudaMemcpyAsync(&mr, maxrow.p, sizeof(int), cudaMemcpyDeviceToHost, st));
+    TRY(check_device_err(ctx));
+    out->M = static_cast<int>(M);
+    out->N = static_cast<int>(N);
+    out->nnz = nnz;
+    out->val_type = vt;
+    out->max_row = mr;
+    return finish_matrix(out, rp, ci, v);
+}
+
+// Copy a device CSR into malloc'd host arrays, indices shifted by `off`.
+int download_u64(sp3mm_ctx* ctx, const sp3mm_dcsr& m, int off, uint64_t* irp, uint64_t* ja,
+                 double* as) {
+    const cudaStream_t st = ctx->stream;
+    DevBuf stage;
+    TRY(stage.alloc(ctx, sizeof(uint64_t) * std::max<long long>(m.M + 1, m.nnz)));
+    launch_widen(m.M + 1, m.row_ptr, off, stage.as<unsigned long long>(), st);
+    CK(ctx, cudaMemcpyAsync(irp, stage.p, sizeof(uint64_t) * (m.M + 1), cudaMemcpyDeviceToHost, st));
+    if (m.nnz > 0) {
+        CK(ctx, cudaStreamSynchronize(st));
+        launch_widen(m.nnz, m.col, off, stage.as<unsigned long long>(), st);
+        CK(ctx, cudaMemcpyAsync(ja, stage.p, sizeof(uint64_t) * m.nnz, cudaMemcpyDeviceToHost, st));
+        if (m.val_type == SP3MM_F64) {
+            CK(ctx, cudaMemcpyAsync(as, m.val, sizeof(double) * m.nnz, cudaMemcpyDeviceToHost, st));
+        } else {
+            CK(ctx, cudaStreamSynchronize(st));
+            launch_convert_values(m.nnz, m.val, m.val_type, stage.p, SP3MM_F64, st);
+            CK(ctx, cudaMemcpyAsync(as, stage.p, sizeof(double) * m.nnz, cudaMemcpyDeviceToHost, st));
+        }
+    }
+    CK(ctx, cudaStreamSynchronize(st));
+    return SP3MM_OK;
+}
+
+int ctx_init(sp3mm_ctx* c, int device) {
+    c->device = device;
+    CK(c, cudaSetDevice(device));
+    cudaDeviceProp prop;
+    CK(c, cudaGetDeviceProperties(&prop, device));
+    if (prop.major < 10)
+        return set_error(c, SP3MM_ECUDA, "device %d (sm_%d%d) is not a Blackwell sm_100 GPU",
+                         device, prop.major, prop.minor);
+    c->num_sms = prop.multiProcessorCount;
+    CK(c, cudaStreamCreateWithFlags(&c->own_stream, cudaStreamNonBlocking));
+    c->stream = c->own_stream;
+    CK(c, cudaMalloc(&c->d_err, sizeof(unsigned)));
+    CK(c, cudaMemset(c->d_err, 0, sizeof(unsigned)));
+    CK(c, cudaEventCreate(&c->ev0));
+    CK(c, cudaEventCreate(&c->ev1));
+    // Keep freed pool memory cached between products.
+    cudaMemPool_t pool;
+    CK(c, cudaDeviceGetDefaultMemPool(&pool, device));
+    uint64_t thr = UINT64_MAX;
+    CK(c, cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &thr));
+    return SP3MM_OK;
+}
+
+// Per-thread default context of the reference-named entry points.
+thread_local sp3mm_ctx* tl_ctx = nullptr;
+
+sp3mm_ctx* default_ctx() {
+    if (tl_ctx) return tl_ctx;
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess) {
+        cudaGetLastError();
+        dev = 0;
+    }
+    sp3mm_ctx* c = new sp3mm_ctx();
+    if (ctx_init(c, dev) != SP3MM_OK) {
+        delete c;
+        return nullptr;
+    }
+    tl_ctx = c;
+    return c;
+}
+
+// ---- layer 1 helpers ------------------------------------------------------
+
+enum { F_NONE = -1 };
+
+int upload_spmat(sp3mm_ctx* ctx, const spmat* m, int off, sp3mm_dcsr* out) {
+    if (!m) return set_error(ctx, SP3MM_EINVAL, "NULL spmat");
+    return upload_u64(ctx, static_cast<long long>(m->M), static_cast<long long>(m->N),
+                      static_cast<long long>(m->NZ), reinterpret_cast<const uint64_t*>(m->IRP),
+                      reinterpret_cast<const uint64_t*>(m->JA), m->AS, off, SP3MM_F64, out);
+}
+
+spmat* download_spmat(sp3mm_ctx* ctx, const sp3mm_dcsr& m, int off) {
+    spmat* out = static_cast<spmat*>(calloc(1, sizeof(spmat)));
+    if (!out) {
+        fprintf(stderr, "sp3mm_b200: output spmat calloc failed\n");
+        return nullptr;
+    }
+    out->M = static_cast<idx_t>(m.M);
+    out->N = static_cast<idx_t>(m.N);
+    out->NZ = static_cast<idx_t>(m.nnz);
+    out->IRP = static_cast<idx_t*>(calloc(static_cast<size_t>(m.M) + 1, sizeof(idx_t)));
+    out->JA = static_cast<idx_t*>(malloc(sizeof(idx_t) * std::max<long long>(m.nnz, 1)));
+    out->AS = static_cast<double*>(malloc(sizeof(double) * std::max<long long>(m.nnz, 1)));
+    if (!out->IRP || !out->JA || !out->AS) {
+        fprintf(stderr, "sp3mm_b200: output spmat arrays allocation failed\n");
+        free(out->IRP);
+        free(out->JA);
+        free(out->AS);
+        free(out);
+        return nullptr;
+    }
+    if (download_u64(ctx, m, off, reinterpret_cast<uint64_t*>(out->IRP),
+                     reinterpret_cast<uint64_t*>(out->JA), out->AS) != SP3MM_OK) {
+        free(out->IRP);
+        free(out->JA);
+        free(out->AS);
+        free(out);
+        return nullptr;
+    }
+    return out;
+}
+
+typedef void (*chunks_fn)(unsigned long, spmat*, CONFIG*);
+
+// Device time of `body` in seconds (events on the context stream).
+template <typename F>
+int timed(sp3mm_ctx* ctx, double* secs, F&& body) {
+    Start = wall_seconds();
+    CK(ctx, cudaEventRecord(ctx->ev0, ctx->stream));
+    const int rc = body();
+    CK(ctx, cudaEventRecord(ctx->ev1, ctx->stream));
+    CK(ctx, cudaEventSynchronize(ctx->ev1));
+    End = wall_seconds();
+    float ms = 0.f;
+    cudaEventElapsedTime(&ms, ctx->ev0, ctx->ev1);
+    *secs = ms * 1e-3;
+    return rc;
+}
+
+struct Uploaded {
+    sp3mm_ctx* ctx;
+    std::vector<sp3mm_dcsr> mats;
+    ~Uploaded() {
+        for (auto& m : mats) free_dcsr_arrays(ctx, &m);
+    }
+};
+
+spmat* host_spmm(spmat* A, spmat* B, CONFIG* cfg, int off, int flavour) {
+    sp3mm_ctx* ctx = default_ctx();
+    if (!ctx) return nullptr;
+    if (!A || !B) {
+        set_error(ctx, SP3MM_EINVAL, "NULL matrix");
+        return nullptr;
+    }
+    Uploaded up{ctx, {}};
+    up.mats.resize(3);
+    if (upload_spmat(ctx, A, off, &up.mats[0]) || upload_spmat(ctx, B, off, &up.mats[1]))
+        return nullptr;
+    double secs = 0;
+    const int rc = timed(ctx, &secs, [&] {
+        return spmm_impl(ctx, up.mats[0], up.mats[1], flavour, SP3MM_F64, &up.mats[2]);
+    });
+    if (rc) return nullptr;
+    ElapsedInternal = secs;
+    spmat* out = download_spmat(ctx, up.mats[2], off);
+    if (out && cfg && cfg->chunkDistrbFunc)
+        reinterpret_cast<chunks_fn>(cfg->chunkDistrbFunc)(static_cast<unsigned long>(A->M), out,
+                                                          cfg);
+    return out;
+}
+
+spmat* host_sp3mm(spmat* R, spmat* AC, spmat* P, CONFIG* cfg, int off, int variant,
+                  int flavour) {
+    sp3mm_ctx* ctx = default_ctx();
+    if (!ctx) return nullptr;
+    if (!R || !AC || !P) {
+        set_error(ctx, SP3MM_EINVAL, "NULL matrix");
+        return nullptr;
+    }
+    Uploaded up{ctx, {}};
+    up.mats.resize(4);
+    if (upload_spmat(ctx, R, off, &up.mats[0]) || upload_spmat(ctx, AC, off, &up.mats[1]) ||
+        upload_spmat(ctx, P, off, &up.mats[2]))
+        return nullptr;
+    double secs = 0;
+    const int rc = timed(ctx, &secs, [&] {
+        return rap_impl(ctx, up.mats[0], up.mats[1], up.mats[2], variant, flavour, SP3MM_F64,
+                        &up.mats[3]);
+    });
+    if (rc) return nullptr;
+    ElapsedInternal = secs;
+    spmat* out = download_spmat(ctx, up.mats[3], off);
+    if (out && cfg && cfg->chunkDistrbFunc)
+        reinterpret_cast<chunks_fn>(cfg->chunkDistrbFunc)(static_cast<unsigned long>(R->M), out,
+                                                          cfg);
+    return out;
+}
+
+idx_t* host_rowsizes(spmat* A, spmat* B, int off, bool exact) {
+    sp3mm_ctx* ctx = default_ctx();
+    if (!ctx) return nullptr;
+    if (!A || !B) {
+        set_error(ctx, SP3MM_EINVAL, "NULL matrix");
+        return nullptr;
+    }
+    Uploaded up{ctx, {}};
+    up.mats.resize(2);
+    if (upload_spmat(ctx, A, off, &up.mats[0]) || upload_spmat(ctx, B, off, &up.mats[1]))
+        return nullptr;
+    const int M = up.mats[0].M;
+    DevBuf rows;
+    if (rows.alloc(ctx, sizeof(int) * (static_cast<size_t>(M) + 1))) return nullptr;
+    int64_t total = 0;
+    if (sp3mm_spmm_rowsizes(ctx, &up.mats[0], &up.mats[1], exact ? 1 : 0, rows.as<int32_t>(),
+                            &total))
+        return nullptr;
+    std::vector<int> h(static_cast<size_t>(M) + 1);
+    if (cudaMemcpyAsync(h.data(), rows.p, sizeof(int) * M, cudaMemcpyDeviceToHost,
+                        ctx->stream) != cudaSuccess ||
+        cudaStreamSynchronize(ctx->stream) != cudaSuccess) {
+        set_error(ctx, SP3MM_ECUDA, "row sizes readback failed");
+        return nullptr;
+    }
+    idx_t* out = static_cast<idx_t*>(calloc(static_cast<size_t>(M) + 1, sizeof(idx_t)));
+    if (!out) {
+        fprintf(stderr, "sp3mm_b200: row sizes calloc failed\n");
+        return nullptr;
+    }
+    for (int i = 0; i < M; ++i) out[i] = static_cast<idx_t>(h[i]);
+    out[M] = static_cast<idx_t>(total);
+    return out;
+}
+
+// SpMM entry points of this library and their flavours, to recognise the
+// `spmm` argument of the pair drivers.
+SPMM* const kUBFuncs[] = {&spmmSerial_0, &spmmRowByRow_0, &spmmRowByRow1DBlocks_0,
+                          &spmmRowByRow2DBlocks_0, &spmmRowByRow2DBlocksAllocated_0,
+                          &spmmSerial_1, &spmmRowByRow_1, &spmmRowByRow1DBlocks_1,
+                          &spmmRowByRow2DBlocks_1, &spmmRowByRow2DBlocksAllocated_1};
+SPMM* const kSNFuncs[] = {&spmmRowByRow_SymbNum_0, &spmmRowByRow1DBlocks_SymbNum_0,
+                          &spmmRowByRow2DBlocks_SymbNum_0,
+                          &spmmRowByRow2DBlocksAllocated_SymbNum_0, &spmmRowByRow_SymbNum_1,
+                          &spmmRowByRow1DBlocks_SymbNum_1, &spmmRowByRow2DBlocks_SymbNum_1,
+                          &spmmRowByRow2DBlocksAllocated_SymbNum_1};
+
+int flavour_of(SPMM_INTERF f) {
+    for (SPMM* g : kUBFuncs)
+        if (f == g) return SP3MM_UB;
+    for (SPMM* g : kSNFuncs)
+        if (f == g) return SP3MM_SYMBNUM;
+    return F_NONE;
+}
+
+// Pair driver: our SpMMs stay on the device; a foreign spmm is called on the
+// host matrices like the reference does (Sp3MM_CSR_OMP_UB_Generic.c:475-491).
+spmat* pair_driver(spmat* R, spmat* AC, spmat* P, CONFIG* cfg, SPMM_INTERF spmm, int off,
+                   int variant, int default_flavour) {
+    int fl = spmm ? flavour_of(spmm) : default_flavour;
+    if (fl != F_NONE) return host_sp3mm(R, AC, P, cfg, off, variant, fl);
+    const double t0 = wall_seconds();
+    spmat* T = variant == SP3MM_PAIR_RIGHT ? spmm(AC, P, cfg) : spmm(R, AC, cfg);
+    if (!T) return nullptr;
+    spmat* out = variant == SP3MM_PAIR_RIGHT ? spmm(R, T, cfg) : spmm(T, P, cfg);
+    free(T->AS);
+    free(T->JA);
+    free(T->IRP);
+    free(T);
+    ElapsedInternal = wall_seconds() - t0;
+    return out;
+}
+
+}  // namespace
+
+// ---------------------------------------------------------------------------
+// Layer 2 C ABI.
+extern "C" {
+
+int sp3mm_ctx_create(int device, sp3mm_ctx** out) {
+    if (!out) return SP3MM_EINVAL;
+    sp3mm_ctx* c = new sp3mm_ctx();
+    const int rc = ctx_init(c, device);
+    if (rc) {
+        delete c;
+        return rc;
+    }
+    *out = c;
+    return SP3MM_OK;
+}
+
+int sp3mm_ctx_destroy(sp3mm_ctx* ctx) {
+    if (!ctx) return SP3MM_EINVAL;
+    cudaSetDevice(ctx->device);
+    cudaStreamSynchronize(ctx->stream);
+    if (ctx->d_err) cudaFree(ctx->d_err);
+    if (ctx->ev0) cudaEventDestroy(ctx->ev0);
+    if (ctx->ev1) cudaEventDestroy(ctx->ev1);
+    if (ctx->own_stream) cudaStreamDestroy(ctx->own_stream);
+    if (tl_ctx == ctx) tl_ctx = nullptr;
+    delete ctx;
+    return SP3MM_OK;
+}
+
+int sp3mm_ctx_set_stream(sp3mm_ctx* ctx, void* stream) {
+    if (!ctx) return SP3MM_EINVAL;
+    ctx->stream = stream ? static_cast<cudaStream_t>(stream) : ctx->own_stream;
+    return SP3MM_OK;
+}
+
+void* sp3mm_ctx_stream(sp3mm_ctx* ctx) { return ctx ? static_cast<void*>(ctx->stream) : nullptr; }
+
+int sp3mm_ctx_set_workspace_limit(sp3mm_ctx* ctx, size_t bytes) {
+    if (!ctx) return SP3MM_EINVAL;
+    ctx->ws_limit = bytes;
+    return SP3MM_OK;
+}
+
+int sp3mm_ctx_trim(sp3mm_ctx* ctx) {
+    if (!ctx) return SP3MM_EINVAL;
+    CK(ctx, cudaStreamSynchronize(ctx->stream));
+    cudaMemPool_t pool;
+    CK(ctx, cudaDeviceGetDefaultMemPool(&pool, ctx->device));
+    CK(ctx, cudaMemPoolTrimTo(pool, 0));
+    return SP3MM_OK;
+}
+
+const char* sp3mm_ctx_last_error(sp3mm_ctx* ctx) { return ctx ? ctx->last_error.c_str() : ""; }
+
+uint64_t sp3mm_ctx_launches(sp3mm_ctx* ctx) {
+    (void)ctx;
+    return launch_count();
+}
+
+int sp3mm_ctx_sync(sp3mm_ctx* ctx) {
+    if (!ctx) return SP3MM_EINVAL;
+    CK(ctx, cudaStreamSynchronize(ctx->stream));
+    return SP3MM_OK;
+}
+
+int sp3mm_ctx_set_profiling(sp3mm_ctx* ctx, int on) {
+    if (!ctx) return SP3MM_EINVAL;
+    CK(ctx, cudaStreamSynchronize(ctx->stream));
+    prof_clear(ctx);
+    ctx->profiling = on != 0;
+    return SP3MM_OK;
+}
+
+int sp3mm_ctx_profile_report(sp3mm_ctx* ctx, char* buf, size_t len) {
+    if (!ctx || !buf || len == 0) return SP3MM_EINVAL;
+    CK(ctx, cudaStreamSynchronize(ctx->stream));
+    struct Agg {
+        std::string label;
+        int count;
+        double total_ms, max_ms;
+    };
+    std::vector<Agg> agg;
+    for (auto& r : ctx->prof) {
+        float ms = 0.f;
+        CK(ctx, cudaEventElapsedTime(&ms, r.a, r.b));
+        auto it = std::find_if(agg.begin(), agg.end(),
+                               [&](const Agg& a) { return a.label == r.label; });
+        if (it == agg.end()) {
+            agg.push_back({r.label, 1, ms, ms});
+        } else {
+            it->count++;
+            it->total_ms += ms;
+            it->max_ms = std::max(it->max_ms, static_cast<double>(ms));
+        }
+    }
+    std::string out;
+    char line[160];
+    for (auto& a : agg) {
+        snprintf(line, sizeof line, "%s %d %.6f %.6f\n", a.label.c_str(), a.count, a.total_ms,
+                 a.max_ms);
+        out += line;
+    }
+    snprintf(buf, len, "%s", out.c_str());
+    return out.size() < len ? SP3MM_OK : SP3MM_EINVAL;
+}
+
+int sp3mm_dcsr_upload(sp3mm_ctx* ctx, const spmat* host, int off_f, int val_type,
+                      sp3mm_dcsr* out) {
+    if (!ctx || !host || !out || (off_f != 0 && off_f != 1)) return SP3MM_EINVAL;
+    return upload_u64(ctx, static_cast<long long>(host->M), static_cast<long long>(host->N),
+                      static_cast<long long>(host->NZ),
+                      reinterpret_cast<const uint64_t*>(host->IRP),
+                      reinterpret_cast<const uint64_t*>(host->JA), host->AS, off_f, val_type, out);
+}
+
+int sp3mm_dcsr_upload_arrays(sp3mm_ctx* ctx, int64_t M, int64_t N, int64_t nnz,
+                             const int64_t* row_ptr, const int64_t* col, const double* val,
+                             int val_type, sp3mm_dcsr* out) {
+    if (!ctx || !out) return SP3MM_EINVAL;
+    return upload_u64(ctx, M, N, nnz, reinterpret_cast<const uint64_t*>(row_ptr),
+                      reinterpret_cast<const uint64_t*>(col), val, 0, val_type, out);
+}
+
+int sp3mm_dcsr_download(sp3mm_ctx* ctx, const sp3mm_dcsr* m, int off_f, spmat** out) {
+    if (!ctx || !out) return SP3MM_EINVAL;
+    TRY(check_dcsr(ctx, m, "matrix"));
+    *out = download_spmat(ctx, *m, off_f);
+    return *out ? SP3MM_OK : SP3MM_ECUDA;
+}
+
+int sp3mm_dcsr_download_arrays(sp3mm_ctx* ctx, const sp3mm_dcsr* m, int64_t* row_ptr,
+                               int64_t* col, double* val) {
+    if (!ctx || !row_ptr) return SP3MM_EINVAL;
+    TRY(check_dcsr(ctx, m, "matrix"));
+    return download_u64(ctx, *m, 0, reinterpret_cast<uint64_t*>(row_ptr),
+                        reinterpret_cast<uint64_t*>(col), val);
+}
+
+int sp3mm_dcsr_free(sp3mm_ctx* ctx, sp3mm_dcsr* m) {
+    if (!ctx || !m) return SP3MM_EINVAL;
+    free_dcsr_arrays(ctx, m);
+    m->nnz = 0;
+    return SP3MM_OK;
+}
+
+int sp3mm_spmm(sp3mm_ctx* ctx, const sp3mm_dcsr* A, const sp3mm_dcsr* B, int flavour,
+               int out_val_type, sp3mm_dcsr* C) {
+    if (!ctx || !C) return SP3MM_EINVAL;
+    TRY(check_dcsr(ctx, A, "A"));
+    TRY(check_dcsr(ctx, B, "B"));
+    return spmm_impl(ctx, *A, *B, flavour, out_val_type, C);
+}
+
+int sp3mm_rap(sp3mm_ctx* ctx, const sp3mm_dcsr* R, const sp3mm_dcsr* A, const sp3mm_dcsr* P,
+              int variant, int flavour, int out_val_type, sp3mm_dcsr* C) {
+    if (!ctx || !C) return SP3MM_EINVAL;
+    TRY(check_dcsr(ctx, R, "R"));
+    TRY(check_dcsr(ctx, A, "A"));
+    TRY(check_dcsr(ctx, P, "P"));
+    return rap_impl(ctx, *R, *A, *P, variant, flavour, out_val_type, C);
+}
+
+int sp3mm_spmm_rowsizes(sp3mm_ctx* ctx, const sp3mm_dcsr* A, const sp3mm_dcsr* B, int exact,
+                        int32_t* rows_dev, int64_t* total) {
+    if (!ctx) return SP3MM_EINVAL;
+    TRY(check_dcsr(ctx, A, "A"));
+    TRY(check_dcsr(ctx, B, "B"));
+    if (A->N != B->M) return set_error(ctx, SP3MM_EINVAL, "inner dimensions differ");
+    const int M = A->M;
+    const cudaStream_t st = ctx->stream;
+    DevBuf cnt_buf, need, row_cnt;
+    TRY(cnt_buf.alloc(ctx, sizeof(Counters)));
+    TRY(need.alloc(ctx, sizeof(int) * (static_cast<size_t>(M) + 1)));
+    Counters* dc = cnt_buf.as<Counters>();
+    CK(ctx, cudaMemsetAsync(dc, 0, sizeof(Counters), st));
+    if (!exact) {
+        // The upper bound proper is the per-row flop count, without the
+        // distinct-column clamp the binning uses.
+        sp3mm_dcsr Bfull = *B;
+        Bfull.N = INT32_MAX;
+        launch_pair_bounds(view(*A), view(Bfull), rows_dev ? rows_dev : need.as<int>(),
+                           &dc->total, st);
+        CK(ctx, cudaGetLastError());
+        Counters h{};
+        CK(ctx, cudaMemcpyAsync(&h, dc, sizeof h, cudaMemcpyDeviceToHost, st));
+        CK(ctx, cudaStreamSynchronize(st));
+        if (total) *total = static_cast<int64_t>(h.total);
+        return SP3MM_OK;
+    }
+    TRY(row_cnt.alloc(ctx, sizeof(int) * (static_cast<size_t>(M) + 1)));
+    launch_pair_bounds(view(*A), view(*B), need.as<int>(), &dc->total, st);
+    Bins bins;
+    TRY(bin_rows(ctx, M, need.as<int>(), dc, row_cnt.as<int>(), bins));
+    PairArgs pa{};
+    pa.A = view(*A);
+    pa.B = view(*B);
+    pa.row_cnt = row_cnt.as<int>();
+    pa.err = ctx->d_err;
+    const int G = choose_group(B->M ? static_cast<double>(B->nnz) / B->M : 1.0);
+    TRY(run_levels(ctx, bins, false, kSymb, G, [&](const LevelPlan& pl, const RowSet& rs, int grid) {
+        launch_pair_rows(pa, kSymb, pl, rs, grid, st);
+    }));
+    DevBuf rp;
+    long long nnz = 0;
+    TRY(scan_counts(ctx, M, row_cnt.as<int>(), rp, &nnz));
+    TRY(check_device_err(ctx));
+    if (rows_dev)
+        CK(ctx, cudaMemcpyAsync(rows_dev, row_cnt.p, sizeof(int) * M, cudaMemcpyDeviceToDevice, st));
+    CK(ctx, cudaStreamSynchronize(st));
+    if (total) *total = nnz;
+    return SP3MM_OK;
+}
+
+int sp3mm_transpose(sp3mm_ctx* ctx, const sp3mm_dcsr* A, sp3mm_dcsr* AT) {
+    if (!ctx || !AT) return SP3MM_EINVAL;
+    TRY(check_dcsr(ctx, A, "A"));
+    const cudaStream_t st = ctx->stream;
+    DevBuf rp, ci, v, counts, cursor;
+    TRY(counts.alloc(ctx, sizeof(int) * (static_cast<size_t>(A->N) + 1)));
+    TRY(cursor.alloc(ctx, sizeof(int) * (static_cast<size_t>(A->N) + 1)));
+    CK(ctx, cudaMemsetAsync(counts.p, 0, sizeof(int) * (static_cast<size_t>(A->N) + 1), st));
+    CK(ctx, cudaMemsetAsync(cursor.p, 0, sizeof(int) * (static_cast<size_t>(A->N) + 1), st));
+    launch_col_counts(A->nnz, A->col, counts.as<int>(), st);
+    long long nnz = 0;
+    TRY(scan_counts(ctx, A->N, counts.as<int>(), rp, &nnz));
+    TRY(ci.alloc(ctx, sizeof(int) * static_cast<size_t>(A->nnz)));
+    TRY(v.alloc(ctx, vbytes(A->val_type) * static_cast<size_t>(A->nnz)));
+    launch_transpose_scatter(view(*A), rp.as<int>(), cursor.as<int>(), ci.as<int>(), v.p, st);
+    // Longest transposed row = largest column count.
+    DevBuf mr;
+    TRY(mr.alloc(ctx, sizeof(int)));
+    CK(ctx, cudaMemsetAsync(mr.p, 0, sizeof(int), st));
+    launch_validate_i32(A->N, A->M, rp.as<int>(), ci.as<int>(), mr.as<int>(), ctx->d_err, st);
+    int max_row = 0;
+    CK(ctx, cudaMemcpyAsync(&max_row, mr.p, sizeof(int), cudaMemcpyDeviceToHost, st));
+    CK(ctx, cudaStreamSynchronize(st));
+    // The scatter order within a row is arbitrary: sort, then re-validate.
+    CK(ctx, cudaMemsetAsync(ctx->d_err, 0, sizeof(unsigned), st));
+    launch_sort_rows(A->N, rp.as<int>(), ci.as<int>(), v.p, A->val_type, max_row, st);
+    CK(ctx, cudaMemsetAsync(mr.p, 0, sizeof(int), st));
+    launch_validate_i32(A->N, A->M, rp.as<int>(), ci.as<int>(), mr.as<int>(), ctx->d_err, st);
+    TRY(check_device_err(ctx));
+    AT->M = A->N;
+    AT->N = A->M;
+    AT->nnz = A->nnz;
+    AT->val_type = A->val_type;
+    AT->max_row = max_row;
+    return finish_matrix(AT, rp, ci, v);
+}
+
+int sp3mm_rap_memory_estimate(const sp3mm_dcsr* R, const sp3mm_dcsr* A, const sp3mm_dcsr* P,
+                              int variant, int flavour, size_t* bytes) {
+    if (!R || !A || !P || !bytes) return SP3MM_EINVAL;
+    auto mr = [](const sp3mm_dcsr* m) -> double {
+        return m->max_row >= 0 ? m->max_row : (m->M ? static_cast<double>(m->N) : 0.0);
+    };
+    // Multiply-add bounds: nnz(X) * longest row of the right operand.
+    const double f_ra = R->nnz * mr(A);
+    const double f_rap = f_ra * mr(P);
+    const double f_ap = A->nnz * mr(P);
+    double b = 0;
+    const double row_ws = 32.0;   // per-row work arrays (need, level, lists, counts, offsets)
+    auto spmm_bytes = [&](double M, double flops) {
+        double s = M * row_ws + std::min(flops, 1e15) * 12.0 * (flavour == SP3MM_UB ? 2 : 1);
+        return s;
+    };
+    if (variant == SP3MM_DIRECT) {
+        b = spmm_bytes(R->M, f_rap);
+    } else if (variant == SP3MM_PAIR) {
+        b = spmm_bytes(R->M, f_ra) + f_ra * 12.0 + spmm_bytes(R->M, f_ra * mr(P));
+    } else {
+        b = spmm_bytes(A->M, f_ap) + f_ap * 12.0 + spmm_bytes(R->M, R->nnz * std::min(f_ap, 1e15));
+    }
+    b += 64.0 * 1024 * 1024;   // global-table scratch and scan temporaries
+    *bytes = static_cast<size_t>(std::min(b, 1.8e19));
+    return SP3MM_OK;
+}
+
+// ---------------------------------------------------------------------------
+// Layer 1: reference entry points.
+
+#define SP3MM_REF_SPMM(name, off, flav) \
+    spmat* name(spmat* A, spmat* B, CONFIG* cfg) { return host_spmm(A, B, cfg, off, flav); }
+
+SP3MM_REF_SPMM(spmmSerial_0, 0, SP3MM_UB)
+SP3MM_REF_SPMM(spmmSerial_1, 1, SP3MM_UB)
+SP3MM_REF_SPMM(spmmRowByRow_0, 0, SP3MM_UB)
+SP3MM_REF_SPMM(spmmRowByRow_1, 1, SP3MM_UB)
+SP3MM_REF_SPMM(spmmRowByRow1DBlocks_0, 0, SP3MM_UB)
+SP3MM_REF_SPMM(spmmRowByRow1DBlocks_1, 1, SP3MM_UB)
+SP3MM_REF_SPMM(spmmRowByRow2DBlocks_0, 0, SP3MM_UB)
+SP3MM_REF_SPMM(spmmRowByRow2DBlocks_1, 1, SP3MM_UB)
+SP3MM_REF_SPMM(spmmRowByRow2DBlocksAllocated_0, 0, SP3MM_UB)
+SP3MM_REF_SPMM(spmmRowByRow2DBlocksAllocated_1, 1, SP3MM_UB)
+SP3MM_REF_SPMM(spmmRowByRow_SymbNum_0, 0, SP3MM_SYMBNUM)
+SP3MM_REF_SPMM(spmmRowByRow_SymbNum_1, 1, SP3MM_SYMBNUM)
+SP3MM_REF_SPMM(spmmRowByRow1DBlocks_SymbNum_0, 0, SP3MM_SYMBNUM)
+SP3MM_REF_SPMM(spmmRowByRow1DBlocks_SymbNum_1, 1, SP3MM_SYMBNUM)
+SP3MM_REF_SPMM(spmmRowByRow2DBlocks_SymbNum_0, 0, SP3MM_SYMBNUM)
+SP3MM_REF_SPMM(spmmRowByRow2DBlocks_SymbNum_1, 1, SP3MM_SYMBNUM)
+SP3MM_REF_SPMM(spmmRowByRow2DBlocksAllocated_SymbNum_0, 0, SP3MM_SYMBNUM)
+SP3MM_REF_SPMM(spmmRowByRow2DBlocksAllocated_SymbNum_1, 1, SP3MM_SYMBNUM)
+
+spmat* sp3mmRowByRowPair_0(spmat* R, spmat* AC, spmat* P, CONFIG* cfg, SPMM_INTERF spmm) {
+    return pair_driver(R, AC, P, cfg, spmm ? spmm : &spmmRowByRow2DBlocks_0, 0, SP3MM_PAIR,
+                       SP3MM_UB);
+}
+spmat* sp3mmRowByRowPair_1(spmat* R, spmat* AC, spmat* P, CONFIG* cfg, SPMM_INTERF spmm) {
+    return pair_driver(R, AC, P, cfg, spmm ? spmm : &spmmRowByRow2DBlocks_1, 1, SP3MM_PAIR,
+                       SP3MM_UB);
+}
+spmat* sp3mmRowByRowPair_SymbNum_0(spmat* R, spmat* AC, spmat* P, CONFIG* cfg,
+                                   SPMM_INTERF spmm) {
+    return pair_driver(R, AC, P, cfg, spmm ? spmm : &spmmRowByRow_SymbNum_0, 0, SP3MM_PAIR,
+                       SP3MM_SYMBNUM);
+}
+spmat* sp3mmRowByRowPair_SymbNum_1(spmat* R, spmat* AC, spmat* P, CONFIG* cfg,
+                                   SPMM_INTERF spmm) {
+    return pair_driver(R, AC, P, cfg, spmm ? spmm : &spmmRowByRow_SymbNum_1, 1, SP3MM_PAIR,
+                       SP3MM_SYMBNUM);
+}
+spmat* sp3mmRowByRowPairRight_0(spmat* R, spmat* AC, spmat* P, CONFIG* cfg, SPMM_INTERF spmm) {
+    return pair_driver(R, AC, P, cfg, spmm, 0, SP3MM_PAIR_RIGHT, SP3MM_UB);
+}
+spmat* sp3mmRowByRowPairRight_1(spmat* R, spmat* AC, spmat* P, CONFIG* cfg, SPMM_INTERF spmm) {
+    return pair_driver(R, AC, P, cfg, spmm, 1, SP3MM_PAIR_RIGHT, SP3MM_UB);
+}
+spmat* sp3mmRowByRowMerged_0(spmat* R, spmat* AC, spmat* P, CONFIG* cfg, SPMM_INTERF spmm) {
+    (void)spmm;
+    return host_sp3mm(R, AC, P, cfg, 0, SP3MM_DIRECT, SP3MM_UB);
+}
+spmat* sp3mmRowByRowMerged_1(spmat* R, spmat* AC, spmat* P, CONFIG* cfg, SPMM_INTERF spmm) {
+    (void)spmm;
+    return host_sp3mm(R, AC, P, cfg, 1, SP3MM_DIRECT, SP3MM_UB);
+}
+spmat* sp3mmRowByRowMerged_SymbNum_0(spmat* R, spmat* AC, spmat* P, CONFIG* cfg,
+                                     SPMM_INTERF spmm) {
+    (void)spmm;
+    return host_sp3mm(R, AC, P, cfg, 0, SP3MM_DIRECT, SP3MM_SYMBNUM);
+}
+spmat* sp3mmRowByRowMerged_SymbNum_1(spmat* R, spmat* AC, spmat* P, CONFIG* cfg,
+                                     SPMM_INTERF spmm) {
+    (void)spmm;
+    return host_sp3mm(R, AC, P, cfg, 1, SP3MM_DIRECT, SP3MM_SYMBNUM);
+}
+
+idx_t* SpMM_Symb___0(ROW_MMSYM_IMPL_MODE mode, spmat* a, spmat* b) {
+    (void)mode;
+    return host_rowsizes(a, b, 0, true);
+}
+idx_t* SpMM_Symb___1(ROW_MMSYM_IMPL_MODE mode, spmat* a, spmat* b) {
+    (void)mode;
+    return host_rowsizes(a, b, 1, true);
+}
+idx_t* spMMSizeUpperbound_0(spmat* A, spmat* B) { return host_rowsizes(A, B, 0, false); }
+idx_t* spMMSizeUpperbound_1(spmat* A, spmat* B) { return host_rowsizes(A, B, 1, false); }
+
+static idx_t* colparts_ub(spmat* A, spmat* B, unsigned short gridCols, idx_t* offs, int off) {
+    sp3mm_ctx* ctx = default_ctx();
+    if (!ctx) return nullptr;
+    if (!A || !B || !offs || gridCols == 0) {
+        set_error(ctx, SP3MM_EINVAL, "invalid column-partition arguments");
+        return nullptr;
+    }
+    Uploaded up{ctx, {}};
+    up.mats.resize(2);
+    if (upload_spmat(ctx, A, off, &up.mats[0]) || upload_spmat(ctx, B, off, &up.mats[1]))
+        return nullptr;
+    const size_t parts = static_cast<size_t>(A->M) * gridCols;
+    const size_t noff = static_cast<size_t>(B->M) * gridCols + 1;
+    DevBuf d_off, d_out, d_tot;
+    if (d_off.alloc(ctx, sizeof(long long) * noff) || d_out.alloc(ctx, sizeof(long long) * (parts + 1)) ||
+        d_tot.alloc(ctx, sizeof(unsigned long long)))
+        return nullptr;
+    idx_t* out = static_cast<idx_t*>(calloc(parts + 1, sizeof(idx_t)));
+    if (!out) {
+        fprintf(stderr, "sp3mm_b200: colparts calloc failed\n");
+        return nullptr;
+    }
+    unsigned long long tot = 0;
+    if (cudaMemcpyAsync(d_off.p, offs, sizeof(long long) * noff, cudaMemcpyHostToDevice,
+                        ctx->stream) != cudaSuccess ||
+        cudaMemsetAsync(d_tot.p, 0, sizeof(unsigned long long), ctx->stream) != cudaSuccess) {
+        free(out);
+        set_error(ctx, SP3MM_ECUDA, "colparts upload failed");
+        return nullptr;
+    }
+    launch_colparts_ub(view(up.mats[0]), view(up.mats[1]), gridCols, d_off.as<long long>(), off,
+                       d_out.as<long long>(), d_tot.as<unsigned long long>(), ctx->stream);
+    if (cudaMemcpyAsync(out, d_out.p, sizeof(long long) * parts, cudaMemcpyDeviceToHost,
+                        ctx->stream) != cudaSuccess ||
+        cudaMemcpyAsync(&tot, d_tot.p, sizeof tot, cudaMemcpyDeviceToHost, ctx->stream) !=
+            cudaSuccess ||
+        cudaStreamSynchronize(ctx->stream) != cudaSuccess) {
+        free(out);
+        set_error(ctx, SP3MM_ECUDA, "colparts readback failed");
+        return nullptr;
+    }
+    out[parts] = static_cast<idx_t>(tot);
+    return out;
+}
+
+idx_t* spMMSizeUpperboundColParts_0(spmat* A, spmat* B, unsigned short gridCols, idx_t* o) {
+    return colparts_ub(A, B, gridCols, o, 0);
+}
+idx_t* spMMSizeUpperboundColParts_1(spmat* A, spmat* B, unsigned short gridCols, idx_t* o) {
+    return colparts_ub(A, B, gridCols, o, 1);
+}
+
+}  // extern "C"
