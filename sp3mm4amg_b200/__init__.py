@@ -213,6 +213,11 @@ class Context:
     def launches(self) -> int:
         return int(self.lib.sp3mm_ctx_launches(self.h))
 
+    def set_tuning(self, lanes_per_row: int = 0, d1: int = -1, d2: int = -1) -> None:
+        """Row-kernel tuning (lanes per row, table-size shifts); results never
+        depend on it -- rows whose tables overflow are recomputed."""
+        self._check(self.lib.sp3mm_ctx_set_tuning(self.h, lanes_per_row, d1, d2))
+
     def set_profiling(self, on: bool) -> None:
         """Time every kernel launch with CUDA events on the context stream."""
         self._check(self.lib.sp3mm_ctx_set_profiling(self.h, 1 if on else 0))

@@ -33,6 +33,7 @@ DEVICE_API = {
     "sp3mm_ctx_last_error": (_c.c_char_p, [_c.c_void_p]),
     "sp3mm_ctx_launches": (_c.c_uint64, [_c.c_void_p]),
     "sp3mm_ctx_sync": (_c.c_int, [_c.c_void_p]),
+    "sp3mm_ctx_set_tuning": (_c.c_int, [_c.c_void_p, _c.c_int, _c.c_int, _c.c_int]),
     "sp3mm_ctx_set_profiling": (_c.c_int, [_c.c_void_p, _c.c_int]),
     "sp3mm_ctx_profile_report": (_c.c_int, [_c.c_void_p, _c.c_char_p, _c.c_size_t]),
     "sp3mm_dcsr_upload": (_c.c_int, [_c.c_void_p, SPMAT_P, _c.c_int, _c.c_int, _c.c_void_p]),

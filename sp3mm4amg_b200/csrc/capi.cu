@@ -33,6 +33,10 @@ struct sp3mm_ctx {
     unsigned* d_err = nullptr;           // sticky device error word
     size_t ws_limit = 0;
     size_t smem_budget = 110 * 1024;
+    // Row-kernel tuning: lanes per row (0: from the operands' mean row
+    // length), table-size shifts d1 (first table from bound >> d1; < 0:
+    // default) and d2 (direct second table = first >> d2).
+    int tune_G = 0, tune_d1 = -1, tune_d2 = -1;
     std::string last_error;
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
     // Optional per-launch timing (events on the context stream).
@@ -153,18 +157,17 @@ int check_dcsr(sp3mm_ctx* ctx, const sp3mm_dcsr* m, const char* what) {
 struct Counters {
     int counts[kLevels + 1];
     int cursors[kLevels];
-    int gmax;
-    int pad;
+    int nmax;
+    int retry_count;
     unsigned long long total;
-    unsigned err;
-    unsigned pad2;
+    unsigned long long cursor;
 };
 
 // Row lists by level, built from per-row `need`.
 struct Bins {
     int counts[kLevels + 1] = {};
     int offsets[kLevels] = {};
-    int gmax = 0;
+    int nmax = 0;
     unsigned long long total = 0;
     DevBuf level, lists;
 };
@@ -187,15 +190,16 @@ int check_device_err(sp3mm_ctx* ctx) {
     return SP3MM_OK;
 }
 
-// Bin M rows by `need`; `dcnt` receives the device counters (total is
-// accumulated there by the bounds kernel beforehand); row_cnt of empty rows
-// is zeroed.
-int bin_rows(sp3mm_ctx* ctx, int M, const int* need, Counters* dcnt, int* row_cnt, Bins& b) {
+// Bin M rows by need[i] >> shift for groups of G lanes; `dcnt` is the
+// device counter block (its `total` was accumulated by the bounds kernel);
+// row_cnt of empty rows is zeroed when given.
+int bin_rows(sp3mm_ctx* ctx, int M, const int* need, int shift, int G, Counters* dcnt,
+             int* row_cnt, Bins& b) {
     TRY(b.level.alloc(ctx, static_cast<size_t>(M) + 1));
     TRY(b.lists.alloc(ctx, sizeof(int) * (static_cast<size_t>(M) + 1)));
     prof(ctx, "bin.levels", [&] {
-        launch_bin_levels(M, need, b.level.as<signed char>(), dcnt->counts, &dcnt->gmax,
-                          row_cnt, ctx->stream);
+        launch_bin_levels(M, need, shift, G, b.level.as<signed char>(), dcnt->counts,
+                          &dcnt->nmax, row_cnt, ctx->stream);
     });
     Counters h{};
     CK(ctx, cudaMemcpyAsync(&h, dcnt, sizeof h, cudaMemcpyDeviceToHost, ctx->stream));
@@ -208,7 +212,7 @@ int bin_rows(sp3mm_ctx* ctx, int M, const int* need, Counters* dcnt, int* row_cn
         off += h.counts[L];
     }
     b.counts[kLevels] = h.counts[kLevels];
-    b.gmax = h.gmax;
+    b.nmax = h.nmax;
     b.total = h.total;
     CK(ctx, cudaMemcpyAsync(dcnt->cursors, h.cursors, sizeof h.cursors, cudaMemcpyHostToDevice,
                             ctx->stream));
@@ -219,65 +223,111 @@ int bin_rows(sp3mm_ctx* ctx, int M, const int* need, Counters* dcnt, int* row_cn
     return SP3MM_OK;
 }
 
-// Run one row kernel family over every non-empty level.
-template <typename Launch>
-int run_levels(sp3mm_ctx* ctx, const Bins& b, bool direct, int mode, int G, Launch&& launch) {
-    for (int L = 0; L < kLevels; ++L) {
-        const int n = b.counts[L];
-        if (!n) continue;
-        LevelPlan pl = plan_level(L, direct, mode, G, ctx->smem_budget);
-        RowSet rs{};
-        rs.rows = b.lists.as<int>() + b.offsets[L];
-        rs.nrows = n;
-        DevBuf gtab;
-        int grid;
-        if (L == kGlobalLevel) pl.slots = static_cast<int>(slots_for(b.gmax));
-        if (!pl.global) {
-            const int gpc = pl.groups_per_cta;
-            grid = (n + gpc - 1) / gpc;
-            const int cap = ctx->num_sms * 8;
-            if (grid > cap) grid = cap;
+// Lanes per row from the right operand's mean row length (or the tuning).
+int pick_group(const sp3mm_ctx* ctx, double mean) {
+    if (ctx->tune_G) return ctx->tune_G;
+    if (mean <= 4.0) return 4;
+    if (mean <= 8.0) return 8;
+    if (mean <= 16.0) return 16;
+    return 32;
+}
+
+// One row-kernel family over a set of rows: shared-memory tables when they
+// fit the CTA budget, global-memory tables otherwise.
+struct RowRunner {
+    sp3mm_ctx* ctx;
+    bool direct;
+    int mode;
+    DirectRowArgs da;
+    PairRowArgs pa;
+
+    int launch(RowParams p, int G, DevBuf& gtab) {
+        const size_t per_group = row_table_bytes(direct, mode, p.S1, p.S2);
+        const int gpw = 32 / G;
+        int warps = static_cast<int>(ctx->smem_budget / (per_group * gpw));
+        if (warps > 8) warps = 8;
+        RowGeom geo{};
+        geo.G = G;
+        if (warps >= 1) {
+            geo.block = 32 * warps;
+            geo.smem = per_group * gpw * warps;
+            const int gpc = gpw * warps;
+            long long grid = (p.nrows + gpc - 1) / gpc;
+            const long long cap = static_cast<long long>(ctx->num_sms) * 16;
+            geo.grid = static_cast<int>(grid < cap ? grid : cap);
+            p.gtab = nullptr;
         } else {
-            // Tables in global memory: one region per group; bound the number
-            // of concurrent groups by a 2 GiB scratch budget.
-            const size_t stride = static_cast<size_t>(bytes_per_slot(direct, mode)) * pl.slots;
-            size_t groups = static_cast<size_t>(n);
-            const size_t cap_groups = static_cast<size_t>(ctx->num_sms) * 8;
-            if (groups > cap_groups) groups = cap_groups;
+            // Tables in global memory, one warp per row; concurrency bounded
+            // by a 2 GiB scratch budget.
+            geo.G = G = 32;
+            const size_t stride = row_table_bytes(direct, mode, p.S1, p.S2);
+            size_t groups = static_cast<size_t>(p.nrows);
+            const size_t cap = static_cast<size_t>(ctx->num_sms) * 8;
+            if (groups > cap) groups = cap;
             const size_t budget = size_t(2) << 30;
             while (groups > 1 && groups * stride > budget) groups >>= 1;
-            groups = (groups + pl.groups_per_cta - 1) / pl.groups_per_cta * pl.groups_per_cta;
+            groups = (groups + 7) / 8 * 8;
             TRY(gtab.alloc(ctx, groups * stride));
-            rs.gtab = gtab.as<unsigned char>();
-            rs.gtab_stride = static_cast<long long>(stride);
-            grid = static_cast<int>(groups / pl.groups_per_cta);
+            p.gtab = gtab.as<unsigned char>();
+            p.gstride = static_cast<long long>(stride);
+            geo.block = 256;
+            geo.smem = 0;
+            geo.grid = static_cast<int>(groups / 8);
         }
-        rs.slots = pl.slots;
-        rs.shift = 32 - ilog2_pow2(static_cast<unsigned>(pl.slots));
         static const char* const kLabels[2][3] = {
             {"pair.rows.symb", "pair.rows.num", "pair.rows.book"},
             {"direct.rows.symb", "direct.rows.num", "direct.rows.book"}};
-        prof(ctx, kLabels[direct ? 1 : 0][mode], [&] { launch(pl, rs, grid); });
-        CK(ctx, cudaGetLastError());
+        cudaError_t e = cudaSuccess;
+        prof(ctx, kLabels[direct ? 1 : 0][mode], [&] {
+            e = direct ? launch_direct_rows(da, p, mode, geo, ctx->stream)
+                       : launch_pair_rows(pa, p, mode, geo, ctx->stream);
+        });
+        if (e != cudaSuccess)
+            return set_error(ctx, SP3MM_ECUDA, "row kernel launch failed: %s",
+                             cudaGetErrorString(e));
+        return SP3MM_OK;
     }
-    return SP3MM_OK;
-}
 
-int alloc_matrix(sp3mm_ctx* ctx, int M, int N, long long nnz, int vt, sp3mm_dcsr* C,
-                 DevBuf& rp, DevBuf& ci, DevBuf& v) {
-    TRY(rp.alloc(ctx, sizeof(int) * (static_cast<size_t>(M) + 1)));
-    TRY(ci.alloc(ctx, sizeof(int) * static_cast<size_t>(nnz)));
-    TRY(v.alloc(ctx, vbytes(vt) * static_cast<size_t>(nnz)));
-    C->M = M;
-    C->N = N;
-    C->nnz = nnz;
-    C->row_ptr = rp.as<int>();
-    C->col = ci.as<int>();
-    C->val = v.p;
-    C->val_type = vt;
-    C->max_row = -1;
-    return SP3MM_OK;
-}
+    // Every level of `bins` with optimistic tables (S1 from the level, S2 =
+    // S1 >> d2), then one retry launch for rows that overflowed, with tables
+    // sized from the bounds s1_max / s2_max.
+    int run(const Bins& bins, RowParams base, int G, int d2, long long s1_max, long long s2_max,
+            Counters* dcnt) {
+        DevBuf retry;
+        TRY(retry.alloc(ctx, sizeof(int) * (static_cast<size_t>(base.nrows) + 1)));
+        CK(ctx, cudaMemsetAsync(&dcnt->retry_count, 0, sizeof(int), ctx->stream));
+        for (int L = 0; L < kLevels; ++L) {
+            if (!bins.counts[L]) continue;
+            RowParams p = base;
+            p.rows = bins.lists.as<int>() + bins.offsets[L];
+            p.nrows = bins.counts[L];
+            p.S1 = 32 << L;
+            p.S2 = direct ? std::max(32, p.S1 >> d2) : 0;
+            p.retry_rows = retry.as<int>();
+            p.retry_count = &dcnt->retry_count;
+            DevBuf gtab;
+            TRY(launch(p, G, gtab));
+        }
+        int nretry = 0;
+        CK(ctx, cudaMemcpyAsync(&nretry, &dcnt->retry_count, sizeof(int), cudaMemcpyDeviceToHost,
+                                ctx->stream));
+        CK(ctx, cudaStreamSynchronize(ctx->stream));
+        if (nretry > 0) {
+            RowParams p = base;
+            p.rows = retry.as<int>();
+            p.nrows = nretry;
+            p.S1 = slots_for_need(s1_max, 32);
+            p.S2 = direct ? slots_for_need(s2_max, 32) : 0;
+            // The direct kernel sorts the C row in the first table's storage.
+            if (p.S1 < p.S2) p.S1 = p.S2;
+            p.retry_rows = nullptr;
+            p.retry_count = nullptr;
+            DevBuf gtab;
+            TRY(launch(p, 32, gtab));
+        }
+        return SP3MM_OK;
+    }
+};
 
 int finish_matrix(sp3mm_dcsr* C, DevBuf& rp, DevBuf& ci, DevBuf& v) {
     C->row_ptr = static_cast<int*>(rp.detach());
@@ -286,7 +336,7 @@ int finish_matrix(sp3mm_dcsr* C, DevBuf& rp, DevBuf& ci, DevBuf& v) {
     return SP3MM_OK;
 }
 
-// Scan row counts into a fresh C; returns the total (checks the int32 limit).
+// Scan row counts into a fresh row_ptr; returns the total.
 int scan_counts(sp3mm_ctx* ctx, int M, const int* row_cnt, DevBuf& rp, long long* total) {
     TRY(rp.alloc(ctx, sizeof(int) * (static_cast<size_t>(M) + 1)));
     DevBuf tmp;
@@ -302,6 +352,89 @@ int scan_counts(sp3mm_ctx* ctx, int M, const int* row_cnt, DevBuf& rp, long long
     return SP3MM_OK;
 }
 
+// The shared tail of every product: symbolic + exact numeric, or booked
+// numeric + compaction.  `need` holds the first table's distinct-key bound
+// per row; s1_max/s2_max bound the tables of the retry launch.
+int product_rows(sp3mm_ctx* ctx, RowRunner& rr, int M, int N, int flavour, int out_vt,
+                 DevBuf& need, Counters* dc, int G, int d1, int d2, long long s1_bound,
+                 long long s2_bound, double p_max_row, sp3mm_dcsr* C) {
+    const cudaStream_t st = ctx->stream;
+    DevBuf row_cnt, row_cnt1, rp, ci, v;
+    TRY(row_cnt.alloc(ctx, sizeof(int) * (static_cast<size_t>(M) + 1)));
+    Bins bins;
+    TRY(bin_rows(ctx, M, need.as<int>(), d1, G, dc, row_cnt.as<int>(), bins));
+    const long long s1_max = std::min<long long>(bins.nmax, s1_bound);
+    const long long s2_max = std::min<long long>(
+        static_cast<long long>(static_cast<double>(bins.nmax) * p_max_row), s2_bound);
+
+    RowParams p{};
+    p.nrows = M;
+    p.row_cnt = row_cnt.as<int>();
+    p.err = ctx->d_err;
+    p.c_vt = out_vt;
+    long long nnz = 0;
+    if (flavour == SP3MM_SYMBNUM) {
+        if (rr.direct) {
+            TRY(row_cnt1.alloc(ctx, sizeof(int) * (static_cast<size_t>(M) + 1)));
+            CK(ctx, cudaMemsetAsync(row_cnt1.p, 0, sizeof(int) * (static_cast<size_t>(M) + 1), st));
+            p.row_cnt1 = row_cnt1.as<int>();
+        }
+        rr.mode = kSymb;
+        TRY(rr.run(bins, p, G, d2, s1_max, s2_max, dc));
+        TRY(scan_counts(ctx, M, row_cnt.as<int>(), rp, &nnz));
+        TRY(check_device_err(ctx));
+        if (nnz < 0 || nnz >= INT32_MAX)
+            return set_error(ctx, SP3MM_ELIMIT, "result has too many nonzeros");
+        TRY(ci.alloc(ctx, sizeof(int) * static_cast<size_t>(nnz)));
+        TRY(v.alloc(ctx, vbytes(out_vt) * static_cast<size_t>(nnz)));
+        // Exact sizes: re-bin by max(C row, R*A row) distinct counts.
+        CK(ctx, cudaMemsetAsync(dc, 0, sizeof(Counters), st));
+        prof(ctx, "need", [&] {
+            launch_need_from_counts(M, row_cnt.as<int>(), rr.direct ? row_cnt1.as<int>() : nullptr,
+                                    need.as<int>(), st);
+        });
+        Bins nb;
+        TRY(bin_rows(ctx, M, need.as<int>(), 0, G, dc, nullptr, nb));
+        p.row_cnt1 = nullptr;
+        p.c_rp = rp.as<int>();
+        p.c_ci = ci.as<int>();
+        p.c_v = v.p;
+        rr.mode = kNumExact;
+        TRY(rr.run(nb, p, G, 0, s1_max, s2_max, dc));
+    } else {
+        const unsigned long long cap = bins.total;
+        DevBuf ub_ci, ub_v, row_off;
+        TRY(ub_ci.alloc(ctx, sizeof(int) * cap));
+        TRY(ub_v.alloc(ctx, vbytes(out_vt) * cap));
+        TRY(row_off.alloc(ctx, sizeof(long long) * (static_cast<size_t>(M) + 1)));
+        CK(ctx, cudaMemsetAsync(&dc->cursor, 0, sizeof(unsigned long long), st));
+        p.cursor = &dc->cursor;
+        p.cap = cap;
+        p.row_off = row_off.as<long long>();
+        p.ub_ci = ub_ci.as<int>();
+        p.ub_v = ub_v.p;
+        rr.mode = kNumBook;
+        TRY(rr.run(bins, p, G, d2, s1_max, s2_max, dc));
+        TRY(scan_counts(ctx, M, row_cnt.as<int>(), rp, &nnz));
+        TRY(check_device_err(ctx));
+        if (nnz < 0 || nnz >= INT32_MAX)
+            return set_error(ctx, SP3MM_ELIMIT, "result has too many nonzeros");
+        TRY(ci.alloc(ctx, sizeof(int) * static_cast<size_t>(nnz)));
+        TRY(v.alloc(ctx, vbytes(out_vt) * static_cast<size_t>(nnz)));
+        prof(ctx, "compact", [&] {
+            launch_compact(M, row_cnt.as<int>(), row_off.as<long long>(), ub_ci.as<int>(), ub_v.p,
+                           rp.as<int>(), ci.as<int>(), v.p, out_vt, st);
+        });
+    }
+    TRY(check_device_err(ctx));
+    C->M = M;
+    C->N = N;
+    C->nnz = nnz;
+    C->val_type = out_vt;
+    C->max_row = -1;
+    return finish_matrix(C, rp, ci, v);
+}
+
 // ---------------------------------------------------------------------------
 // C = A*B.
 int spmm_impl(sp3mm_ctx* ctx, const sp3mm_dcsr& A, const sp3mm_dcsr& B, int flavour, int out_vt,
@@ -310,82 +443,18 @@ int spmm_impl(sp3mm_ctx* ctx, const sp3mm_dcsr& A, const sp3mm_dcsr& B, int flav
         return set_error(ctx, SP3MM_EINVAL, "inner dimensions differ (%d vs %d)", A.N, B.M);
     const int M = A.M;
     const cudaStream_t st = ctx->stream;
-    const CsrView a = view(A), bv = view(B);
-    const int G = choose_group(B.M ? static_cast<double>(B.nnz) / B.M : 1.0);
-
-    DevBuf cnt_buf, need, row_cnt;
+    const int G = pick_group(ctx, B.M ? static_cast<double>(B.nnz) / B.M : 1.0);
+    const int d1 = ctx->tune_d1 >= 0 ? ctx->tune_d1 : 2;
+    DevBuf cnt_buf, need;
     TRY(cnt_buf.alloc(ctx, sizeof(Counters)));
     TRY(need.alloc(ctx, sizeof(int) * (static_cast<size_t>(M) + 1)));
-    TRY(row_cnt.alloc(ctx, sizeof(int) * (static_cast<size_t>(M) + 1)));
     Counters* dc = cnt_buf.as<Counters>();
     CK(ctx, cudaMemsetAsync(dc, 0, sizeof(Counters), st));
-    prof(ctx, "pair.bounds", [&] { launch_pair_bounds(a, bv, need.as<int>(), &dc->total, st); });
-    Bins bins;
-    TRY(bin_rows(ctx, M, need.as<int>(), dc, row_cnt.as<int>(), bins));
-
-    PairArgs pa{};
-    pa.A = a;
-    pa.B = bv;
-    pa.row_cnt = row_cnt.as<int>();
-    pa.err = ctx->d_err;
-    pa.c_vtype = out_vt;
-
-    DevBuf rp, ci, v;
-    long long nnz = 0;
-    if (flavour == SP3MM_SYMBNUM) {
-        TRY(run_levels(ctx, bins, false, kSymb, G, [&](const LevelPlan& pl, const RowSet& rs, int grid) {
-            launch_pair_rows(pa, kSymb, pl, rs, grid, st);
-        }));
-        TRY(scan_counts(ctx, M, row_cnt.as<int>(), rp, &nnz));
-        TRY(check_device_err(ctx));
-        if (nnz < 0 || nnz >= INT32_MAX)
-            return set_error(ctx, SP3MM_ELIMIT, "result has too many nonzeros");
-        TRY(ci.alloc(ctx, sizeof(int) * static_cast<size_t>(nnz)));
-        TRY(v.alloc(ctx, vbytes(out_vt) * static_cast<size_t>(nnz)));
-        // Re-bin by exact sizes: tighter tables for the numeric pass.
-        CK(ctx, cudaMemsetAsync(dc, 0, sizeof(Counters), st));
-        launch_need_from_counts(M, row_cnt.as<int>(), nullptr, need.as<int>(), st);
-        Bins nb;
-        TRY(bin_rows(ctx, M, need.as<int>(), dc, nullptr, nb));
-        pa.c_rp = rp.as<int>();
-        pa.c_ci = ci.as<int>();
-        pa.c_v = v.p;
-        TRY(run_levels(ctx, nb, false, kNumExact, G, [&](const LevelPlan& pl, const RowSet& rs, int grid) {
-            launch_pair_rows(pa, kNumExact, pl, rs, grid, st);
-        }));
-    } else {
-        const unsigned long long cap = bins.total;
-        DevBuf ub_ci, ub_v, row_off;
-        TRY(ub_ci.alloc(ctx, sizeof(int) * cap));
-        TRY(ub_v.alloc(ctx, vbytes(out_vt) * cap));
-        TRY(row_off.alloc(ctx, sizeof(long long) * (static_cast<size_t>(M) + 1)));
-        pa.book_cursor = &dc->total;   // reuse: reset below
-        CK(ctx, cudaMemsetAsync(&dc->total, 0, sizeof(unsigned long long), st));
-        pa.book_cap = cap;
-        pa.row_off = row_off.as<long long>();
-        pa.ub_ci = ub_ci.as<int>();
-        pa.ub_v = ub_v.p;
-        TRY(run_levels(ctx, bins, false, kNumBook, G, [&](const LevelPlan& pl, const RowSet& rs, int grid) {
-            launch_pair_rows(pa, kNumBook, pl, rs, grid, st);
-        }));
-        TRY(scan_counts(ctx, M, row_cnt.as<int>(), rp, &nnz));
-        TRY(check_device_err(ctx));
-        if (nnz < 0 || nnz >= INT32_MAX)
-            return set_error(ctx, SP3MM_ELIMIT, "result has too many nonzeros");
-        TRY(ci.alloc(ctx, sizeof(int) * static_cast<size_t>(nnz)));
-        TRY(v.alloc(ctx, vbytes(out_vt) * static_cast<size_t>(nnz)));
-        prof(ctx, "compact", [&] {
-            launch_compact(M, row_cnt.as<int>(), row_off.as<long long>(), ub_ci.as<int>(),
-                           ub_v.p, rp.as<int>(), ci.as<int>(), v.p, out_vt, st);
-        });
-    }
-    TRY(check_device_err(ctx));
-    C->M = M;
-    C->N = B.N;
-    C->nnz = nnz;
-    C->val_type = out_vt;
-    C->max_row = -1;
-    return finish_matrix(C, rp, ci, v);
+    prof(ctx, "pair.bounds", [&] {
+        launch_pair_bounds(view(A), view(B), need.as<int>(), &dc->total, st);
+    });
+    RowRunner rr{ctx, false, kSymb, {}, PairRowArgs{view(A), view(B)}};
+    return product_rows(ctx, rr, M, B.N, flavour, out_vt, need, dc, G, d1, 0, B.N, 0, 0.0, C);
 }
 
 // C = R*A*P, direct (row forwarding).
@@ -397,87 +466,21 @@ int direct_impl(sp3mm_ctx* ctx, const sp3mm_dcsr& R, const sp3mm_dcsr& A, const 
     const cudaStream_t st = ctx->stream;
     const double mean = std::max(A.M ? static_cast<double>(A.nnz) / A.M : 1.0,
                                  P.M ? static_cast<double>(P.nnz) / P.M : 1.0);
-    const int G = choose_group(mean);
-
-    DevBuf cnt_buf, need, row_cnt, row_cnt1;
+    const int G = pick_group(ctx, mean);
+    const int d1 = ctx->tune_d1 >= 0 ? ctx->tune_d1 : 1;
+    const int d2 = ctx->tune_d2 >= 0 ? ctx->tune_d2 : 1;
+    const int pmax = P.max_row >= 0 ? P.max_row : P.N;
+    DevBuf cnt_buf, need;
     TRY(cnt_buf.alloc(ctx, sizeof(Counters)));
     TRY(need.alloc(ctx, sizeof(int) * (static_cast<size_t>(M) + 1)));
-    TRY(row_cnt.alloc(ctx, sizeof(int) * (static_cast<size_t>(M) + 1)));
     Counters* dc = cnt_buf.as<Counters>();
     CK(ctx, cudaMemsetAsync(dc, 0, sizeof(Counters), st));
     prof(ctx, "direct.bounds", [&] {
-        launch_direct_bounds(view(R), view(A), view(P), need.as<int>(), &dc->total, st);
+        launch_direct_bounds(view(R), view(A), pmax, need.as<int>(), &dc->total, st);
     });
-    Bins bins;
-    TRY(bin_rows(ctx, M, need.as<int>(), dc, row_cnt.as<int>(), bins));
-
-    DirectArgs da{};
-    da.R = view(R);
-    da.A = view(A);
-    da.P = view(P);
-    da.row_cnt = row_cnt.as<int>();
-    da.err = ctx->d_err;
-    da.c_vtype = out_vt;
-
-    DevBuf rp, ci, v;
-    long long nnz = 0;
-    if (flavour == SP3MM_SYMBNUM) {
-        TRY(row_cnt1.alloc(ctx, sizeof(int) * (static_cast<size_t>(M) + 1)));
-        CK(ctx, cudaMemsetAsync(row_cnt1.p, 0, sizeof(int) * (static_cast<size_t>(M) + 1), st));
-        da.row_cnt1 = row_cnt1.as<int>();
-        TRY(run_levels(ctx, bins, true, kSymb, G, [&](const LevelPlan& pl, const RowSet& rs, int grid) {
-            launch_direct_rows(da, kSymb, pl, rs, grid, st);
-        }));
-        TRY(scan_counts(ctx, M, row_cnt.as<int>(), rp, &nnz));
-        TRY(check_device_err(ctx));
-        if (nnz < 0 || nnz >= INT32_MAX)
-            return set_error(ctx, SP3MM_ELIMIT, "result has too many nonzeros");
-        TRY(ci.alloc(ctx, sizeof(int) * static_cast<size_t>(nnz)));
-        TRY(v.alloc(ctx, vbytes(out_vt) * static_cast<size_t>(nnz)));
-        CK(ctx, cudaMemsetAsync(dc, 0, sizeof(Counters), st));
-        launch_need_from_counts(M, row_cnt.as<int>(), row_cnt1.as<int>(), need.as<int>(), st);
-        Bins nb;
-        TRY(bin_rows(ctx, M, need.as<int>(), dc, nullptr, nb));
-        da.row_cnt1 = nullptr;
-        da.c_rp = rp.as<int>();
-        da.c_ci = ci.as<int>();
-        da.c_v = v.p;
-        TRY(run_levels(ctx, nb, true, kNumExact, G, [&](const LevelPlan& pl, const RowSet& rs, int grid) {
-            launch_direct_rows(da, kNumExact, pl, rs, grid, st);
-        }));
-    } else {
-        const unsigned long long cap = bins.total;
-        DevBuf ub_ci, ub_v, row_off;
-        TRY(ub_ci.alloc(ctx, sizeof(int) * cap));
-        TRY(ub_v.alloc(ctx, vbytes(out_vt) * cap));
-        TRY(row_off.alloc(ctx, sizeof(long long) * (static_cast<size_t>(M) + 1)));
-        CK(ctx, cudaMemsetAsync(&dc->total, 0, sizeof(unsigned long long), st));
-        da.book_cursor = &dc->total;
-        da.book_cap = cap;
-        da.row_off = row_off.as<long long>();
-        da.ub_ci = ub_ci.as<int>();
-        da.ub_v = ub_v.p;
-        TRY(run_levels(ctx, bins, true, kNumBook, G, [&](const LevelPlan& pl, const RowSet& rs, int grid) {
-            launch_direct_rows(da, kNumBook, pl, rs, grid, st);
-        }));
-        TRY(scan_counts(ctx, M, row_cnt.as<int>(), rp, &nnz));
-        TRY(check_device_err(ctx));
-        if (nnz < 0 || nnz >= INT32_MAX)
-            return set_error(ctx, SP3MM_ELIMIT, "result has too many nonzeros");
-        TRY(ci.alloc(ctx, sizeof(int) * static_cast<size_t>(nnz)));
-        TRY(v.alloc(ctx, vbytes(out_vt) * static_cast<size_t>(nnz)));
-        prof(ctx, "compact", [&] {
-            launch_compact(M, row_cnt.as<int>(), row_off.as<long long>(), ub_ci.as<int>(),
-                           ub_v.p, rp.as<int>(), ci.as<int>(), v.p, out_vt, st);
-        });
-    }
-    TRY(check_device_err(ctx));
-    C->M = M;
-    C->N = P.N;
-    C->nnz = nnz;
-    C->val_type = out_vt;
-    C->max_row = -1;
-    return finish_matrix(C, rp, ci, v);
+    RowRunner rr{ctx, true, kSymb, DirectRowArgs{view(R), view(A), view(P)}, {}};
+    return product_rows(ctx, rr, M, P.N, flavour, out_vt, need, dc, G, d1, d2, A.N, P.N,
+                        static_cast<double>(pmax), C);
 }
 
 void free_dcsr_arrays(sp3mm_ctx* ctx, sp3mm_dcsr* m) {
@@ -877,6 +880,18 @@ int sp3mm_ctx_sync(sp3mm_ctx* ctx) {
     return SP3MM_OK;
 }
 
+int sp3mm_ctx_set_tuning(sp3mm_ctx* ctx, int lanes_per_row, int d1, int d2) {
+    if (!ctx) return SP3MM_EINVAL;
+    if (lanes_per_row != 0 && lanes_per_row != 4 && lanes_per_row != 8 && lanes_per_row != 16 &&
+        lanes_per_row != 32)
+        return set_error(ctx, SP3MM_EINVAL, "lanes per row must be 0, 4, 8, 16 or 32");
+    if (d1 > 16 || d2 > 16) return set_error(ctx, SP3MM_EINVAL, "table shifts must be <= 16");
+    ctx->tune_G = lanes_per_row;
+    ctx->tune_d1 = d1;
+    ctx->tune_d2 = d2;
+    return SP3MM_OK;
+}
+
 int sp3mm_ctx_set_profiling(sp3mm_ctx* ctx, int on) {
     if (!ctx) return SP3MM_EINVAL;
     CK(ctx, cudaStreamSynchronize(ctx->stream));
@@ -1003,17 +1018,16 @@ int sp3mm_spmm_rowsizes(sp3mm_ctx* ctx, const sp3mm_dcsr* A, const sp3mm_dcsr* B
     }
     TRY(row_cnt.alloc(ctx, sizeof(int) * (static_cast<size_t>(M) + 1)));
     launch_pair_bounds(view(*A), view(*B), need.as<int>(), &dc->total, st);
+    const int G = pick_group(ctx, B->M ? static_cast<double>(B->nnz) / B->M : 1.0);
+    const int d1 = ctx->tune_d1 >= 0 ? ctx->tune_d1 : 2;
     Bins bins;
-    TRY(bin_rows(ctx, M, need.as<int>(), dc, row_cnt.as<int>(), bins));
-    PairArgs pa{};
-    pa.A = view(*A);
-    pa.B = view(*B);
-    pa.row_cnt = row_cnt.as<int>();
-    pa.err = ctx->d_err;
-    const int G = choose_group(B->M ? static_cast<double>(B->nnz) / B->M : 1.0);
-    TRY(run_levels(ctx, bins, false, kSymb, G, [&](const LevelPlan& pl, const RowSet& rs, int grid) {
-        launch_pair_rows(pa, kSymb, pl, rs, grid, st);
-    }));
+    TRY(bin_rows(ctx, M, need.as<int>(), d1, G, dc, row_cnt.as<int>(), bins));
+    RowRunner rr{ctx, false, kSymb, {}, PairRowArgs{view(*A), view(*B)}};
+    RowParams p{};
+    p.nrows = M;
+    p.row_cnt = row_cnt.as<int>();
+    p.err = ctx->d_err;
+    TRY(rr.run(bins, p, G, 0, std::min<long long>(bins.nmax, B->N), 0, dc));
     DevBuf rp;
     long long nnz = 0;
     TRY(scan_counts(ctx, M, row_cnt.as<int>(), rp, &nnz));
@@ -1199,8 +1213,8 @@ static idx_t* colparts_ub(spmat* A, spmat* B, unsigned short gridCols, idx_t* of
         set_error(ctx, SP3MM_ECUDA, "colparts upload failed");
         return nullptr;
     }
-    launch_colparts_ub(view(up.mats[0]), view(up.mats[1]), gridCols, d_off.as<long long>(), off,
-                       d_out.as<long long>(), d_tot.as<unsigned long long>(), ctx->stream);
+    launch_colparts_ub(view(up.mats[0]), gridCols, d_off.as<long long>(), d_out.as<long long>(),
+                       d_tot.as<unsigned long long>(), ctx->stream);
     if (cudaMemcpyAsync(out, d_out.p, sizeof(long long) * parts, cudaMemcpyDeviceToHost,
                         ctx->stream) != cudaSuccess ||
         cudaMemcpyAsync(&tot, d_tot.p, sizeof tot, cudaMemcpyDeviceToHost, ctx->stream) !=

@@ -1,38 +1,15 @@
-// kernels.cu -- sm_100a kernels of the Sp3MM triple product.
+// kernels.cu -- bounds, binning, scans, compaction, conversions and
+// transpose kernels of the Sp3MM library (sm_100a).  The per-row
+// accumulation kernels are in rows.cu.
 //
-// Gustavson row-by-row products on ordered CSR, re-designed for the GPU:
-//
-//  * Row binning by upper-bound size.  A bounds kernel computes, per output
-//    row, the number of multiply-adds (the reference's upper bound,
-//    code/src/include/SpMMUtilsGeneric.h:112-139, extended to R*A*P for the
-//    direct product) and the number of table slots the row can need.  Rows
-//    are binned into table-size levels (32 .. 4096 slots in shared memory,
-//    larger in global memory) by a count / scatter pair of kernels.  This
-//    replaces the reference's OpenMP 1D / 2D row and column partitions
-//    (code/src/Sp3MM_CSR_OMP_UB_Generic.c:85-105, :153-182, :216-302).
-//
-//  * Per-row accumulators: a group of G lanes (G = 4..32, picked from the
-//    right operand's mean row length) owns one row and one open-addressing
-//    hash table.  This replaces the dense accumulator + index bitmap
-//    (code/src/include/sparseMatrix.h:60-110) and the RB-tree
-//    (code/src/Sp3MM_CSR_OMP_SymbStep_Generic.c:84-161).
-//
-//  * Reference summation order without value atomics: the lanes walk the
-//    left row's entries one step at a time, and within a step they cover the
-//    selected right row, whose column indices are distinct, so no two lanes
-//    touch the same slot.  Each output entry therefore receives its
-//    contributions in ascending left-row position, as in the reference's
-//    scSparseVectMul_ loop (code/src/include/SpMMUtilsGeneric.h:39-55), and
-//    the values are bit-identical to the reference's.
-//
-//  * First-touch order for the direct product: new keys of a step are
-//    ranked by ballot + popc in lane order, which is the order in which the
-//    reference's bitmap appends them to nnzIdx; the R*A row is then forwarded
-//    into P in that order (code/src/Sp3MM_CSR_OMP_UB_Generic.c:542-545).
-//
-//  * Sorted write-out: the row's keys are compacted and sorted (rank sort
-//    for short rows, bitonic sort for long rows), replacing the per-row
-//    qsort of sparsifyDirect (code/src/include/SpMMUtilsGeneric.h:230-241).
+//  * Row binning by upper-bound size replaces the reference's OpenMP 1D / 2D
+//    row and column partitions (code/src/Sp3MM_CSR_OMP_UB_Generic.c:85-105,
+//    :153-182, :216-302): a bounds kernel gives each output row the number of
+//    distinct keys its first table can receive (the reference's upper bound,
+//    code/src/include/SpMMUtilsGeneric.h:112-139), and rows are grouped into
+//    table-size levels by a count / scatter pair of kernels.
+//  * The upper-bound flavour's merge (code/src/include/SpMMUtilsGeneric.h:
+//    364-403) becomes a scan of the booked row lengths and a compaction kernel.
 #include <cub/device/device_scan.cuh>
 
 #include <atomic>
@@ -45,10 +22,8 @@ namespace sp3mm {
 
 static std::atomic<uint64_t> g_launches{0};
 uint64_t launch_count() { return g_launches.load(); }
-static inline void counted() { g_launches.fetch_add(1, std::memory_order_relaxed); }
+void note_launch() { g_launches.fetch_add(1, std::memory_order_relaxed); }
 
-// ---------------------------------------------------------------------------
-// Value access in either storage type (uniform branch per launch).
 __device__ __forceinline__ double load_val(const void* p, int vt, long long i) {
     if (vt == SP3MM_F32) return static_cast<double>(__ldg(static_cast<const float*>(p) + i));
     return __ldg(static_cast<const double*>(p) + i);
@@ -61,8 +36,7 @@ __device__ __forceinline__ void store_val(void* p, int vt, long long i, double v
 // ---------------------------------------------------------------------------
 // Bounds.
 
-// need[i] = slots bound of row i of A*B (distinct keys <= min(flops, N)),
-// total_flops += flops.
+// need[i] = min(flops_i, B.N) with flops_i = sum_{k in A(i)} len(B(k)).
 template <int G>
 __global__ void __launch_bounds__(256) k_pair_bounds(CsrView A, CsrView B, int* need,
                                                       unsigned long long* total) {
@@ -83,41 +57,33 @@ __global__ void __launch_bounds__(256) k_pair_bounds(CsrView A, CsrView B, int* 
             mine += static_cast<unsigned long long>(f);
         }
     }
-    // Every lane reaches this point: one atomic per warp.
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) mine += __shfl_xor_sync(0xffffffffu, mine, o);
     if ((threadIdx.x & 31) == 0 && mine) atomicAdd(total, mine);
 }
 
-// Direct R*A*P: need[i] = max(distinct bound of the R*A row, of the C row);
-// total_flops += sum_{k in R(i)} sum_{c in A(k)} len(P(c)).
+// Direct R*A*P: need[i] = min(u1_i, A.N) with u1_i = sum_{k in R(i)} len(A(k))
+// (the R*A row's products); total += u1_i * p_max_row, a bound on the C row's
+// multiply-adds (each R*A entry forwards one P row of at most p_max_row
+// entries).
 template <int G>
-__global__ void __launch_bounds__(256) k_direct_bounds(CsrView R, CsrView A, CsrView P,
+__global__ void __launch_bounds__(256) k_direct_bounds(CsrView R, CsrView A, int p_max_row,
                                                         int* need, unsigned long long* total) {
     const Group<G> g;
     const int groups = (gridDim.x * blockDim.x) / G;
     unsigned long long mine = 0;
     for (int row = (blockIdx.x * blockDim.x + threadIdx.x) / G; row < R.M; row += groups) {
         const int rb = __ldg(R.rp + row), re = __ldg(R.rp + row + 1);
-        long long u1 = 0, u2 = 0;
+        long long u1 = 0;
         for (int t = rb + g.gl; t < re; t += G) {
             const int k = __ldg(R.ci + t);
-            const int ab = __ldg(A.rp + k), ae = __ldg(A.rp + k + 1);
-            u1 += ae - ab;
-            for (int i = ab; i < ae; ++i) {
-                const int c = __ldg(A.ci + i);
-                u2 += __ldg(P.rp + c + 1) - __ldg(P.rp + c);
-            }
+            u1 += __ldg(A.rp + k + 1) - __ldg(A.rp + k);
         }
         u1 = g.sum64(u1);
-        u2 = g.sum64(u2);
         if (g.gl == 0) {
-            const long long d1 = u1 < A.N ? u1 : A.N;
-            const long long d2 = u2 < P.N ? u2 : P.N;
-            const long long d = d1 > d2 ? d1 : d2;
-            // A row that forwards nothing needs no table.
-            need[row] = u2 == 0 ? 0 : static_cast<int>(d < INT_MAX ? d : INT_MAX);
-            mine += static_cast<unsigned long long>(u2);
+            const long long d = u1 < A.N ? u1 : A.N;
+            need[row] = static_cast<int>(d < INT_MAX ? d : INT_MAX);
+            mine += static_cast<unsigned long long>(u1) * static_cast<unsigned long long>(p_max_row);
         }
     }
 #pragma unroll
@@ -136,37 +102,52 @@ __global__ void k_need_from_counts(int M, const int* cnt, const int* cnt1, int* 
 // ---------------------------------------------------------------------------
 // Binning by table-size level.
 
-__host__ __device__ __forceinline__ int level_of(int need) {
-    if (need <= 0) return -1;   // empty output row
-    long long want = static_cast<long long>(need) + need / 4 + 1;
-    int lg = kMinLogSlots;
-    while ((1ll << lg) < want) ++lg;
-    const int L = lg - kMinLogSlots;
-    return L < kSharedLevels ? L : kGlobalLevel;
+__host__ __device__ __forceinline__ int limit_of(long long S, int G) {
+    const long long a = S - G - 1, b = (7 * S) / 8;
+    return static_cast<int>(a < b ? a : b);
 }
 
-__global__ void __launch_bounds__(256) k_bin_levels(int M, const int* need, signed char* level,
-                                                     int* counts, int* gmax, int* row_cnt_zero) {
+__host__ __device__ __forceinline__ int level_of(long long need, int G) {
+    if (need <= 0) return -1;
+    int L = 0;
+    while (L < kLevels - 1 && limit_of(32ll << L, G) < need) ++L;
+    return L;
+}
+
+int slots_for_need(long long need, int G) {
+    const int L = level_of(need < 1 ? 1 : need, G);
+    return 32 << L;
+}
+int level_for_need(long long need, int G) { return level_of(need, G); }
+
+__global__ void __launch_bounds__(256) k_bin_levels(int M, const int* need, int shift, int G,
+                                                     signed char* level, int* counts,
+                                                     int* nmax, int* row_cnt_zero) {
     __shared__ int sc[kLevels + 1];
     __shared__ int smax;
-    if (threadIdx.x <= kLevels) sc[threadIdx.x] = 0;
+    for (int i = threadIdx.x; i <= kLevels; i += blockDim.x) sc[i] = 0;
     if (threadIdx.x == 0) smax = 0;
     __syncthreads();
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < M; i += gridDim.x * blockDim.x) {
         const int n = need[i];
-        const int L = level_of(n);
+        int L = -1;
+        if (n > 0) {
+            const int s = n >> shift;
+            L = level_of(s > 0 ? s : 1, G);
+        }
         level[i] = static_cast<signed char>(L);
         if (L < 0) {
             atomicAdd(&sc[kLevels], 1);
             if (row_cnt_zero) row_cnt_zero[i] = 0;
         } else {
             atomicAdd(&sc[L], 1);
-            if (L == kGlobalLevel) atomicMax(&smax, n);
+            atomicMax(&smax, n);
         }
     }
     __syncthreads();
-    if (threadIdx.x <= kLevels && sc[threadIdx.x]) atomicAdd(counts + threadIdx.x, sc[threadIdx.x]);
-    if (threadIdx.x == 0 && smax) atomicMax(gmax, smax);
+    for (int i = threadIdx.x; i <= kLevels; i += blockDim.x)
+        if (sc[i]) atomicAdd(counts + i, sc[i]);
+    if (threadIdx.x == 0 && smax) atomicMax(nmax, smax);
 }
 
 // Append every row to its level's list (cursors hold each list's start).
@@ -175,7 +156,7 @@ __global__ void __launch_bounds__(256) k_bin_scatter(int M, const signed char* l
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     const bool in = i < M;
     const int L = in ? level[i] : -1;
-    // Warp-aggregated append keeps rows of a warp contiguous and ascending.
+    // Warp-aggregated append keeps the rows of a warp contiguous and ascending.
     const unsigned act = __ballot_sync(0xffffffffu, in && L >= 0);
     if (!(in && L >= 0)) return;
     const unsigned peers = __match_any_sync(act, L);
@@ -188,333 +169,19 @@ __global__ void __launch_bounds__(256) k_bin_scatter(int M, const signed char* l
 }
 
 // ---------------------------------------------------------------------------
-// Row accumulation.
-
-// Left row read from a global CSR (entries [b, e) of ci / v).
-struct LeftGlobal {
-    const int* ci;
-    const void* v;
-    int vt;
-    int b, e;
-    __device__ __forceinline__ int key(int t) const { return __ldg(ci + t); }
-    __device__ __forceinline__ double val(int t) const { return load_val(v, vt, t); }
-};
-// Left row held in shared memory (the forwarded R*A row of the direct
-// product, in first-touch order).
-struct LeftShared {
-    const int* lc;
-    const double* lv;
-    int b, e;
-    __device__ __forceinline__ int key(int t) const { return lc[t]; }
-    __device__ __forceinline__ double val(int t) const { return lv[t]; }
-};
-
-// Accumulate sum_t left.val(t) * B(left.key(t), :) into the table, in
-// ascending t.  ord[n..] receives the slots of new keys in first-touch order.
-// Returns the number of distinct keys; `fail` is set (group-uniformly) when
-// the table ran out of slots.
-template <int G, bool NUM, class Left>
-__device__ __forceinline__ int accumulate(const Group<G>& g, const Left& L, const int* b_rp,
-                                          const int* b_ci, const void* b_v, int b_vt,
-                                          int* keys, double* vals, int* ord, unsigned smask,
-                                          int shift, bool& fail) {
-    int n = 0;
-    for (int t0 = L.b; t0 < L.e; t0 += G) {
-        // Prefetch G steps: lane j holds step t0+j's scalar and B row bounds.
-        const int t = t0 + g.gl;
-        int bb = 0, be = 0;
-        double av = 0.0;
-        if (t < L.e) {
-            const int k = L.key(t);
-            if (NUM) av = L.val(t);
-            bb = __ldg(b_rp + k);
-            be = __ldg(b_rp + k + 1);
-        }
-        const int cnt = min(G, L.e - t0);
-        for (int j = 0; j < cnt; ++j) {
-            const int jb = g.bcast(bb, j), je = g.bcast(be, j);
-            const double jav = NUM ? g.bcast(av, j) : 0.0;
-            for (int e0 = jb; e0 < je; e0 += G) {
-                const int e = e0 + g.gl;
-                bool is_new = false, bad = false;
-                int s = 0;
-                if (e < je) {
-                    const int c = __ldg(b_ci + e);
-                    s = table_insert(keys, smask, shift, c, is_new);
-                    if (s < 0) {
-                        bad = true;
-                    } else if (NUM) {
-                        const double bv = load_val(b_v, b_vt, e);
-                        vals[s] = __dadd_rn(vals[s], __dmul_rn(bv, jav));
-                    }
-                }
-                const unsigned nb = g.ballot(is_new);
-                if (is_new) ord[n + __popc(nb & g.below)] = s;
-                n += __popc(nb);
-                if (g.ballot(bad)) { fail = true; return n; }
-            }
-            g.sync();
-        }
-    }
-    return n;
-}
-
-// Clear the slots listed in ord[0..n) (and their values).
-template <int G, bool NUM>
-__device__ __forceinline__ void table_clear(const Group<G>& g, int* keys, double* vals,
-                                            const int* ord, int n) {
-    for (int i = g.gl; i < n; i += G) {
-        const int s = ord[i];
-        keys[s] = kEmpty;
-        if (NUM) vals[s] = 0.0;
-    }
-    g.sync();
-}
-
-// Clear a whole table (after a failed row, whose ord may be incomplete).
-template <int G, bool NUM>
-__device__ __forceinline__ void table_clear_all(const Group<G>& g, int* keys, double* vals,
-                                                int slots) {
-    for (int s = g.gl; s < slots; s += G) {
-        keys[s] = kEmpty;
-        if (NUM) vals[s] = 0.0;
-    }
-    g.sync();
-}
-
-// Move the row's n entries out of the table into (ck, cv) [ck may alias
-// ord: entry i is read then written by the same lane], clearing the slots.
-template <int G>
-__device__ __forceinline__ void table_extract(const Group<G>& g, int* keys, double* vals,
-                                              int* ord, int* ck, double* cv, int n) {
-    for (int i = g.gl; i < n; i += G) {
-        const int s = ord[i];
-        const int k = keys[s];
-        const double v = vals[s];
-        keys[s] = kEmpty;
-        vals[s] = 0.0;
-        ck[i] = k;
-        cv[i] = v;
-    }
-    g.sync();
-}
-
-constexpr int kRankSortMax = 96;
-
-// Write the n (key, value) pairs in ascending key order to out[base ..].
-// Short rows: rank by counting smaller keys.  Long rows: in-place bitonic
-// sort over next_pow2(n) entries (capacity >= that), then a coalesced copy.
-template <int G>
-__device__ __forceinline__ void sorted_write(const Group<G>& g, int* ck, double* cv, int n,
-                                             int* out_ci, void* out_v, int out_vt,
-                                             long long base) {
-    if (n <= kRankSortMax) {
-        for (int i = g.gl; i < n; i += G) {
-            const int k = ck[i];
-            int r = 0;
-            for (int j = 0; j < n; ++j) r += ck[j] < k;
-            out_ci[base + r] = k;
-            store_val(out_v, out_vt, base + r, cv[i]);
-        }
-        g.sync();
-        return;
-    }
-    const int P2 = static_cast<int>(next_pow2(static_cast<unsigned>(n)));
-    for (int i = n + g.gl; i < P2; i += G) ck[i] = INT_MAX;
-    g.sync();
-    for (int k = 2; k <= P2; k <<= 1) {
-        for (int j = k >> 1; j > 0; j >>= 1) {
-            for (int i = g.gl; i < P2; i += G) {
-                const int ixj = i ^ j;
-                if (ixj > i) {
-                    const int a = ck[i], b = ck[ixj];
-                    const bool up = (i & k) == 0;
-                    if ((a > b) == up) {
-                        ck[i] = b;
-                        ck[ixj] = a;
-                        const double t = cv[i];
-                        cv[i] = cv[ixj];
-                        cv[ixj] = t;
-                    }
-                }
-            }
-            g.sync();
-        }
-    }
-    for (int i = g.gl; i < n; i += G) {
-        out_ci[base + i] = ck[i];
-        store_val(out_v, out_vt, base + i, cv[i]);
-    }
-    g.sync();
-}
-
-// Symbolic write-out of row sizes.
-template <int G>
-__device__ __forceinline__ void record_count(const Group<G>& g, int* row_cnt, int row, int n) {
-    if (g.gl == 0) row_cnt[row] = n;
-}
-
-// Output base of a numeric row: the exact row pointer, or a booking in the
-// upper-bound space.  Returns -1 when the row cannot be written.
-template <int G, int MODE>
-__device__ __forceinline__ long long output_base(const Group<G>& g, int row, int n,
-                                                 const int* c_rp, unsigned long long* cursor,
-                                                 unsigned long long cap, long long* row_off,
-                                                 int* row_cnt, unsigned* err) {
-    if (MODE == kNumExact) {
-        const int b = c_rp[row];
-        if (c_rp[row + 1] - b != n) {
-            if (g.gl == 0) atomicOr(err, kErrCount);
-            return -1;
-        }
-        return b;
-    }
-    unsigned long long off = 0;
-    if (g.gl == 0) off = atomicAdd(cursor, static_cast<unsigned long long>(n));
-    off = g.bcast(off, 0);
-    if (off + n > cap) {
-        if (g.gl == 0) {
-            atomicOr(err, kErrBook);
-            row_off[row] = 0;
-            row_cnt[row] = 0;
-        }
-        return -1;
-    }
-    if (g.gl == 0) {
-        row_off[row] = static_cast<long long>(off);
-        row_cnt[row] = n;
-    }
-    return static_cast<long long>(off);
-}
-
-// Per-group table region.  Numeric: vals[S] cv[S] keys[S] ord[S] (24 B per
-// slot); symbolic: keys[S] ord[S] (8 B per slot).
-template <int G, int MODE>
-__global__ void __launch_bounds__(256) k_pair_rows(PairArgs p, RowSet rs) {
-    constexpr bool NUM = MODE != kSymb;
-    extern __shared__ __align__(16) unsigned char smem[];
-    const Group<G> g;
-    const int gpc = blockDim.x / G;
-    const int gid = threadIdx.x / G;
-    const int S = rs.slots;
-    const unsigned smask = static_cast<unsigned>(S - 1);
-    unsigned char* region = rs.gtab
-        ? rs.gtab + static_cast<long long>(blockIdx.x * gpc + gid) * rs.gtab_stride
-        : smem + static_cast<size_t>(gid) * (NUM ? 24 : 8) * S;
-    double* vals = reinterpret_cast<double*>(region);
-    double* cv = vals + S;
-    int* keys = NUM ? reinterpret_cast<int*>(cv + S) : reinterpret_cast<int*>(region);
-    int* ord = keys + S;
-    table_clear_all<G, NUM>(g, keys, vals, S);
-
-    for (int it = blockIdx.x * gpc + gid; it < rs.nrows; it += gridDim.x * gpc) {
-        const int row = rs.rows[it];
-        LeftGlobal L{p.A.ci, p.A.v, p.A.vtype, __ldg(p.A.rp + row), __ldg(p.A.rp + row + 1)};
-        bool fail = false;
-        const int n = accumulate<G, NUM>(g, L, p.B.rp, p.B.ci, p.B.v, p.B.vtype, keys, vals,
-                                         ord, smask, rs.shift, fail);
-        if (fail) {
-            if (g.gl == 0) atomicOr(p.err, kErrTable);
-            table_clear_all<G, NUM>(g, keys, vals, S);
-            continue;
-        }
-        if (!NUM) {
-            record_count(g, p.row_cnt, row, n);
-            table_clear<G, false>(g, keys, vals, ord, n);
-            continue;
-        }
-        table_extract(g, keys, vals, ord, ord, cv, n);
-        const long long base = output_base<G, MODE>(g, row, n, p.c_rp, p.book_cursor,
-                                                    p.book_cap, p.row_off, p.row_cnt, p.err);
-        if (base < 0) continue;
-        if (MODE == kNumExact) sorted_write(g, ord, cv, n, p.c_ci, p.c_v, p.c_vtype, base);
-        else sorted_write(g, ord, cv, n, p.ub_ci, p.ub_v, p.c_vtype, base);
-    }
-}
-
-// Direct R*A*P rows.  Numeric region: vals[S] lv[S] keys[S] ord[S] lc[S]
-// (28 B per slot); symbolic: keys[S] ord[S] lc[S] (12 B per slot).
-template <int G, int MODE>
-__global__ void __launch_bounds__(256) k_direct_rows(DirectArgs p, RowSet rs) {
-    constexpr bool NUM = MODE != kSymb;
-    extern __shared__ __align__(16) unsigned char smem[];
-    const Group<G> g;
-    const int gpc = blockDim.x / G;
-    const int gid = threadIdx.x / G;
-    const int S = rs.slots;
-    const unsigned smask = static_cast<unsigned>(S - 1);
-    unsigned char* region = rs.gtab
-        ? rs.gtab + static_cast<long long>(blockIdx.x * gpc + gid) * rs.gtab_stride
-        : smem + static_cast<size_t>(gid) * (NUM ? 28 : 12) * S;
-    double* vals = reinterpret_cast<double*>(region);
-    double* lv = vals + S;
-    int* keys = NUM ? reinterpret_cast<int*>(lv + S) : reinterpret_cast<int*>(region);
-    int* ord = keys + S;
-    int* lc = ord + S;
-    table_clear_all<G, NUM>(g, keys, vals, S);
-
-    for (int it = blockIdx.x * gpc + gid; it < rs.nrows; it += gridDim.x * gpc) {
-        const int row = rs.rows[it];
-        // Phase 1: the R*A row, first-touch order in ord.
-        LeftGlobal L1{p.R.ci, p.R.v, p.R.vtype, __ldg(p.R.rp + row), __ldg(p.R.rp + row + 1)};
-        bool fail = false;
-        const int n1 = accumulate<G, NUM>(g, L1, p.A.rp, p.A.ci, p.A.v, p.A.vtype, keys, vals,
-                                          ord, smask, rs.shift, fail);
-        if (fail) {
-            if (g.gl == 0) atomicOr(p.err, kErrTable);
-            table_clear_all<G, NUM>(g, keys, vals, S);
-            continue;
-        }
-        // Move the R*A row to (lc, lv) in first-touch order; free the table.
-        if (NUM) {
-            table_extract(g, keys, vals, ord, lc, lv, n1);
-        } else {
-            for (int i = g.gl; i < n1; i += G) {
-                const int s = ord[i];
-                lc[i] = keys[s];
-                keys[s] = kEmpty;
-            }
-            g.sync();
-        }
-        // Phase 2: forward into P.
-        LeftShared L2{lc, lv, 0, n1};
-        const int n2 = accumulate<G, NUM>(g, L2, p.P.rp, p.P.ci, p.P.v, p.P.vtype, keys, vals,
-                                          ord, smask, rs.shift, fail);
-        if (fail) {
-            if (g.gl == 0) atomicOr(p.err, kErrTable);
-            table_clear_all<G, NUM>(g, keys, vals, S);
-            continue;
-        }
-        if (!NUM) {
-            record_count(g, p.row_cnt, row, n2);
-            if (p.row_cnt1 && g.gl == 0) p.row_cnt1[row] = n1;
-            table_clear<G, false>(g, keys, vals, ord, n2);
-            continue;
-        }
-        table_extract(g, keys, vals, ord, ord, lv, n2);
-        const long long base = output_base<G, MODE>(g, row, n2, p.c_rp, p.book_cursor,
-                                                    p.book_cap, p.row_off, p.row_cnt, p.err);
-        if (base < 0) continue;
-        if (MODE == kNumExact) sorted_write(g, ord, lv, n2, p.c_ci, p.c_v, p.c_vtype, base);
-        else sorted_write(g, ord, lv, n2, p.ub_ci, p.ub_v, p.c_vtype, base);
-    }
-}
-
-// ---------------------------------------------------------------------------
-// Upper-bound flavour: compaction of booked rows into exact CSR
-// (replaces mergeRows, code/src/include/SpMMUtilsGeneric.h:364-403).
+// Upper-bound flavour: copy of booked rows into exact CSR.  8 lanes per row.
 __global__ void __launch_bounds__(256) k_compact(int M, const int* row_cnt,
                                                   const long long* row_off, const int* ub_ci,
                                                   const void* ub_v, const int* c_rp, int* c_ci,
                                                   void* c_v, int vt) {
-    const Group<32> g;
-    const int warps = (gridDim.x * blockDim.x) / 32;
-    for (int row = (blockIdx.x * blockDim.x + threadIdx.x) / 32; row < M; row += warps) {
+    const Group<8> g;
+    const int groups = (gridDim.x * blockDim.x) / 8;
+    for (int row = (blockIdx.x * blockDim.x + threadIdx.x) / 8; row < M; row += groups) {
         const int n = row_cnt[row];
         if (!n) continue;
         const long long src = row_off[row];
         const long long dst = c_rp[row];
-        for (int i = g.gl; i < n; i += 32) {
+        for (int i = g.gl; i < n; i += 8) {
             c_ci[dst + i] = ub_ci[src + i];
             if (vt == SP3MM_F32)
                 static_cast<float*>(c_v)[dst + i] = static_cast<const float*>(ub_v)[src + i];
@@ -627,8 +294,8 @@ __global__ void __launch_bounds__(256) k_transpose_scatter(CsrView A, const int*
     }
 }
 
-// Sort each row's (col, val) by col.  Warp per row; short rows by rank in
-// registers, long rows by an odd-even transposition over global memory.
+// Sort each row's (col, val) by col.  Warp per row; rows up to 32 entries by
+// rank in registers, longer rows by odd-even transposition in place.
 __global__ void __launch_bounds__(256) k_sort_rows(int M, const int* rp, int* ci, void* v,
                                                     int vt) {
     const int lane = threadIdx.x & 31;
@@ -697,158 +364,51 @@ static inline int grid_for(long long work, int block, int cap = 148 * 16) {
     return static_cast<int>(g);
 }
 
-int choose_group(double mean) {
-    if (mean <= 4.0) return 4;
-    if (mean <= 8.0) return 8;
-    if (mean <= 16.0) return 16;
-    return 32;
-}
-
-LevelPlan plan_level(int level, bool direct, int mode, int G, size_t budget) {
-    LevelPlan pl{};
-    pl.slots = 32 << level;
-    const size_t per_group = static_cast<size_t>(bytes_per_slot(direct, mode)) * pl.slots;
-    if (level >= kSharedLevels || per_group > budget) {
-        pl.global = true;
-        pl.G = 32;
-        pl.groups_per_cta = 8;
-        pl.smem_bytes = 0;
-        return pl;
-    }
-    // Large tables use a whole warp per row.
-    int g = G;
-    if (pl.slots >= 1024 && g < 32) g = 32;
-    if (pl.slots >= 512 && g < 16) g = 16;
-    const int per_warp = 32 / g;
-    int warps = static_cast<int>(budget / (per_group * per_warp));
-    if (warps < 1) {
-        // Fewer groups than a warp holds: go to one full-warp group.
-        g = 32;
-        warps = static_cast<int>(budget / per_group);
-        if (warps < 1) {
-            pl.global = true;
-            pl.G = 32;
-            pl.groups_per_cta = 8;
-            pl.smem_bytes = 0;
-            return pl;
-        }
-    }
-    if (warps > 8) warps = 8;
-    pl.G = g;
-    pl.groups_per_cta = warps * (32 / g);
-    pl.smem_bytes = per_group * pl.groups_per_cta;
-    pl.global = false;
-    return pl;
-}
-
 void launch_pair_bounds(const CsrView& A, const CsrView& B, int* need,
                         unsigned long long* total, cudaStream_t st) {
     if (A.M == 0) return;
-    const int grid = grid_for(static_cast<long long>(A.M) * 8, 256);
-    k_pair_bounds<8><<<grid, 256, 0, st>>>(A, B, need, total);
-    counted();
+    k_pair_bounds<8><<<grid_for(static_cast<long long>(A.M) * 8, 256), 256, 0, st>>>(A, B, need,
+                                                                                     total);
+    note_launch();
 }
 
-void launch_direct_bounds(const CsrView& R, const CsrView& A, const CsrView& P, int* need,
+void launch_direct_bounds(const CsrView& R, const CsrView& A, int p_max_row, int* need,
                           unsigned long long* total, cudaStream_t st) {
     if (R.M == 0) return;
-    const int grid = grid_for(static_cast<long long>(R.M) * 8, 256);
-    k_direct_bounds<8><<<grid, 256, 0, st>>>(R, A, P, need, total);
-    counted();
+    k_direct_bounds<8><<<grid_for(static_cast<long long>(R.M) * 8, 256), 256, 0, st>>>(
+        R, A, p_max_row, need, total);
+    note_launch();
 }
 
 void launch_need_from_counts(int M, const int* cnt, const int* cnt1, int* need,
                              cudaStream_t st) {
     if (M == 0) return;
     k_need_from_counts<<<(M + 255) / 256, 256, 0, st>>>(M, cnt, cnt1, need);
-    counted();
+    note_launch();
 }
 
-void launch_bin_levels(int M, const int* need, signed char* level, int* counts, int* gmax,
-                       int* row_cnt_zero, cudaStream_t st) {
+void launch_bin_levels(int M, const int* need, int shift, int G, signed char* level,
+                       int* counts, int* nmax, int* row_cnt_zero, cudaStream_t st) {
     if (M == 0) return;
-    k_bin_levels<<<grid_for(M, 256), 256, 0, st>>>(M, need, level, counts, gmax,
+    k_bin_levels<<<grid_for(M, 256), 256, 0, st>>>(M, need, shift, G, level, counts, nmax,
                                                     row_cnt_zero);
-    counted();
+    note_launch();
 }
 
 void launch_bin_scatter(int M, const signed char* level, int* cursors, int* lists,
                         cudaStream_t st) {
     if (M == 0) return;
     k_bin_scatter<<<(M + 255) / 256, 256, 0, st>>>(M, level, cursors, lists);
-    counted();
+    note_launch();
 }
-
-template <template <int, int> class K>
-struct Dummy {};
-
-#define SP3MM_DISPATCH_G(G, BODY) \
-    switch (G) {                 \
-        case 4: { constexpr int GG = 4; BODY; } break;   \
-        case 8: { constexpr int GG = 8; BODY; } break;   \
-        case 16: { constexpr int GG = 16; BODY; } break; \
-        default: { constexpr int GG = 32; BODY; } break; \
-    }
-
-template <int G, int MODE>
-static void pair_rows_g(const PairArgs& a, const LevelPlan& pl, const RowSet& rs, int grid,
-                        cudaStream_t st) {
-    auto k = k_pair_rows<G, MODE>;
-    if (pl.smem_bytes > 48 * 1024)
-        cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                             static_cast<int>(pl.smem_bytes));
-    k<<<grid, pl.groups_per_cta * G, pl.smem_bytes, st>>>(a, rs);
-    counted();
-}
-
-template <int G, int MODE>
-static void direct_rows_g(const DirectArgs& a, const LevelPlan& pl, const RowSet& rs, int grid,
-                          cudaStream_t st) {
-    auto k = k_direct_rows<G, MODE>;
-    if (pl.smem_bytes > 48 * 1024)
-        cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                             static_cast<int>(pl.smem_bytes));
-    k<<<grid, pl.groups_per_cta * G, pl.smem_bytes, st>>>(a, rs);
-    counted();
-}
-
-void launch_pair_rows(const PairArgs& a, int mode, const LevelPlan& pl, const RowSet& rs,
-                      int grid, cudaStream_t st) {
-    if (rs.nrows == 0) return;
-    switch (mode) {
-        case kSymb: SP3MM_DISPATCH_G(pl.G, (pair_rows_g<GG, kSymb>(a, pl, rs, grid, st))); break;
-        case kNumExact:
-            SP3MM_DISPATCH_G(pl.G, (pair_rows_g<GG, kNumExact>(a, pl, rs, grid, st)));
-            break;
-        default: SP3MM_DISPATCH_G(pl.G, (pair_rows_g<GG, kNumBook>(a, pl, rs, grid, st))); break;
-    }
-}
-
-void launch_direct_rows(const DirectArgs& a, int mode, const LevelPlan& pl, const RowSet& rs,
-                        int grid, cudaStream_t st) {
-    if (rs.nrows == 0) return;
-    switch (mode) {
-        case kSymb:
-            SP3MM_DISPATCH_G(pl.G, (direct_rows_g<GG, kSymb>(a, pl, rs, grid, st)));
-            break;
-        case kNumExact:
-            SP3MM_DISPATCH_G(pl.G, (direct_rows_g<GG, kNumExact>(a, pl, rs, grid, st)));
-            break;
-        default:
-            SP3MM_DISPATCH_G(pl.G, (direct_rows_g<GG, kNumBook>(a, pl, rs, grid, st)));
-            break;
-    }
-}
-
-size_t row_kernel_max_smem() { return 110 * 1024; }
 
 void launch_compact(int M, const int* row_cnt, const long long* row_off, const int* ub_ci,
                     const void* ub_v, const int* c_rp, int* c_ci, void* c_v, int vt,
                     cudaStream_t st) {
     if (M == 0) return;
-    k_compact<<<grid_for(static_cast<long long>(M) * 32, 256), 256, 0, st>>>(
+    k_compact<<<grid_for(static_cast<long long>(M) * 8, 256), 256, 0, st>>>(
         M, row_cnt, row_off, ub_ci, ub_v, c_rp, c_ci, c_v, vt);
-    counted();
+    note_launch();
 }
 
 size_t scan_temp_bytes(int M) {
@@ -863,13 +423,13 @@ void launch_scan(int M, const int* cnt, int* row_ptr, void* temp, size_t temp_by
     cudaMemsetAsync(row_ptr, 0, sizeof(int), st);
     if (M == 0) return;
     cub::DeviceScan::InclusiveSum(temp, temp_bytes, cnt, row_ptr + 1, M, st);
-    counted();
+    note_launch();
 }
 
 void launch_narrow_rowptr(long long M, long long nnz, const unsigned long long* src, int off,
                           int* dst, unsigned* err, cudaStream_t st) {
     k_narrow_rowptr<<<grid_for(M + 1, 256), 256, 0, st>>>(M, nnz, src, off, dst, err);
-    counted();
+    note_launch();
 }
 
 void launch_narrow_cols(long long M, long long N, const int* rp, const unsigned long long* src,
@@ -877,21 +437,21 @@ void launch_narrow_cols(long long M, long long N, const int* rp, const unsigned 
     if (M == 0) return;
     k_narrow_cols<<<grid_for(M * 32, 256), 256, 0, st>>>(M, N, rp, src, off, dst, max_row,
                                                          err);
-    counted();
+    note_launch();
 }
 
 void launch_widen(long long n, const int* src, int off, unsigned long long* dst,
                   cudaStream_t st) {
     if (n == 0) return;
     k_widen<<<grid_for(n, 256), 256, 0, st>>>(n, src, off, dst);
-    counted();
+    note_launch();
 }
 
 void launch_convert_values(long long n, const void* src, int src_type, void* dst, int dst_type,
                            cudaStream_t st) {
     if (n == 0) return;
     k_convert_values<<<grid_for(n, 256), 256, 0, st>>>(n, src, src_type, dst, dst_type);
-    counted();
+    note_launch();
 }
 
 void launch_validate_i32(int M, int N, const int* rp, const int* ci, int* max_row,
@@ -899,13 +459,13 @@ void launch_validate_i32(int M, int N, const int* rp, const int* ci, int* max_ro
     if (M == 0) return;
     k_validate_i32<<<grid_for(static_cast<long long>(M) * 32, 256), 256, 0, st>>>(
         M, N, rp, ci, max_row, err);
-    counted();
+    note_launch();
 }
 
 void launch_col_counts(long long nnz, const int* ci, int* counts, cudaStream_t st) {
     if (nnz == 0) return;
     k_col_counts<<<grid_for(nnz, 256), 256, 0, st>>>(nnz, ci, counts);
-    counted();
+    note_launch();
 }
 
 void launch_transpose_scatter(const CsrView& A, const int* t_rp, int* cursor, int* t_ci,
@@ -913,7 +473,7 @@ void launch_transpose_scatter(const CsrView& A, const int* t_rp, int* cursor, in
     if (A.M == 0) return;
     k_transpose_scatter<<<grid_for(static_cast<long long>(A.M) * 32, 256), 256, 0, st>>>(
         A, t_rp, cursor, t_ci, t_v);
-    counted();
+    note_launch();
 }
 
 void launch_sort_rows(int M, const int* rp, int* ci, void* v, int vt, int max_row,
@@ -921,18 +481,15 @@ void launch_sort_rows(int M, const int* rp, int* ci, void* v, int vt, int max_ro
     if (M == 0 || max_row <= 1) return;
     k_sort_rows<<<grid_for(static_cast<long long>(M) * 32, 256), 256, 0, st>>>(M, rp, ci, v,
                                                                               vt);
-    counted();
+    note_launch();
 }
 
-void launch_colparts_ub(const CsrView& A, const CsrView& B, int gridCols,
-                        const long long* bColOffsets, int off, long long* out,
-                        unsigned long long* total, cudaStream_t st) {
-    (void)B;
-    (void)off;
+void launch_colparts_ub(const CsrView& A, int gridCols, const long long* bColOffsets,
+                        long long* out, unsigned long long* total, cudaStream_t st) {
     const long long work = static_cast<long long>(A.M) * gridCols;
     if (work == 0) return;
     k_colparts_ub<<<grid_for(work, 256), 256, 0, st>>>(A, gridCols, bColOffsets, out, total);
-    counted();
+    note_launch();
 }
 
 }  // namespace sp3mm

@@ -19,106 +19,76 @@ struct CsrView {
 // Row-kernel modes.
 enum Mode : int { kSymb = 0, kNumExact = 1, kNumBook = 2 };
 
-// Table-size levels: level L holds slots = 32 << L.  Levels below
-// kSharedLevels keep their tables in shared memory; the last level keeps
-// them in global memory.
+// Table-size levels: level L uses 32 << L slots.
 constexpr int kMinLogSlots = 5;
-constexpr int kSharedLevels = 8;          // 32 .. 4096 slots
-constexpr int kLevels = kSharedLevels + 1;
-constexpr int kGlobalLevel = kSharedLevels;
+constexpr int kLevels = 24;
 
-// Slots a row needs for `bound` distinct keys (load factor <= 0.8).
-inline unsigned slots_for(long long bound) {
-    long long need = bound + bound / 4 + 1;
-    unsigned s = 32;
-    while ((long long)s < need && s < (1u << 30)) s <<= 1;
-    return s;
-}
-
-// Bytes of table state per slot for a kernel family/mode.
-inline int bytes_per_slot(bool direct, int mode) {
-    if (direct) return mode == kSymb ? 12 : 28;
-    return mode == kSymb ? 8 : 24;
-}
-
-// Shared-memory plan of one level: group size, groups per CTA, bytes.
-struct LevelPlan {
-    int G;
-    int groups_per_cta;
-    int slots;
-    size_t smem_bytes;   // per CTA (0 for the global level)
-    bool global;
+struct DirectRowArgs {
+    CsrView R, A, P;   // C = R*A*P, one output row per row of R
+};
+struct PairRowArgs {
+    CsrView A, B;      // C = A*B, one output row per row of A
 };
 
-// Per-launch row set of one level.
-struct RowSet {
-    const int* rows;
+// Per-launch parameters shared by both row-kernel families.
+struct RowParams {
+    const int* rows;          // the rows of this launch
     int nrows;
-    int slots;
-    int shift;
-    unsigned char* gtab;     // global tables (nullptr: shared memory)
-    long long gtab_stride;   // bytes per group in gtab
-};
-
-struct PairArgs {
-    CsrView A, B;            // C = A*B, rows of A processed
-    int* row_cnt;            // kSymb: exact length; kNumBook: booked length
-    const int* c_rp;         // kNumExact: output row pointers
+    int S1, S2;               // table slots (powers of two >= 32); S2: direct only
+    unsigned char* gtab;      // tables in global memory (nullptr: shared memory)
+    long long gstride;        // bytes per group in gtab
+    int* retry_rows;          // rows whose table overflowed (nullptr: error)
+    int* retry_count;
+    int* row_cnt;             // kSymb: C row length; kNumBook: booked length
+    int* row_cnt1;            // kSymb, direct: R*A row length (may be null)
+    const int* c_rp;          // kNumExact: output row pointers
     int* c_ci;
     void* c_v;
-    int c_vtype;
-    unsigned long long* book_cursor;
-    unsigned long long book_cap;
-    long long* row_off;      // kNumBook: offset of each row in the UB space
+    int c_vt;
+    unsigned long long* cursor;   // kNumBook: booking cursor
+    unsigned long long cap;       //           and capacity (entries)
+    long long* row_off;           //           offset of each row
     int* ub_ci;
     void* ub_v;
     unsigned* err;
 };
 
-struct DirectArgs {
-    CsrView R, A, P;         // C = R*A*P, rows of R processed
-    int* row_cnt;            // kSymb: exact C row length; kNumBook: booked
-    int* row_cnt1;           // kSymb: distinct R*A row length (may be null)
-    const int* c_rp;
-    int* c_ci;
-    void* c_v;
-    int c_vtype;
-    unsigned long long* book_cursor;
-    unsigned long long book_cap;
-    long long* row_off;
-    int* ub_ci;
-    void* ub_v;
-    unsigned* err;
+// Launch geometry of one row-kernel launch.
+struct RowGeom {
+    int G;        // lanes per row
+    int grid, block;
+    size_t smem;  // dynamic shared memory per CTA
 };
 
-// Choose the group size (lanes per row) from the right operand's mean row
-// length, and derive the per-level launch plan.
-int choose_group(double mean_right_row_len);
-LevelPlan plan_level(int level, bool direct, int mode, int G, size_t smem_budget);
+size_t row_table_bytes(bool direct, int mode, int S1, int S2);
+int row_table_limit(int S, int G);
+cudaError_t launch_direct_rows(const DirectRowArgs& a, const RowParams& p, int mode,
+                               const RowGeom& geo, cudaStream_t st);
+cudaError_t launch_pair_rows(const PairRowArgs& a, const RowParams& p, int mode,
+                             const RowGeom& geo, cudaStream_t st);
 
-// Bounds: per-row table size requirement (`need`, distinct-key bound) and
-// the total multiply-add count (upper bound of the output size).
+// Bounds: need[i] = distinct-key bound of the first table (A*B: min(flops,
+// N); R*A*P: min(len of the R*A products, A.N)); total += the multiply-add
+// bound of the output (A*B: flops; R*A*P: R*A flops times P's longest row).
 void launch_pair_bounds(const CsrView& A, const CsrView& B, int* need,
-                        unsigned long long* total_flops, cudaStream_t st);
-void launch_direct_bounds(const CsrView& R, const CsrView& A, const CsrView& P, int* need,
-                          unsigned long long* total_flops, cudaStream_t st);
+                        unsigned long long* total, cudaStream_t st);
+void launch_direct_bounds(const CsrView& R, const CsrView& A, int p_max_row, int* need,
+                          unsigned long long* total, cudaStream_t st);
 // need from exact counts: max(cnt[i], cnt1[i]) (cnt1 may be null).
 void launch_need_from_counts(int M, const int* cnt, const int* cnt1, int* need,
                              cudaStream_t st);
 
-// Binning: level of every row from `need`; counts[kLevels+1] (the extra
-// entry counts empty rows, whose row_cnt is zeroed); global_need_max.
-void launch_bin_levels(int M, const int* need, signed char* level, int* counts,
-                       int* global_need_max, int* row_cnt_zero, cudaStream_t st);
+// Binning: level of every row from need[i] >> shift for a group of G lanes
+// (counts[kLevels] = empty rows, whose row_cnt is zeroed when given);
+// nmax = largest need.
+void launch_bin_levels(int M, const int* need, int shift, int G, signed char* level,
+                       int* counts, int* nmax, int* row_cnt_zero, cudaStream_t st);
 void launch_bin_scatter(int M, const signed char* level, int* cursors, int* lists,
                         cudaStream_t st);
-
-// Row kernels.
-void launch_pair_rows(const PairArgs& a, int mode, const LevelPlan& plan, const RowSet& rs,
-                      int grid, cudaStream_t st);
-void launch_direct_rows(const DirectArgs& a, int mode, const LevelPlan& plan,
-                        const RowSet& rs, int grid, cudaStream_t st);
-size_t row_kernel_max_smem();
+// Smallest slot count (power of two >= 32) whose load limit for G lanes
+// admits `need` distinct keys.
+int slots_for_need(long long need, int G);
+int level_for_need(long long need, int G);
 
 // Upper-bound flavour: copy each booked row into exact CSR.
 void launch_compact(int M, const int* row_cnt, const long long* row_off, const int* ub_ci,
@@ -150,10 +120,10 @@ void launch_sort_rows(int M, const int* rp, int* ci, void* v, int vtype, int max
                       cudaStream_t st);
 
 // 2D column-partition upper bounds.
-void launch_colparts_ub(const CsrView& A, const CsrView& B, int gridCols,
-                        const long long* bColOffsets, int off, long long* out,
-                        unsigned long long* total, cudaStream_t st);
+void launch_colparts_ub(const CsrView& A, int gridCols, const long long* bColOffsets,
+                        long long* out, unsigned long long* total, cudaStream_t st);
 
+void note_launch();
 uint64_t launch_count();
 
 }  // namespace sp3mm

@@ -1,0 +1,597 @@
+// rows.cu -- per-row accumulation kernels of the Sp3MM products (sm_100a).
+//
+// One group of G lanes owns one output row and its hash tables.  The lanes
+// walk the left row one step at a time; within a step they cover the selected
+// right row, whose columns are distinct, so every output entry receives its
+// contributions in ascending left-row position -- the order of the
+// reference's scSparseVectMul_ loop (code/src/include/SpMMUtilsGeneric.h:
+// 39-55) -- with no value atomics, and the values are bit-identical to the
+// reference's.  New keys of a step are ranked by ballot + popc in lane order,
+// which reproduces the first-touch order in which the reference's index map
+// appends them (code/src/include/sparseMatrix.h:85-104); the direct product
+// forwards the R*A row into P in that order
+// (code/src/Sp3MM_CSR_OMP_UB_Generic.c:542-545).
+//
+// Latency: the row pointers of the right operand are loaded two chunks of G
+// steps ahead and the right-row entries one chunk ahead, into registers, so
+// the dependent chain left key -> row pointer -> entries is off the critical
+// path of the sequential accumulation.
+//
+// Table sizes are runtime powers of two.  A row whose distinct-key count
+// would pass the table's load limit stops, clears its slots and is appended
+// to a retry list, which a second launch processes with tables sized from a
+// proven bound; results do not depend on the table size.
+#include <climits>
+
+#include "kernels.cuh"
+#include "sp3mm_internal.cuh"
+
+namespace sp3mm {
+
+__device__ __forceinline__ double ldv(const void* p, int vt, long long i) {
+    if (vt == SP3MM_F32) return static_cast<double>(__ldg(static_cast<const float*>(p) + i));
+    return __ldg(static_cast<const double*>(p) + i);
+}
+__device__ __forceinline__ void stv(void* p, int vt, long long i, double v) {
+    if (vt == SP3MM_F32) static_cast<float*>(p)[i] = __double2float_rn(v);
+    else static_cast<double*>(p)[i] = v;
+}
+
+// Left row in global memory: entries [b, b+n) of (ci, v).
+struct LeftG {
+    const int* ci;
+    const void* v;
+    int vt;
+    int b, n;
+    __device__ __forceinline__ int key(int t) const { return __ldg(ci + b + t); }
+    __device__ __forceinline__ double val(int t) const { return ldv(v, vt, b + t); }
+};
+// Left row held in a shared table, read in the order of `ord` (first touch).
+struct LeftT {
+    const int* keys;
+    const double* vals;
+    const int* ord;
+    int n;
+    __device__ __forceinline__ int key(int t) const { return keys[ord[t]]; }
+    __device__ __forceinline__ double val(int t) const { return vals[ord[t]]; }
+};
+
+// Distinct keys a table of S slots accepts before the row is retried: at
+// most G keys arrive per sub-step, so the table never fills, and the load
+// factor stays <= 7/8.
+__host__ __device__ __forceinline__ int table_limit(int S, int G) {
+    const int a = S - G - 1, b = (7 * S) / 8;
+    return a < b ? a : b;
+}
+
+template <int G, bool NUM>
+struct Acc {
+    int* keys;
+    double* vals;
+    int* ord;
+    unsigned smask;
+    int shift;
+    int limit;
+};
+
+// One sub-step: lanes with `act` add prod = bv*s into key c.  Returns false
+// (group-uniformly) when the distinct count passed the limit.
+template <int G, bool NUM>
+__device__ __forceinline__ bool sub_step(const Group<G>& g, const Acc<G, NUM>& T, bool act,
+                                         int c, double bv, double s, int& nk) {
+    bool is_new = false;
+    int slot = 0;
+    if (act) {
+        slot = table_insert(T.keys, T.smask, T.shift, c, is_new);
+        if (NUM && slot >= 0) T.vals[slot] = __dadd_rn(T.vals[slot], __dmul_rn(bv, s));
+    }
+    const unsigned nb = g.ballot(is_new);
+    if (is_new) T.ord[nk + __popc(nb & g.below)] = slot;
+    nk += __popc(nb);
+    return nk <= T.limit;
+}
+
+// Accumulate sum_t L.val(t) * B(L.key(t), :) in ascending t.  Returns the
+// distinct-key count; `fail` when the table limit was passed.
+template <int G, int EP, bool NUM, class Left>
+__device__ __forceinline__ int accumulate(const Group<G>& g, const Left& L,
+                                          const int* __restrict__ b_rp,
+                                          const int* __restrict__ b_ci, const void* b_v,
+                                          int b_vt, const Acc<G, NUM>& T, bool& fail) {
+    const int n = L.n;
+    int nk = 0;
+    if (n <= 0) return 0;
+
+    // Pointers of chunk c (lane j <-> step c*G + j) and c+1.
+    int pb0 = 0, pe0 = 0, pb1 = 0, pe1 = 0;
+    double ps0 = 0.0, ps1 = 0.0;
+    auto load_ptrs = [&](int t0, int& pb, int& pe, double& ps) {
+        const int t = t0 + g.gl;
+        pb = 0;
+        pe = 0;
+        ps = 0.0;
+        if (t < n) {
+            const int k = L.key(t);
+            if (NUM) ps = L.val(t);
+            pb = __ldg(b_rp + k);
+            pe = __ldg(b_rp + k + 1);
+        }
+    };
+    // Entries of a chunk: [j][m] = entry gl + m*G of step j.
+    constexpr int EPA = EP > 0 ? EP : 1;   // array extent (EP == 0: no prefetch)
+    int ec0[G][EPA], ec1[G][EPA];
+    double ev0[G][EPA], ev1[G][EPA];
+    auto load_entries = [&](int pb, int pe, int (&ec)[G][EPA], double (&ev)[G][EPA]) {
+#pragma unroll
+        for (int j = 0; j < G; ++j) {
+            const int jb = g.bcast(pb, j), je = g.bcast(pe, j);
+#pragma unroll
+            for (int m = 0; m < EP; ++m) {
+                const int e = jb + m * G + g.gl;
+                ec[j][m] = -1;
+                ev[j][m] = 0.0;
+                if (e < je) {
+                    ec[j][m] = __ldg(b_ci + e);
+                    if (NUM) ev[j][m] = ldv(b_v, b_vt, e);
+                }
+            }
+        }
+    };
+
+    load_ptrs(0, pb0, pe0, ps0);
+    load_ptrs(G, pb1, pe1, ps1);
+    load_entries(pb0, pe0, ec0, ev0);
+    for (int base = 0; base < n; base += G) {
+        load_entries(pb1, pe1, ec1, ev1);
+        int pb2, pe2;
+        double ps2;
+        load_ptrs(base + 2 * G, pb2, pe2, ps2);
+        const int cnt = min(G, n - base);
+#pragma unroll
+        for (int j = 0; j < G; ++j) {
+            if (j < cnt) {
+                const int jb = g.bcast(pb0, j), je = g.bcast(pe0, j);
+                const double js = NUM ? g.bcast(ps0, j) : 0.0;
+#pragma unroll
+                for (int m = 0; m < EP; ++m) {
+                    if (jb + m * G < je) {
+                        const bool act = jb + m * G + g.gl < je;
+                        if (!sub_step<G, NUM>(g, T, act, ec0[j][m], ev0[j][m], js, nk)) {
+                            fail = true;
+                            return nk;
+                        }
+                    }
+                }
+                // Right rows longer than EP*G: the rest is loaded in place.
+                for (int e0 = jb + EP * G; e0 < je; e0 += G) {
+                    const int e = e0 + g.gl;
+                    const bool act = e < je;
+                    int c = -1;
+                    double bv = 0.0;
+                    if (act) {
+                        c = __ldg(b_ci + e);
+                        if (NUM) bv = ldv(b_v, b_vt, e);
+                    }
+                    if (!sub_step<G, NUM>(g, T, act, c, bv, js, nk)) {
+                        fail = true;
+                        return nk;
+                    }
+                }
+                g.sync();
+            }
+        }
+        pb0 = pb1;
+        pe0 = pe1;
+        ps0 = ps1;
+        pb1 = pb2;
+        pe1 = pe2;
+        ps1 = ps2;
+#pragma unroll
+        for (int j = 0; j < G; ++j)
+#pragma unroll
+            for (int m = 0; m < EP; ++m) {
+                ec0[j][m] = ec1[j][m];
+                ev0[j][m] = ev1[j][m];
+            }
+    }
+    return nk;
+}
+
+// Clear the slots listed in ord[0..n).
+template <int G, bool NUM>
+__device__ __forceinline__ void clear_listed(const Group<G>& g, const Acc<G, NUM>& T, int n) {
+    for (int i = g.gl; i < n; i += G) {
+        const int s = T.ord[i];
+        T.keys[s] = kEmpty;
+        if (NUM) T.vals[s] = 0.0;
+    }
+}
+
+template <int G, bool NUM>
+__device__ __forceinline__ void clear_all(const Group<G>& g, int* keys, double* vals, int S) {
+    for (int s = g.gl; s < S; s += G) {
+        keys[s] = kEmpty;
+        if (NUM) vals[s] = 0.0;
+    }
+}
+
+// Move the n listed entries of T into (ck, cv)[0..n), clearing T.
+template <int G>
+__device__ __forceinline__ void extract(const Group<G>& g, const Acc<G, true>& T, int n, int* ck,
+                                        double* cv) {
+    for (int i = g.gl; i < n; i += G) {
+        const int s = T.ord[i];
+        ck[i] = T.keys[s];
+        cv[i] = T.vals[s];
+        T.keys[s] = kEmpty;
+        T.vals[s] = 0.0;
+    }
+}
+
+// Write (ck, cv)[0..n) in ascending key order to out[base..].  Rows up to 64
+// entries: rank sort with each lane's keys cached in registers.  Longer rows:
+// bitonic sort in place (ck/cv hold next_pow2(n) slots), then a linear copy.
+// On return ck[0..n) / cv[0..n) are reset to kEmpty / 0.
+template <int G>
+__device__ __forceinline__ void sorted_write(const Group<G>& g, int* ck, double* cv, int n,
+                                             int* out_ci, void* out_v, int vt, long long base) {
+    constexpr int RM = 64 / G;
+    if (n <= 64) {
+        int mk[RM], rk[RM];
+#pragma unroll
+        for (int m = 0; m < RM; ++m) {
+            const int i = g.gl + m * G;
+            mk[m] = i < n ? ck[i] : INT_MAX;
+            rk[m] = 0;
+        }
+        for (int j = 0; j < n; ++j) {
+            const int kj = ck[j];
+#pragma unroll
+            for (int m = 0; m < RM; ++m) rk[m] += kj < mk[m];
+        }
+#pragma unroll
+        for (int m = 0; m < RM; ++m) {
+            const int i = g.gl + m * G;
+            if (i < n) {
+                out_ci[base + rk[m]] = mk[m];
+                stv(out_v, vt, base + rk[m], cv[i]);
+            }
+        }
+        g.sync();
+#pragma unroll
+        for (int m = 0; m < RM; ++m) {
+            const int i = g.gl + m * G;
+            if (i < n) {
+                ck[i] = kEmpty;
+                cv[i] = 0.0;
+            }
+        }
+        g.sync();
+        return;
+    }
+    const int P2 = static_cast<int>(next_pow2(static_cast<unsigned>(n)));
+    for (int i = n + g.gl; i < P2; i += G) ck[i] = INT_MAX;
+    g.sync();
+    for (int k = 2; k <= P2; k <<= 1) {
+        for (int j = k >> 1; j > 0; j >>= 1) {
+            for (int i = g.gl; i < P2; i += G) {
+                const int ixj = i ^ j;
+                if (ixj > i) {
+                    const int a = ck[i], b = ck[ixj];
+                    if ((a > b) == ((i & k) == 0)) {
+                        ck[i] = b;
+                        ck[ixj] = a;
+                        const double t = cv[i];
+                        cv[i] = cv[ixj];
+                        cv[ixj] = t;
+                    }
+                }
+            }
+            g.sync();
+        }
+    }
+    for (int i = g.gl; i < n; i += G) {
+        out_ci[base + i] = ck[i];
+        stv(out_v, vt, base + i, cv[i]);
+    }
+    g.sync();
+    for (int i = g.gl; i < P2; i += G) {
+        ck[i] = kEmpty;
+        cv[i] = 0.0;
+    }
+    g.sync();
+}
+
+// Warp-aggregated booking of n (group leaders contribute) in the upper-bound
+// space: one atomic per warp.  Returns the group's offset, or -1 when the
+// space is exhausted.  Every lane of the warp must call it.
+template <int G>
+__device__ __forceinline__ long long book_warp(const Group<G>& g, bool contributes, int n,
+                                               unsigned long long* cursor,
+                                               unsigned long long cap, unsigned* err) {
+    const int lane = threadIdx.x & 31;
+    const unsigned long long mine = (contributes && g.gl == 0) ? static_cast<unsigned long long>(n) : 0ull;
+    unsigned long long incl = mine;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        const unsigned long long v = __shfl_up_sync(0xffffffffu, incl, o);
+        if (lane >= o) incl += v;
+    }
+    const unsigned long long total = __shfl_sync(0xffffffffu, incl, 31);
+    unsigned long long wbase = 0;
+    if (lane == 0 && total) wbase = atomicAdd(cursor, total);
+    wbase = __shfl_sync(0xffffffffu, wbase, 0);
+    if (wbase + total > cap) {
+        if (lane == 0 && total) atomicOr(err, kErrBook);
+        return -1;
+    }
+    const unsigned long long off = g.bcast(wbase + incl - mine, 0);
+    return static_cast<long long>(off);
+}
+
+template <int G>
+__device__ __forceinline__ void retry_row(const Group<G>& g, const RowParams& p, int row) {
+    if (g.gl != 0) return;
+    if (p.retry_rows) {
+        const int pos = atomicAdd(p.retry_count, 1);
+        p.retry_rows[pos] = row;
+    } else {
+        atomicOr(p.err, kErrTable);
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Direct R*A*P.  Per-group region (numeric): vals1[S1] vals2[S2] keys1[S1]
+// keys2[S2] ord1[S1] ord2[S2]; symbolic: keys1 keys2 ord1 ord2.
+template <int G, int MODE>
+__global__ void __launch_bounds__(256) k_direct_rows(DirectRowArgs a, RowParams p) {
+    constexpr bool NUM = MODE != kSymb;
+    constexpr int EP = G <= 4 ? 2 : (G <= 8 ? 1 : 0);
+    extern __shared__ __align__(16) unsigned char smem[];
+    const Group<G> g;
+    const int gpc = blockDim.x / G;
+    const int gid = threadIdx.x / G;
+    const int S1 = p.S1, S2 = p.S2;
+    const long long bytes = static_cast<long long>(NUM ? 16 : 8) * (S1 + S2);
+    unsigned char* region = p.gtab
+        ? p.gtab + (static_cast<long long>(blockIdx.x) * gpc + gid) * p.gstride
+        : smem + static_cast<long long>(gid) * bytes;
+    double* vals1 = reinterpret_cast<double*>(region);
+    double* vals2 = vals1 + S1;
+    int* keys1 = NUM ? reinterpret_cast<int*>(vals2 + S2) : reinterpret_cast<int*>(region);
+    int* keys2 = keys1 + S1;
+    int* ord1 = reinterpret_cast<int*>(keys2 + S2);
+    int* ord2 = ord1 + S1;
+    const Acc<G, NUM> T1{keys1, vals1, ord1, static_cast<unsigned>(S1 - 1),
+                         32 - ilog2_pow2(static_cast<unsigned>(S1)), table_limit(S1, G)};
+    const Acc<G, NUM> T2{keys2, vals2, ord2, static_cast<unsigned>(S2 - 1),
+                         32 - ilog2_pow2(static_cast<unsigned>(S2)), table_limit(S2, G)};
+    clear_all<G, NUM>(g, keys1, vals1, S1);
+    clear_all<G, NUM>(g, keys2, vals2, S2);
+    g.sync();
+
+    const int gpw = 32 / G;
+    const long long warps = static_cast<long long>(gridDim.x) * (blockDim.x >> 5);
+    const long long wid = static_cast<long long>(blockIdx.x) * (blockDim.x >> 5) + (threadIdx.x >> 5);
+    for (long long wbase = wid * gpw; wbase < p.nrows; wbase += warps * gpw) {
+        const long long it = wbase + ((threadIdx.x & 31) / G);
+        const bool has = it < p.nrows;
+        const int row = has ? p.rows[it] : 0;
+        bool ok = false;
+        int n2 = 0;
+        if (has) {
+            const int rb = __ldg(a.R.rp + row);
+            const LeftG L1{a.R.ci, a.R.v, a.R.vtype, rb, __ldg(a.R.rp + row + 1) - rb};
+            bool fail = false;
+            const int n1 = accumulate<G, EP, NUM>(g, L1, a.A.rp, a.A.ci, a.A.v, a.A.vtype, T1, fail);
+            g.sync();
+            if (!fail) {
+                const LeftT L2{keys1, vals1, ord1, n1};
+                n2 = accumulate<G, EP, NUM>(g, L2, a.P.rp, a.P.ci, a.P.v, a.P.vtype, T2, fail);
+                g.sync();
+            }
+            clear_listed<G, NUM>(g, T1, n1);
+            g.sync();
+            if (fail) {
+                clear_listed<G, NUM>(g, T2, n2);
+                retry_row(g, p, row);
+                g.sync();
+            } else {
+                ok = true;
+                if constexpr (NUM) {
+                    extract(g, T2, n2, keys1, vals1);   // H1 is free: sort scratch
+                } else {
+                    if (g.gl == 0) {
+                        p.row_cnt[row] = n2;
+                        if (p.row_cnt1) p.row_cnt1[row] = n1;
+                    }
+                    clear_listed<G, NUM>(g, T2, n2);
+                }
+                g.sync();
+            }
+        }
+        if (NUM) {
+            long long base = -1;
+            if (MODE == kNumBook) {
+                base = book_warp(g, ok, n2, p.cursor, p.cap, p.err);
+                if (ok && base >= 0 && g.gl == 0) {
+                    p.row_off[row] = base;
+                    p.row_cnt[row] = n2;
+                }
+            } else if (ok) {
+                base = p.c_rp[row];
+                if (p.c_rp[row + 1] - base != n2) {
+                    if (g.gl == 0) atomicOr(p.err, kErrCount);
+                    base = -1;
+                }
+            }
+            if (ok) {
+                if (base >= 0) {
+                    int* oc = MODE == kNumBook ? p.ub_ci : p.c_ci;
+                    void* ov = MODE == kNumBook ? p.ub_v : p.c_v;
+                    sorted_write(g, keys1, vals1, n2, oc, ov, p.c_vt, base);
+                } else {
+                    for (int i = g.gl; i < n2; i += G) {
+                        keys1[i] = kEmpty;
+                        vals1[i] = 0.0;
+                    }
+                    g.sync();
+                }
+            }
+        }
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Pair-wise A*B.  Region (numeric): vals[S] cv[S] keys[S] ck[S] ord[S];
+// symbolic: keys[S] ord[S].
+template <int G, int MODE>
+__global__ void __launch_bounds__(256) k_pair_rows(PairRowArgs a, RowParams p) {
+    constexpr bool NUM = MODE != kSymb;
+    constexpr int EP = G <= 4 ? 2 : (G <= 8 ? 1 : 0);
+    extern __shared__ __align__(16) unsigned char smem[];
+    const Group<G> g;
+    const int gpc = blockDim.x / G;
+    const int gid = threadIdx.x / G;
+    const int S = p.S1;
+    const long long bytes = static_cast<long long>(NUM ? 28 : 8) * S;
+    unsigned char* region = p.gtab
+        ? p.gtab + (static_cast<long long>(blockIdx.x) * gpc + gid) * p.gstride
+        : smem + static_cast<long long>(gid) * bytes;
+    double* vals = reinterpret_cast<double*>(region);
+    double* cv = vals + S;
+    int* keys = NUM ? reinterpret_cast<int*>(cv + S) : reinterpret_cast<int*>(region);
+    int* ck = NUM ? keys + S : nullptr;
+    int* ord = reinterpret_cast<int*>(NUM ? ck + S : keys + S);
+    const Acc<G, NUM> T{keys, vals, ord, static_cast<unsigned>(S - 1),
+                        32 - ilog2_pow2(static_cast<unsigned>(S)), table_limit(S, G)};
+    clear_all<G, NUM>(g, keys, vals, S);
+    if (NUM) clear_all<G, NUM>(g, ck, cv, S);
+    g.sync();
+
+    const int gpw = 32 / G;
+    const long long warps = static_cast<long long>(gridDim.x) * (blockDim.x >> 5);
+    const long long wid = static_cast<long long>(blockIdx.x) * (blockDim.x >> 5) + (threadIdx.x >> 5);
+    for (long long wbase = wid * gpw; wbase < p.nrows; wbase += warps * gpw) {
+        const long long it = wbase + ((threadIdx.x & 31) / G);
+        const bool has = it < p.nrows;
+        const int row = has ? p.rows[it] : 0;
+        bool ok = false;
+        int n = 0;
+        if (has) {
+            const int ab = __ldg(a.A.rp + row);
+            const LeftG L{a.A.ci, a.A.v, a.A.vtype, ab, __ldg(a.A.rp + row + 1) - ab};
+            bool fail = false;
+            n = accumulate<G, EP, NUM>(g, L, a.B.rp, a.B.ci, a.B.v, a.B.vtype, T, fail);
+            g.sync();
+            if (fail) {
+                clear_listed<G, NUM>(g, T, n);
+                retry_row(g, p, row);
+                g.sync();
+            } else {
+                ok = true;
+                if constexpr (NUM) {
+                    extract(g, T, n, ck, cv);
+                } else {
+                    if (g.gl == 0) p.row_cnt[row] = n;
+                    clear_listed<G, NUM>(g, T, n);
+                }
+                g.sync();
+            }
+        }
+        if (NUM) {
+            long long base = -1;
+            if (MODE == kNumBook) {
+                base = book_warp(g, ok, n, p.cursor, p.cap, p.err);
+                if (ok && base >= 0 && g.gl == 0) {
+                    p.row_off[row] = base;
+                    p.row_cnt[row] = n;
+                }
+            } else if (ok) {
+                base = p.c_rp[row];
+                if (p.c_rp[row + 1] - base != n) {
+                    if (g.gl == 0) atomicOr(p.err, kErrCount);
+                    base = -1;
+                }
+            }
+            if (ok) {
+                if (base >= 0) {
+                    int* oc = MODE == kNumBook ? p.ub_ci : p.c_ci;
+                    void* ov = MODE == kNumBook ? p.ub_v : p.c_v;
+                    sorted_write(g, ck, cv, n, oc, ov, p.c_vt, base);
+                } else {
+                    for (int i = g.gl; i < n; i += G) {
+                        ck[i] = kEmpty;
+                        cv[i] = 0.0;
+                    }
+                    g.sync();
+                }
+            }
+        }
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Host side.
+
+size_t row_table_bytes(bool direct, int mode, int S1, int S2) {
+    const bool num = mode != kSymb;
+    if (direct) return static_cast<size_t>(num ? 16 : 8) * (S1 + S2);
+    return static_cast<size_t>(num ? 28 : 8) * S1;
+}
+
+int row_table_limit(int S, int G) { return table_limit(S, G); }
+
+template <int G, int MODE>
+static cudaError_t direct_g(const DirectRowArgs& a, const RowParams& p, const RowGeom& geo,
+                            cudaStream_t st) {
+    auto k = k_direct_rows<G, MODE>;
+    if (geo.smem > 48 * 1024) {
+        cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                             static_cast<int>(geo.smem));
+        if (e != cudaSuccess) return e;
+    }
+    k<<<geo.grid, geo.block, geo.smem, st>>>(a, p);
+    return cudaGetLastError();
+}
+
+template <int G, int MODE>
+static cudaError_t pair_g(const PairRowArgs& a, const RowParams& p, const RowGeom& geo,
+                          cudaStream_t st) {
+    auto k = k_pair_rows<G, MODE>;
+    if (geo.smem > 48 * 1024) {
+        cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                             static_cast<int>(geo.smem));
+        if (e != cudaSuccess) return e;
+    }
+    k<<<geo.grid, geo.block, geo.smem, st>>>(a, p);
+    return cudaGetLastError();
+}
+
+#define SP3MM_G_SWITCH(G, CALL)                          \
+    switch (G) {                                         \
+        case 4: { constexpr int GG = 4; return CALL; }   \
+        case 8: { constexpr int GG = 8; return CALL; }   \
+        case 16: { constexpr int GG = 16; return CALL; } \
+        default: { constexpr int GG = 32; return CALL; } \
+    }
+
+cudaError_t launch_direct_rows(const DirectRowArgs& a, const RowParams& p, int mode,
+                               const RowGeom& geo, cudaStream_t st) {
+    if (p.nrows <= 0) return cudaSuccess;
+    note_launch();
+    if (mode == kSymb) SP3MM_G_SWITCH(geo.G, (direct_g<GG, kSymb>(a, p, geo, st)));
+    if (mode == kNumExact) SP3MM_G_SWITCH(geo.G, (direct_g<GG, kNumExact>(a, p, geo, st)));
+    SP3MM_G_SWITCH(geo.G, (direct_g<GG, kNumBook>(a, p, geo, st)));
+}
+
+cudaError_t launch_pair_rows(const PairRowArgs& a, const RowParams& p, int mode,
+                             const RowGeom& geo, cudaStream_t st) {
+    if (p.nrows <= 0) return cudaSuccess;
+    note_launch();
+    if (mode == kSymb) SP3MM_G_SWITCH(geo.G, (pair_g<GG, kSymb>(a, p, geo, st)));
+    if (mode == kNumExact) SP3MM_G_SWITCH(geo.G, (pair_g<GG, kNumExact>(a, p, geo, st)));
+    SP3MM_G_SWITCH(geo.G, (pair_g<GG, kNumBook>(a, p, geo, st)));
+}
+
+}  // namespace sp3mm

@@ -130,6 +130,28 @@ def test_random_rectangular_all_variants(orc, seed):
             assert_same(ctx.rap(dR, dA, dP, S.PAIR_RIGHT, fl).download(), right)
 
 
+@pytest.mark.parametrize("lanes", [4, 8, 16, 32])
+def test_results_do_not_depend_on_tuning(golden, orc, lanes):
+    # Every lanes-per-row instantiation, and table shifts from generous to
+    # tiny (d1 = 8 forces nearly every row through the overflow/retry path).
+    g = golden["poisson2d_64_agg2"]
+    R, A, P = _random_triple(7)
+    want_r = (orc.sp3mm_pair(R, A, P), orc.sp3mm_direct(R, A, P))
+    with S.Context() as ctx:
+        for d1, d2 in ((0, 0), (1, 1), (3, 2), (8, 4)):
+            ctx.set_tuning(lanes, d1, d2)
+            for (r, a, p), (pair, direct) in (((g["R"], g["A"], g["P"]), (g["pair"], g["direct"])),
+                                              ((R, A, P), want_r)):
+                dR, dA, dP = ctx.upload(r), ctx.upload(a), ctx.upload(p)
+                for fl in (S.UB, S.SYMBNUM):
+                    assert_same(ctx.rap(dR, dA, dP, S.PAIR, fl).download(), pair,
+                                what=(lanes, d1, d2, fl, "pair"))
+                    assert_same(ctx.rap(dR, dA, dP, S.DIRECT, fl).download(), direct,
+                                what=(lanes, d1, d2, fl, "direct"))
+                for m in (dR, dA, dP):
+                    m.free()
+
+
 @pytest.mark.parametrize("flavour", [0, 1])
 def test_long_rows_use_large_and_global_tables(orc, flavour):
     # Dense-ish rows push bounds past the shared-memory levels (up to 4096
