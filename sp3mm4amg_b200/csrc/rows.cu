@@ -1,16 +1,22 @@
 // rows.cu -- per-row accumulation kernels of the Sp3MM products (sm_100a).
 //
-// One group of G lanes owns one output row and its hash tables.  The lanes
-// walk the left row one step at a time; within a step they cover the selected
-// right row, whose columns are distinct, so every output entry receives its
-// contributions in ascending left-row position -- the order of the
-// reference's scSparseVectMul_ loop (code/src/include/SpMMUtilsGeneric.h:
-// 39-55) -- with no value atomics, and the values are bit-identical to the
-// reference's.  New keys of a step are ranked by ballot + popc in lane order,
-// which reproduces the first-touch order in which the reference's index map
-// appends them (code/src/include/sparseMatrix.h:85-104); the direct product
-// forwards the R*A row into P in that order
-// (code/src/Sp3MM_CSR_OMP_UB_Generic.c:542-545).
+// One group of G lanes owns one output row and its hash tables; a warp holds
+// 32/G groups.  The lanes walk the left row one step at a time; within a step
+// they cover the selected right row, whose columns are distinct, so every
+// output entry receives its contributions in ascending left-row position --
+// the order of the reference's scSparseVectMul_ loop
+// (code/src/include/SpMMUtilsGeneric.h:39-55) -- with no value atomics, and
+// the values are bit-identical to the reference's.  New keys of a step are
+// ranked by ballot + popc in lane order, which reproduces the first-touch
+// order in which the reference's index map appends them
+// (code/src/include/sparseMatrix.h:85-104); the direct product forwards the
+// R*A row into P in that order (code/src/Sp3MM_CSR_OMP_UB_Generic.c:542-545).
+//
+// Warp-synchronous execution: every loop that contains a warp collective runs
+// to a warp-uniform bound (the maximum over the warp's groups) with per-group
+// predicates, and every vote / shuffle / barrier names the full warp.  The
+// groups of a warp therefore issue together; with group-masked barriers they
+// would drift apart and the warp would run its groups one after another.
 //
 // Latency: the row pointers of the right operand are loaded two chunks of G
 // steps ahead and the right-row entries one chunk ahead, into registers, so
@@ -18,15 +24,17 @@
 // path of the sequential accumulation.
 //
 // Table sizes are runtime powers of two.  A row whose distinct-key count
-// would pass the table's load limit stops, clears its slots and is appended
-// to a retry list, which a second launch processes with tables sized from a
-// proven bound; results do not depend on the table size.
+// passes the table's load limit stops inserting, clears its slots and is
+// appended to a retry list, which a second launch processes with tables
+// sized from a proven bound; results do not depend on the table size.
 #include <climits>
 
 #include "kernels.cuh"
 #include "sp3mm_internal.cuh"
 
 namespace sp3mm {
+
+constexpr unsigned kFull = 0xffffffffu;
 
 __device__ __forceinline__ double ldv(const void* p, int vt, long long i) {
     if (vt == SP3MM_F32) return static_cast<double>(__ldg(static_cast<const float*>(p) + i));
@@ -37,12 +45,19 @@ __device__ __forceinline__ void stv(void* p, int vt, long long i, double v) {
     else static_cast<double*>(p)[i] = v;
 }
 
+template <int G> __device__ __forceinline__ int wshfl(int v, int j) {
+    return __shfl_sync(kFull, v, j, G);
+}
+template <int G> __device__ __forceinline__ double wshfl(double v, int j) {
+    return __shfl_sync(kFull, v, j, G);
+}
+
 // Left row in global memory: entries [b, b+n) of (ci, v).
 struct LeftG {
     const int* ci;
     const void* v;
     int vt;
-    int b, n;
+    int b;
     __device__ __forceinline__ int key(int t) const { return __ldg(ci + b + t); }
     __device__ __forceinline__ double val(int t) const { return ldv(v, vt, b + t); }
 };
@@ -51,20 +66,19 @@ struct LeftT {
     const int* keys;
     const double* vals;
     const int* ord;
-    int n;
     __device__ __forceinline__ int key(int t) const { return keys[ord[t]]; }
     __device__ __forceinline__ double val(int t) const { return vals[ord[t]]; }
 };
 
 // Distinct keys a table of S slots accepts before the row is retried: at
-// most G keys arrive per sub-step, so the table never fills, and the load
-// factor stays <= 7/8.
+// most G keys arrive per sub-step and a group stops inserting once it passed
+// the limit, so the table never fills; the load factor stays <= 7/8.
 __host__ __device__ __forceinline__ int table_limit(int S, int G) {
     const int a = S - G - 1, b = (7 * S) / 8;
     return a < b ? a : b;
 }
 
-template <int G, bool NUM>
+template <bool NUM>
 struct Acc {
     int* keys;
     double* vals;
@@ -74,37 +88,38 @@ struct Acc {
     int limit;
 };
 
-// One sub-step: lanes with `act` add prod = bv*s into key c.  Returns false
-// (group-uniformly) when the distinct count passed the limit.
+// One sub-step for the whole warp: lanes with `act` add bv*s into key c.
+// `live` (group-uniform) turns false once the group passed its table limit.
 template <int G, bool NUM>
-__device__ __forceinline__ bool sub_step(const Group<G>& g, const Acc<G, NUM>& T, bool act,
-                                         int c, double bv, double s, int& nk) {
+__device__ __forceinline__ void sub_step(const Group<G>& g, const Acc<NUM>& T, bool act, int c,
+                                         double bv, double s, int& nk, bool& live) {
     bool is_new = false;
     int slot = 0;
-    if (act) {
+    if (act && live) {
         slot = table_insert(T.keys, T.smask, T.shift, c, is_new);
         if (NUM && slot >= 0) T.vals[slot] = __dadd_rn(T.vals[slot], __dmul_rn(bv, s));
     }
-    const unsigned nb = g.ballot(is_new);
+    const unsigned nb = __ballot_sync(kFull, is_new);
     if (is_new) T.ord[nk + __popc(nb & g.below)] = slot;
-    nk += __popc(nb);
-    return nk <= T.limit;
+    nk += __popc(nb & g.mask);
+    if (nk > T.limit) live = false;
 }
 
-// Accumulate sum_t L.val(t) * B(L.key(t), :) in ascending t.  Returns the
-// distinct-key count; `fail` when the table limit was passed.
+// Accumulate sum_{t<n} L.val(t) * B(L.key(t), :) in ascending t; n is this
+// group's left-row length (0 for an idle group).  Every lane of the warp
+// must call it.  Returns the distinct-key count; `fail` when the group
+// passed its table limit.
 template <int G, int EP, bool NUM, class Left>
-__device__ __forceinline__ int accumulate(const Group<G>& g, const Left& L,
+__device__ __forceinline__ int accumulate(const Group<G>& g, const Left& L, int n,
                                           const int* __restrict__ b_rp,
                                           const int* __restrict__ b_ci, const void* b_v,
-                                          int b_vt, const Acc<G, NUM>& T, bool& fail) {
-    const int n = L.n;
+                                          int b_vt, const Acc<NUM>& T, bool& fail) {
     int nk = 0;
-    if (n <= 0) return 0;
+    bool live = n > 0;
+    const int nmax = __reduce_max_sync(kFull, n);
+    if (nmax == 0) return 0;
 
-    // Pointers of chunk c (lane j <-> step c*G + j) and c+1.
-    int pb0 = 0, pe0 = 0, pb1 = 0, pe1 = 0;
-    double ps0 = 0.0, ps1 = 0.0;
+    // Row pointers and scalar of step t0 + gl (lane j <-> step t0 + j).
     auto load_ptrs = [&](int t0, int& pb, int& pe, double& ps) {
         const int t = t0 + g.gl;
         pb = 0;
@@ -124,7 +139,7 @@ __device__ __forceinline__ int accumulate(const Group<G>& g, const Left& L,
     auto load_entries = [&](int pb, int pe, int (&ec)[G][EPA], double (&ev)[G][EPA]) {
 #pragma unroll
         for (int j = 0; j < G; ++j) {
-            const int jb = g.bcast(pb, j), je = g.bcast(pe, j);
+            const int jb = wshfl<G>(pb, j), je = wshfl<G>(pe, j);
 #pragma unroll
             for (int m = 0; m < EP; ++m) {
                 const int e = jb + m * G + g.gl;
@@ -138,32 +153,30 @@ __device__ __forceinline__ int accumulate(const Group<G>& g, const Left& L,
         }
     };
 
+    int pb0, pe0, pb1, pe1;
+    double ps0, ps1;
     load_ptrs(0, pb0, pe0, ps0);
     load_ptrs(G, pb1, pe1, ps1);
-    load_entries(pb0, pe0, ec0, ev0);
-    for (int base = 0; base < n; base += G) {
-        load_entries(pb1, pe1, ec1, ev1);
+    if constexpr (EP > 0) load_entries(pb0, pe0, ec0, ev0);
+    for (int base = 0; base < nmax; base += G) {
+        if constexpr (EP > 0) load_entries(pb1, pe1, ec1, ev1);
         int pb2, pe2;
         double ps2;
         load_ptrs(base + 2 * G, pb2, pe2, ps2);
-        const int cnt = min(G, n - base);
 #pragma unroll
         for (int j = 0; j < G; ++j) {
-            if (j < cnt) {
-                const int jb = g.bcast(pb0, j), je = g.bcast(pe0, j);
-                const double js = NUM ? g.bcast(ps0, j) : 0.0;
+            if (base + j < nmax) {
+                const int jb = wshfl<G>(pb0, j), je = wshfl<G>(pe0, j);
+                const double js = NUM ? wshfl<G>(ps0, j) : 0.0;
 #pragma unroll
                 for (int m = 0; m < EP; ++m) {
-                    if (jb + m * G < je) {
+                    if (__any_sync(kFull, jb + m * G < je)) {
                         const bool act = jb + m * G + g.gl < je;
-                        if (!sub_step<G, NUM>(g, T, act, ec0[j][m], ev0[j][m], js, nk)) {
-                            fail = true;
-                            return nk;
-                        }
+                        sub_step<G, NUM>(g, T, act, ec0[j][m], ev0[j][m], js, nk, live);
                     }
                 }
                 // Right rows longer than EP*G: the rest is loaded in place.
-                for (int e0 = jb + EP * G; e0 < je; e0 += G) {
+                for (int e0 = jb + EP * G; __any_sync(kFull, e0 < je); e0 += G) {
                     const int e = e0 + g.gl;
                     const bool act = e < je;
                     int c = -1;
@@ -172,12 +185,9 @@ __device__ __forceinline__ int accumulate(const Group<G>& g, const Left& L,
                         c = __ldg(b_ci + e);
                         if (NUM) bv = ldv(b_v, b_vt, e);
                     }
-                    if (!sub_step<G, NUM>(g, T, act, c, bv, js, nk)) {
-                        fail = true;
-                        return nk;
-                    }
+                    sub_step<G, NUM>(g, T, act, c, bv, js, nk, live);
                 }
-                g.sync();
+                __syncwarp();
             }
         }
         pb0 = pb1;
@@ -186,20 +196,23 @@ __device__ __forceinline__ int accumulate(const Group<G>& g, const Left& L,
         pb1 = pb2;
         pe1 = pe2;
         ps1 = ps2;
+        if constexpr (EP > 0) {
 #pragma unroll
-        for (int j = 0; j < G; ++j)
+            for (int j = 0; j < G; ++j)
 #pragma unroll
-            for (int m = 0; m < EP; ++m) {
-                ec0[j][m] = ec1[j][m];
-                ev0[j][m] = ev1[j][m];
-            }
+                for (int m = 0; m < EP; ++m) {
+                    ec0[j][m] = ec1[j][m];
+                    ev0[j][m] = ev1[j][m];
+                }
+        }
     }
+    fail = n > 0 && !live;
     return nk;
 }
 
 // Clear the slots listed in ord[0..n).
 template <int G, bool NUM>
-__device__ __forceinline__ void clear_listed(const Group<G>& g, const Acc<G, NUM>& T, int n) {
+__device__ __forceinline__ void clear_listed(const Group<G>& g, const Acc<NUM>& T, int n) {
     for (int i = g.gl; i < n; i += G) {
         const int s = T.ord[i];
         T.keys[s] = kEmpty;
@@ -217,7 +230,7 @@ __device__ __forceinline__ void clear_all(const Group<G>& g, int* keys, double* 
 
 // Move the n listed entries of T into (ck, cv)[0..n), clearing T.
 template <int G>
-__device__ __forceinline__ void extract(const Group<G>& g, const Acc<G, true>& T, int n, int* ck,
+__device__ __forceinline__ void extract(const Group<G>& g, const Acc<true>& T, int n, int* ck,
                                         double* cv) {
     for (int i = g.gl; i < n; i += G) {
         const int s = T.ord[i];
@@ -228,15 +241,20 @@ __device__ __forceinline__ void extract(const Group<G>& g, const Acc<G, true>& T
     }
 }
 
-// Write (ck, cv)[0..n) in ascending key order to out[base..].  Rows up to 64
-// entries: rank sort with each lane's keys cached in registers.  Longer rows:
-// bitonic sort in place (ck/cv hold next_pow2(n) slots), then a linear copy.
-// On return ck[0..n) / cv[0..n) are reset to kEmpty / 0.
+// Write (ck, cv)[0..n) in ascending key order to out[base..] for every group
+// with base >= 0 (n = 0 for idle groups).  Every lane of the warp must call
+// it.  Rows up to 64 entries: rank sort with each lane's keys cached in
+// registers.  Longer rows: bitonic sort in place (ck/cv hold
+// next_pow2(max n) slots), then a linear copy.  On return ck / cv are reset
+// to kEmpty / 0 where they were used.
 template <int G>
 __device__ __forceinline__ void sorted_write(const Group<G>& g, int* ck, double* cv, int n,
                                              int* out_ci, void* out_v, int vt, long long base) {
+    const bool writes = base >= 0;
+    const int nmax = __reduce_max_sync(kFull, n);
+    if (nmax == 0) return;
     constexpr int RM = 64 / G;
-    if (n <= 64) {
+    if (nmax <= 64) {
         int mk[RM], rk[RM];
 #pragma unroll
         for (int m = 0; m < RM; ++m) {
@@ -244,20 +262,20 @@ __device__ __forceinline__ void sorted_write(const Group<G>& g, int* ck, double*
             mk[m] = i < n ? ck[i] : INT_MAX;
             rk[m] = 0;
         }
-        for (int j = 0; j < n; ++j) {
-            const int kj = ck[j];
+        for (int j = 0; j < nmax; ++j) {
+            const int kj = j < n ? ck[j] : INT_MAX;
 #pragma unroll
             for (int m = 0; m < RM; ++m) rk[m] += kj < mk[m];
         }
 #pragma unroll
         for (int m = 0; m < RM; ++m) {
             const int i = g.gl + m * G;
-            if (i < n) {
+            if (i < n && writes) {
                 out_ci[base + rk[m]] = mk[m];
                 stv(out_v, vt, base + rk[m], cv[i]);
             }
         }
-        g.sync();
+        __syncwarp();
 #pragma unroll
         for (int m = 0; m < RM; ++m) {
             const int i = g.gl + m * G;
@@ -266,12 +284,12 @@ __device__ __forceinline__ void sorted_write(const Group<G>& g, int* ck, double*
                 cv[i] = 0.0;
             }
         }
-        g.sync();
+        __syncwarp();
         return;
     }
-    const int P2 = static_cast<int>(next_pow2(static_cast<unsigned>(n)));
+    const int P2 = static_cast<int>(next_pow2(static_cast<unsigned>(nmax)));
     for (int i = n + g.gl; i < P2; i += G) ck[i] = INT_MAX;
-    g.sync();
+    __syncwarp();
     for (int k = 2; k <= P2; k <<= 1) {
         for (int j = k >> 1; j > 0; j >>= 1) {
             for (int i = g.gl; i < P2; i += G) {
@@ -287,24 +305,27 @@ __device__ __forceinline__ void sorted_write(const Group<G>& g, int* ck, double*
                     }
                 }
             }
-            g.sync();
+            __syncwarp();
         }
     }
-    for (int i = g.gl; i < n; i += G) {
-        out_ci[base + i] = ck[i];
-        stv(out_v, vt, base + i, cv[i]);
+    if (writes) {
+        for (int i = g.gl; i < n; i += G) {
+            out_ci[base + i] = ck[i];
+            stv(out_v, vt, base + i, cv[i]);
+        }
     }
-    g.sync();
+    __syncwarp();
     for (int i = g.gl; i < P2; i += G) {
         ck[i] = kEmpty;
         cv[i] = 0.0;
     }
-    g.sync();
+    __syncwarp();
 }
 
 // Warp-aggregated booking of n (group leaders contribute) in the upper-bound
 // space: one atomic per warp.  Returns the group's offset, or -1 when the
-// space is exhausted.  Every lane of the warp must call it.
+// space is exhausted or the group does not contribute.  Every lane of the
+// warp must call it.
 template <int G>
 __device__ __forceinline__ long long book_warp(const Group<G>& g, bool contributes, int n,
                                                unsigned long long* cursor,
@@ -314,19 +335,19 @@ __device__ __forceinline__ long long book_warp(const Group<G>& g, bool contribut
     unsigned long long incl = mine;
 #pragma unroll
     for (int o = 1; o < 32; o <<= 1) {
-        const unsigned long long v = __shfl_up_sync(0xffffffffu, incl, o);
+        const unsigned long long v = __shfl_up_sync(kFull, incl, o);
         if (lane >= o) incl += v;
     }
-    const unsigned long long total = __shfl_sync(0xffffffffu, incl, 31);
+    const unsigned long long total = __shfl_sync(kFull, incl, 31);
     unsigned long long wbase = 0;
     if (lane == 0 && total) wbase = atomicAdd(cursor, total);
-    wbase = __shfl_sync(0xffffffffu, wbase, 0);
+    wbase = __shfl_sync(kFull, wbase, 0);
     if (wbase + total > cap) {
         if (lane == 0 && total) atomicOr(err, kErrBook);
         return -1;
     }
-    const unsigned long long off = g.bcast(wbase + incl - mine, 0);
-    return static_cast<long long>(off);
+    const unsigned long long off = __shfl_sync(kFull, wbase + incl - mine, 0, G);
+    return contributes ? static_cast<long long>(off) : -1;
 }
 
 template <int G>
@@ -338,6 +359,28 @@ __device__ __forceinline__ void retry_row(const Group<G>& g, const RowParams& p,
     } else {
         atomicOr(p.err, kErrTable);
     }
+}
+
+// Output offset of an accumulated row (all lanes of the warp call it):
+// booking in the upper-bound space, or the exact row pointer.
+template <int G, int MODE>
+__device__ __forceinline__ long long out_base(const Group<G>& g, const RowParams& p, bool ok,
+                                              int row, int n) {
+    if (MODE == kNumBook) {
+        const long long b = book_warp(g, ok, n, p.cursor, p.cap, p.err);
+        if (ok && b >= 0 && g.gl == 0) {
+            p.row_off[row] = b;
+            p.row_cnt[row] = n;
+        }
+        return b;
+    }
+    if (!ok) return -1;
+    const long long b = p.c_rp[row];
+    if (p.c_rp[row + 1] - b != n) {
+        if (g.gl == 0) atomicOr(p.err, kErrCount);
+        return -1;
+    }
+    return b;
 }
 
 // ---------------------------------------------------------------------------
@@ -360,15 +403,15 @@ __global__ void __launch_bounds__(256) k_direct_rows(DirectRowArgs a, RowParams 
     double* vals2 = vals1 + S1;
     int* keys1 = NUM ? reinterpret_cast<int*>(vals2 + S2) : reinterpret_cast<int*>(region);
     int* keys2 = keys1 + S1;
-    int* ord1 = reinterpret_cast<int*>(keys2 + S2);
+    int* ord1 = keys2 + S2;
     int* ord2 = ord1 + S1;
-    const Acc<G, NUM> T1{keys1, vals1, ord1, static_cast<unsigned>(S1 - 1),
-                         32 - ilog2_pow2(static_cast<unsigned>(S1)), table_limit(S1, G)};
-    const Acc<G, NUM> T2{keys2, vals2, ord2, static_cast<unsigned>(S2 - 1),
-                         32 - ilog2_pow2(static_cast<unsigned>(S2)), table_limit(S2, G)};
+    const Acc<NUM> T1{keys1, vals1, ord1, static_cast<unsigned>(S1 - 1),
+                      32 - ilog2_pow2(static_cast<unsigned>(S1)), table_limit(S1, G)};
+    const Acc<NUM> T2{keys2, vals2, ord2, static_cast<unsigned>(S2 - 1),
+                      32 - ilog2_pow2(static_cast<unsigned>(S2)), table_limit(S2, G)};
     clear_all<G, NUM>(g, keys1, vals1, S1);
     clear_all<G, NUM>(g, keys2, vals2, S2);
-    g.sync();
+    __syncwarp();
 
     const int gpw = 32 / G;
     const long long warps = static_cast<long long>(gridDim.x) * (blockDim.x >> 5);
@@ -377,67 +420,46 @@ __global__ void __launch_bounds__(256) k_direct_rows(DirectRowArgs a, RowParams 
         const long long it = wbase + ((threadIdx.x & 31) / G);
         const bool has = it < p.nrows;
         const int row = has ? p.rows[it] : 0;
-        bool ok = false;
-        int n2 = 0;
+        int rb = 0, rlen = 0;
         if (has) {
-            const int rb = __ldg(a.R.rp + row);
-            const LeftG L1{a.R.ci, a.R.v, a.R.vtype, rb, __ldg(a.R.rp + row + 1) - rb};
-            bool fail = false;
-            const int n1 = accumulate<G, EP, NUM>(g, L1, a.A.rp, a.A.ci, a.A.v, a.A.vtype, T1, fail);
-            g.sync();
-            if (!fail) {
-                const LeftT L2{keys1, vals1, ord1, n1};
-                n2 = accumulate<G, EP, NUM>(g, L2, a.P.rp, a.P.ci, a.P.v, a.P.vtype, T2, fail);
-                g.sync();
-            }
-            clear_listed<G, NUM>(g, T1, n1);
-            g.sync();
-            if (fail) {
-                clear_listed<G, NUM>(g, T2, n2);
-                retry_row(g, p, row);
-                g.sync();
+            rb = __ldg(a.R.rp + row);
+            rlen = __ldg(a.R.rp + row + 1) - rb;
+        }
+        // Phase 1: the R*A row, first-touch order in ord1.
+        bool fail1 = false, fail2 = false;
+        const LeftG L1{a.R.ci, a.R.v, a.R.vtype, rb};
+        const int n1 = accumulate<G, EP, NUM>(g, L1, rlen, a.A.rp, a.A.ci, a.A.v, a.A.vtype, T1,
+                                              fail1);
+        __syncwarp();
+        // Phase 2: forward the R*A row into P in first-touch order.
+        const LeftT L2{keys1, vals1, ord1};
+        const int n2 = accumulate<G, EP, NUM>(g, L2, fail1 ? 0 : n1, a.P.rp, a.P.ci, a.P.v,
+                                              a.P.vtype, T2, fail2);
+        __syncwarp();
+        clear_listed<G, NUM>(g, T1, n1);
+        __syncwarp();
+        const bool fail = fail1 || fail2;
+        const bool ok = has && !fail;
+        if (fail) {
+            clear_listed<G, NUM>(g, T2, n2);
+            retry_row(g, p, row);
+        } else if (ok) {
+            if constexpr (NUM) {
+                extract(g, T2, n2, keys1, vals1);   // H1 is free: sort scratch
             } else {
-                ok = true;
-                if constexpr (NUM) {
-                    extract(g, T2, n2, keys1, vals1);   // H1 is free: sort scratch
-                } else {
-                    if (g.gl == 0) {
-                        p.row_cnt[row] = n2;
-                        if (p.row_cnt1) p.row_cnt1[row] = n1;
-                    }
-                    clear_listed<G, NUM>(g, T2, n2);
+                if (g.gl == 0) {
+                    p.row_cnt[row] = n2;
+                    if (p.row_cnt1) p.row_cnt1[row] = n1;
                 }
-                g.sync();
+                clear_listed<G, NUM>(g, T2, n2);
             }
         }
-        if (NUM) {
-            long long base = -1;
-            if (MODE == kNumBook) {
-                base = book_warp(g, ok, n2, p.cursor, p.cap, p.err);
-                if (ok && base >= 0 && g.gl == 0) {
-                    p.row_off[row] = base;
-                    p.row_cnt[row] = n2;
-                }
-            } else if (ok) {
-                base = p.c_rp[row];
-                if (p.c_rp[row + 1] - base != n2) {
-                    if (g.gl == 0) atomicOr(p.err, kErrCount);
-                    base = -1;
-                }
-            }
-            if (ok) {
-                if (base >= 0) {
-                    int* oc = MODE == kNumBook ? p.ub_ci : p.c_ci;
-                    void* ov = MODE == kNumBook ? p.ub_v : p.c_v;
-                    sorted_write(g, keys1, vals1, n2, oc, ov, p.c_vt, base);
-                } else {
-                    for (int i = g.gl; i < n2; i += G) {
-                        keys1[i] = kEmpty;
-                        vals1[i] = 0.0;
-                    }
-                    g.sync();
-                }
-            }
+        __syncwarp();
+        if constexpr (NUM) {
+            const long long base = out_base<G, MODE>(g, p, ok, row, n2);
+            int* oc = MODE == kNumBook ? p.ub_ci : p.c_ci;
+            void* ov = MODE == kNumBook ? p.ub_v : p.c_v;
+            sorted_write(g, keys1, vals1, ok ? n2 : 0, oc, ov, p.c_vt, base);
         }
     }
 }
@@ -462,12 +484,12 @@ __global__ void __launch_bounds__(256) k_pair_rows(PairRowArgs a, RowParams p) {
     double* cv = vals + S;
     int* keys = NUM ? reinterpret_cast<int*>(cv + S) : reinterpret_cast<int*>(region);
     int* ck = NUM ? keys + S : nullptr;
-    int* ord = reinterpret_cast<int*>(NUM ? ck + S : keys + S);
-    const Acc<G, NUM> T{keys, vals, ord, static_cast<unsigned>(S - 1),
-                        32 - ilog2_pow2(static_cast<unsigned>(S)), table_limit(S, G)};
+    int* ord = NUM ? ck + S : keys + S;
+    const Acc<NUM> T{keys, vals, ord, static_cast<unsigned>(S - 1),
+                     32 - ilog2_pow2(static_cast<unsigned>(S)), table_limit(S, G)};
     clear_all<G, NUM>(g, keys, vals, S);
     if (NUM) clear_all<G, NUM>(g, ck, cv, S);
-    g.sync();
+    __syncwarp();
 
     const int gpw = 32 / G;
     const long long warps = static_cast<long long>(gridDim.x) * (blockDim.x >> 5);
@@ -476,57 +498,34 @@ __global__ void __launch_bounds__(256) k_pair_rows(PairRowArgs a, RowParams p) {
         const long long it = wbase + ((threadIdx.x & 31) / G);
         const bool has = it < p.nrows;
         const int row = has ? p.rows[it] : 0;
-        bool ok = false;
-        int n = 0;
+        int ab = 0, alen = 0;
         if (has) {
-            const int ab = __ldg(a.A.rp + row);
-            const LeftG L{a.A.ci, a.A.v, a.A.vtype, ab, __ldg(a.A.rp + row + 1) - ab};
-            bool fail = false;
-            n = accumulate<G, EP, NUM>(g, L, a.B.rp, a.B.ci, a.B.v, a.B.vtype, T, fail);
-            g.sync();
-            if (fail) {
-                clear_listed<G, NUM>(g, T, n);
-                retry_row(g, p, row);
-                g.sync();
+            ab = __ldg(a.A.rp + row);
+            alen = __ldg(a.A.rp + row + 1) - ab;
+        }
+        bool fail = false;
+        const LeftG L{a.A.ci, a.A.v, a.A.vtype, ab};
+        const int n = accumulate<G, EP, NUM>(g, L, alen, a.B.rp, a.B.ci, a.B.v, a.B.vtype, T,
+                                             fail);
+        __syncwarp();
+        const bool ok = has && !fail;
+        if (fail) {
+            clear_listed<G, NUM>(g, T, n);
+            retry_row(g, p, row);
+        } else if (ok) {
+            if constexpr (NUM) {
+                extract(g, T, n, ck, cv);
             } else {
-                ok = true;
-                if constexpr (NUM) {
-                    extract(g, T, n, ck, cv);
-                } else {
-                    if (g.gl == 0) p.row_cnt[row] = n;
-                    clear_listed<G, NUM>(g, T, n);
-                }
-                g.sync();
+                if (g.gl == 0) p.row_cnt[row] = n;
+                clear_listed<G, NUM>(g, T, n);
             }
         }
-        if (NUM) {
-            long long base = -1;
-            if (MODE == kNumBook) {
-                base = book_warp(g, ok, n, p.cursor, p.cap, p.err);
-                if (ok && base >= 0 && g.gl == 0) {
-                    p.row_off[row] = base;
-                    p.row_cnt[row] = n;
-                }
-            } else if (ok) {
-                base = p.c_rp[row];
-                if (p.c_rp[row + 1] - base != n) {
-                    if (g.gl == 0) atomicOr(p.err, kErrCount);
-                    base = -1;
-                }
-            }
-            if (ok) {
-                if (base >= 0) {
-                    int* oc = MODE == kNumBook ? p.ub_ci : p.c_ci;
-                    void* ov = MODE == kNumBook ? p.ub_v : p.c_v;
-                    sorted_write(g, ck, cv, n, oc, ov, p.c_vt, base);
-                } else {
-                    for (int i = g.gl; i < n; i += G) {
-                        ck[i] = kEmpty;
-                        cv[i] = 0.0;
-                    }
-                    g.sync();
-                }
-            }
+        __syncwarp();
+        if constexpr (NUM) {
+            const long long base = out_base<G, MODE>(g, p, ok, row, n);
+            int* oc = MODE == kNumBook ? p.ub_ci : p.c_ci;
+            void* ov = MODE == kNumBook ? p.ub_v : p.c_v;
+            sorted_write(g, ck, cv, ok ? n : 0, oc, ov, p.c_vt, base);
         }
     }
 }
