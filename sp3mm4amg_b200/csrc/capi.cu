@@ -240,6 +240,8 @@ struct RowRunner {
     int mode;
     DirectRowArgs da;
     PairRowArgs pa;
+    // Longest row of the right operands (first / last; -1: unknown).
+    int a_max = -1, b_max = -1;
 
     int launch(RowParams p, int G, DevBuf& gtab) {
         const size_t per_group = row_table_bytes(direct, mode, p.S1, p.S2);
@@ -274,6 +276,9 @@ struct RowRunner {
             geo.smem = 0;
             geo.grid = static_cast<int>(groups / 8);
         }
+        const int cover = row_prefetch_cover(geo.G);
+        p.a_long = a_max < 0 || a_max > cover;
+        p.b_long = b_max < 0 || b_max > cover;
         static const char* const kLabels[2][3] = {
             {"pair.rows.symb", "pair.rows.num", "pair.rows.book"},
             {"direct.rows.symb", "direct.rows.num", "direct.rows.book"}};
@@ -441,6 +446,8 @@ int spmm_impl(sp3mm_ctx* ctx, const sp3mm_dcsr& A, const sp3mm_dcsr& B, int flav
               sp3mm_dcsr* C) {
     if (A.N != B.M)
         return set_error(ctx, SP3MM_EINVAL, "inner dimensions differ (%d vs %d)", A.N, B.M);
+    if (A.val_type != B.val_type)
+        return set_error(ctx, SP3MM_EINVAL, "operands must share one value storage type");
     const int M = A.M;
     const cudaStream_t st = ctx->stream;
     const int G = pick_group(ctx, B.M ? static_cast<double>(B.nnz) / B.M : 1.0);
@@ -453,7 +460,7 @@ int spmm_impl(sp3mm_ctx* ctx, const sp3mm_dcsr& A, const sp3mm_dcsr& B, int flav
     prof(ctx, "pair.bounds", [&] {
         launch_pair_bounds(view(A), view(B), need.as<int>(), &dc->total, st);
     });
-    RowRunner rr{ctx, false, kSymb, {}, PairRowArgs{view(A), view(B)}};
+    RowRunner rr{ctx, false, kSymb, {}, PairRowArgs{view(A), view(B)}, -1, B.max_row};
     return product_rows(ctx, rr, M, B.N, flavour, out_vt, need, dc, G, d1, 0, B.N, 0, 0.0, C);
 }
 
@@ -462,6 +469,8 @@ int direct_impl(sp3mm_ctx* ctx, const sp3mm_dcsr& R, const sp3mm_dcsr& A, const 
                 int flavour, int out_vt, sp3mm_dcsr* C) {
     if (R.N != A.M || A.N != P.M)
         return set_error(ctx, SP3MM_EINVAL, "inner dimensions differ");
+    if (R.val_type != A.val_type || A.val_type != P.val_type)
+        return set_error(ctx, SP3MM_EINVAL, "operands must share one value storage type");
     const int M = R.M;
     const cudaStream_t st = ctx->stream;
     const double mean = std::max(A.M ? static_cast<double>(A.nnz) / A.M : 1.0,
@@ -478,7 +487,8 @@ int direct_impl(sp3mm_ctx* ctx, const sp3mm_dcsr& R, const sp3mm_dcsr& A, const 
     prof(ctx, "direct.bounds", [&] {
         launch_direct_bounds(view(R), view(A), pmax, need.as<int>(), &dc->total, st);
     });
-    RowRunner rr{ctx, true, kSymb, DirectRowArgs{view(R), view(A), view(P)}, {}};
+    RowRunner rr{ctx, true, kSymb, DirectRowArgs{view(R), view(A), view(P)}, {}, A.max_row,
+                 P.max_row};
     return product_rows(ctx, rr, M, P.N, flavour, out_vt, need, dc, G, d1, d2, A.N, P.N,
                         static_cast<double>(pmax), C);
 }
@@ -498,11 +508,13 @@ int rap_impl(sp3mm_ctx* ctx, const sp3mm_dcsr& R, const sp3mm_dcsr& A, const sp3
     if (variant == SP3MM_DIRECT) return direct_impl(ctx, R, A, P, flavour, out_vt, C);
     sp3mm_dcsr T{};
     int rc;
+    // The intermediate is stored in the operands' value type (FP64 operands:
+    // an FP64 intermediate, so the pair is bit-identical to the reference).
     if (variant == SP3MM_PAIR) {
-        TRY(spmm_impl(ctx, R, A, flavour, SP3MM_F64, &T));
+        TRY(spmm_impl(ctx, R, A, flavour, R.val_type, &T));
         rc = spmm_impl(ctx, T, P, flavour, out_vt, C);
     } else if (variant == SP3MM_PAIR_RIGHT) {
-        TRY(spmm_impl(ctx, A, P, flavour, SP3MM_F64, &T));
+        TRY(spmm_impl(ctx, A, P, flavour, A.val_type, &T));
         rc = spmm_impl(ctx, R, T, flavour, out_vt, C);
     } else {
         return set_error(ctx, SP3MM_EINVAL, "unknown variant %d", variant);
@@ -1022,7 +1034,7 @@ int sp3mm_spmm_rowsizes(sp3mm_ctx* ctx, const sp3mm_dcsr* A, const sp3mm_dcsr* B
     const int d1 = ctx->tune_d1 >= 0 ? ctx->tune_d1 : 2;
     Bins bins;
     TRY(bin_rows(ctx, M, need.as<int>(), d1, G, dc, row_cnt.as<int>(), bins));
-    RowRunner rr{ctx, false, kSymb, {}, PairRowArgs{view(*A), view(*B)}};
+    RowRunner rr{ctx, false, kSymb, {}, PairRowArgs{view(*A), view(*B)}, -1, B->max_row};
     RowParams p{};
     p.nrows = M;
     p.row_cnt = row_cnt.as<int>();

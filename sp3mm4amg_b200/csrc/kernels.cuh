@@ -51,6 +51,9 @@ struct RowParams {
     int* ub_ci;
     void* ub_v;
     unsigned* err;
+    // Some row of the first (a_long, direct only) / last (b_long) right
+    // operand is longer than the entries the kernel prefetches per step.
+    bool a_long, b_long;
 };
 
 // Launch geometry of one row-kernel launch.
@@ -62,6 +65,8 @@ struct RowGeom {
 
 size_t row_table_bytes(bool direct, int mode, int S1, int S2);
 int row_table_limit(int S, int G);
+// Right-row entries a G-lane group prefetches per step (0: none).
+int row_prefetch_cover(int G);
 cudaError_t launch_direct_rows(const DirectRowArgs& a, const RowParams& p, int mode,
                                const RowGeom& geo, cudaStream_t st);
 cudaError_t launch_pair_rows(const PairRowArgs& a, const RowParams& p, int mode,

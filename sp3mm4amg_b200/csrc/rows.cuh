@@ -1,4 +1,4 @@
-// rows.cu -- per-row accumulation kernels of the Sp3MM products (sm_100a).
+// rows.cuh -- per-row accumulation kernels of the Sp3MM products (sm_100a).
 //
 // One group of G lanes owns one output row and its hash tables; a warp holds
 // 32/G groups.  The lanes walk the left row one step at a time; within a step
@@ -14,19 +14,24 @@
 //
 // Warp-synchronous execution: every loop that contains a warp collective runs
 // to a warp-uniform bound (the maximum over the warp's groups) with per-group
-// predicates, and every vote / shuffle / barrier names the full warp.  The
-// groups of a warp therefore issue together; with group-masked barriers they
-// would drift apart and the warp would run its groups one after another.
+// predicates, and every vote / shuffle / barrier names the full warp, so the
+// groups of a warp issue together.
 //
 // Latency: the row pointers of the right operand are loaded two chunks of G
-// steps ahead and the right-row entries one chunk ahead, into registers, so
-// the dependent chain left key -> row pointer -> entries is off the critical
-// path of the sequential accumulation.
+// steps ahead and the right-row entries one chunk ahead, into two register
+// buffers used in turn.
+//
+// Value types are template parameters (TV: storage type of every input, TO:
+// of the output; accumulation is always FP64), and the tables live in shared
+// memory except in the GT (global-table) instantiation used for very long
+// rows, so the compiler emits 32-bit shared addressing in the common case.
 //
 // Table sizes are runtime powers of two.  A row whose distinct-key count
 // passes the table's load limit stops inserting, clears its slots and is
 // appended to a retry list, which a second launch processes with tables
 // sized from a proven bound; results do not depend on the table size.
+#pragma once
+
 #include <climits>
 
 #include "kernels.cuh"
@@ -36,13 +41,11 @@ namespace sp3mm {
 
 constexpr unsigned kFull = 0xffffffffu;
 
-__device__ __forceinline__ double ldv(const void* p, int vt, long long i) {
-    if (vt == SP3MM_F32) return static_cast<double>(__ldg(static_cast<const float*>(p) + i));
-    return __ldg(static_cast<const double*>(p) + i);
+template <typename T> __device__ __forceinline__ double ldv(const T* p, long long i) {
+    return static_cast<double>(__ldg(p + i));
 }
-__device__ __forceinline__ void stv(void* p, int vt, long long i, double v) {
-    if (vt == SP3MM_F32) static_cast<float*>(p)[i] = __double2float_rn(v);
-    else static_cast<double*>(p)[i] = v;
+template <typename T> __device__ __forceinline__ void stv(T* p, long long i, double v) {
+    p[i] = static_cast<T>(v);
 }
 
 template <int G> __device__ __forceinline__ int wshfl(int v, int j) {
@@ -53,15 +56,15 @@ template <int G> __device__ __forceinline__ double wshfl(double v, int j) {
 }
 
 // Left row in global memory: entries [b, b+n) of (ci, v).
+template <typename TV>
 struct LeftG {
     const int* ci;
-    const void* v;
-    int vt;
+    const TV* v;
     int b;
     __device__ __forceinline__ int key(int t) const { return __ldg(ci + b + t); }
-    __device__ __forceinline__ double val(int t) const { return ldv(v, vt, b + t); }
+    __device__ __forceinline__ double val(int t) const { return ldv(v, b + t); }
 };
-// Left row held in a shared table, read in the order of `ord` (first touch).
+// Left row held in a table, read in the order of `ord` (first touch).
 struct LeftT {
     const int* keys;
     const double* vals;
@@ -93,27 +96,45 @@ struct Acc {
 template <int G, bool NUM>
 __device__ __forceinline__ void sub_step(const Group<G>& g, const Acc<NUM>& T, bool act, int c,
                                          double bv, double s, int& nk, bool& live) {
+    act = act && live;
+    unsigned slot = hash_slot(c, T.shift);
+    const int k0 = act ? T.keys[slot] : c;   // idle lanes count as hits
     bool is_new = false;
-    int slot = 0;
-    if (act && live) {
-        slot = table_insert(T.keys, T.smask, T.shift, c, is_new);
-        if (NUM && slot >= 0) T.vals[slot] = __dadd_rn(T.vals[slot], __dmul_rn(bv, s));
+    if (k0 != c) {
+        // Miss: probe until the key or an empty slot (one always exists:
+        // the table never passes its limit).  Bounded by the table size.
+        int k = k0;
+        for (unsigned probe = 0; probe <= T.smask; ++probe) {
+            if (k == kEmpty) {
+                const int old = atomicCAS(T.keys + slot, kEmpty, c);
+                if (old == kEmpty) {
+                    is_new = true;
+                    break;
+                }
+                k = old;
+                if (k == c) break;
+            }
+            slot = (slot + 1) & T.smask;
+            k = T.keys[slot];
+            if (k == c) break;
+        }
     }
+    if (NUM && act) T.vals[slot] = __dadd_rn(T.vals[slot], __dmul_rn(bv, s));
     const unsigned nb = __ballot_sync(kFull, is_new);
-    if (is_new) T.ord[nk + __popc(nb & g.below)] = slot;
+    if (is_new) T.ord[nk + __popc(nb & g.below)] = static_cast<int>(slot);
     nk += __popc(nb & g.mask);
-    if (nk > T.limit) live = false;
+    live = nk <= T.limit;
 }
 
 // Accumulate sum_{t<n} L.val(t) * B(L.key(t), :) in ascending t; n is this
 // group's left-row length (0 for an idle group).  Every lane of the warp
 // must call it.  Returns the distinct-key count; `fail` when the group
-// passed its table limit.
-template <int G, int EP, bool NUM, class Left>
+// passed its table limit.  b_long: some right row is longer than EP*G.
+template <int G, int EP, bool NUM, typename TB, class Left>
 __device__ __forceinline__ int accumulate(const Group<G>& g, const Left& L, int n,
                                           const int* __restrict__ b_rp,
-                                          const int* __restrict__ b_ci, const void* b_v,
-                                          int b_vt, const Acc<NUM>& T, bool& fail) {
+                                          const int* __restrict__ b_ci, const TB* __restrict__ b_v,
+                                          bool b_long, const Acc<NUM>& T, bool& fail) {
     int nk = 0;
     bool live = n > 0;
     const int nmax = __reduce_max_sync(kFull, n);
@@ -132,79 +153,85 @@ __device__ __forceinline__ int accumulate(const Group<G>& g, const Left& L, int 
             pe = __ldg(b_rp + k + 1);
         }
     };
-    // Entries of a chunk: [j][m] = entry gl + m*G of step j.
     constexpr int EPA = EP > 0 ? EP : 1;   // array extent (EP == 0: no prefetch)
-    int ec0[G][EPA], ec1[G][EPA];
-    double ev0[G][EPA], ev1[G][EPA];
+    // Entries of a chunk: [j][m] = entry gl + m*G of step j.
     auto load_entries = [&](int pb, int pe, int (&ec)[G][EPA], double (&ev)[G][EPA]) {
+        if constexpr (EP > 0) {
 #pragma unroll
-        for (int j = 0; j < G; ++j) {
-            const int jb = wshfl<G>(pb, j), je = wshfl<G>(pe, j);
+            for (int j = 0; j < G; ++j) {
+                const int jb = wshfl<G>(pb, j), je = wshfl<G>(pe, j);
 #pragma unroll
-            for (int m = 0; m < EP; ++m) {
-                const int e = jb + m * G + g.gl;
-                ec[j][m] = -1;
-                ev[j][m] = 0.0;
-                if (e < je) {
-                    ec[j][m] = __ldg(b_ci + e);
-                    if (NUM) ev[j][m] = ldv(b_v, b_vt, e);
+                for (int m = 0; m < EP; ++m) {
+                    const int e = jb + m * G + g.gl;
+                    ec[j][m] = -1;
+                    ev[j][m] = 0.0;
+                    if (e < je) {
+                        ec[j][m] = __ldg(b_ci + e);
+                        if (NUM) ev[j][m] = ldv(b_v, e);
+                    }
                 }
             }
         }
     };
-
-    int pb0, pe0, pb1, pe1;
-    double ps0, ps1;
-    load_ptrs(0, pb0, pe0, ps0);
-    load_ptrs(G, pb1, pe1, ps1);
-    if constexpr (EP > 0) load_entries(pb0, pe0, ec0, ev0);
-    for (int base = 0; base < nmax; base += G) {
-        if constexpr (EP > 0) load_entries(pb1, pe1, ec1, ev1);
-        int pb2, pe2;
-        double ps2;
-        load_ptrs(base + 2 * G, pb2, pe2, ps2);
+    // Steps [base, base+G) from the chunk's pointers (pb, pe, ps) and
+    // prefetched entries (ec, ev).
+    auto run_chunk = [&](int base, int pb, int pe, double ps, const int (&ec)[G][EPA],
+                         const double (&ev)[G][EPA]) {
 #pragma unroll
         for (int j = 0; j < G; ++j) {
             if (base + j < nmax) {
-                const int jb = wshfl<G>(pb0, j), je = wshfl<G>(pe0, j);
-                const double js = NUM ? wshfl<G>(ps0, j) : 0.0;
+                const int jb = wshfl<G>(pb, j), je = wshfl<G>(pe, j);
+                const double js = NUM ? wshfl<G>(ps, j) : 0.0;
+                if constexpr (EP > 0) {
 #pragma unroll
-                for (int m = 0; m < EP; ++m) {
-                    if (__any_sync(kFull, jb + m * G < je)) {
-                        const bool act = jb + m * G + g.gl < je;
-                        sub_step<G, NUM>(g, T, act, ec0[j][m], ev0[j][m], js, nk, live);
+                    for (int m = 0; m < EP; ++m) {
+                        if (m == 0 || __any_sync(kFull, jb + m * G < je)) {
+                            const bool act = jb + m * G + g.gl < je;
+                            sub_step<G, NUM>(g, T, act, ec[j][m], ev[j][m], js, nk, live);
+                        }
                     }
                 }
-                // Right rows longer than EP*G: the rest is loaded in place.
-                for (int e0 = jb + EP * G; __any_sync(kFull, e0 < je); e0 += G) {
-                    const int e = e0 + g.gl;
-                    const bool act = e < je;
-                    int c = -1;
-                    double bv = 0.0;
-                    if (act) {
-                        c = __ldg(b_ci + e);
-                        if (NUM) bv = ldv(b_v, b_vt, e);
+                if (EP == 0 || b_long) {
+                    // Entries not prefetched are loaded in place.
+                    for (int e0 = jb + EP * G; __any_sync(kFull, e0 < je); e0 += G) {
+                        const int e = e0 + g.gl;
+                        const bool act = e < je;
+                        int c = -1;
+                        double bv = 0.0;
+                        if (act) {
+                            c = __ldg(b_ci + e);
+                            if (NUM) bv = ldv(b_v, e);
+                        }
+                        sub_step<G, NUM>(g, T, act, c, bv, js, nk, live);
                     }
-                    sub_step<G, NUM>(g, T, act, c, bv, js, nk, live);
                 }
                 __syncwarp();
             }
         }
-        pb0 = pb1;
-        pe0 = pe1;
-        ps0 = ps1;
-        pb1 = pb2;
-        pe1 = pe2;
-        ps1 = ps2;
-        if constexpr (EP > 0) {
-#pragma unroll
-            for (int j = 0; j < G; ++j)
-#pragma unroll
-                for (int m = 0; m < EP; ++m) {
-                    ec0[j][m] = ec1[j][m];
-                    ev0[j][m] = ev1[j][m];
-                }
-        }
+    };
+
+    int ecA[G][EPA], ecB[G][EPA];
+    double evA[G][EPA], evB[G][EPA];
+    int pbA, peA, pbB, peB, pbC, peC;
+    double psA, psB, psC;
+    load_ptrs(0, pbA, peA, psA);
+    load_ptrs(G, pbB, peB, psB);
+    load_entries(pbA, peA, ecA, evA);
+    // Two chunks per iteration: buffers A and B alternate without copies.
+    for (int base = 0; base < nmax; base += 2 * G) {
+        load_entries(pbB, peB, ecB, evB);
+        load_ptrs(base + 2 * G, pbC, peC, psC);
+        run_chunk(base, pbA, peA, psA, ecA, evA);
+        if (base + G >= nmax) break;
+        load_entries(pbC, peC, ecA, evA);
+        load_ptrs(base + 3 * G, pbA, peA, psA);
+        run_chunk(base + G, pbB, peB, psB, ecB, evB);
+        pbB = pbA;
+        peB = peA;
+        psB = psA;
+        pbA = pbC;
+        peA = peC;
+        psA = psC;
     }
     fail = n > 0 && !live;
     return nk;
@@ -247,9 +274,9 @@ __device__ __forceinline__ void extract(const Group<G>& g, const Acc<true>& T, i
 // registers.  Longer rows: bitonic sort in place (ck/cv hold
 // next_pow2(max n) slots), then a linear copy.  On return ck / cv are reset
 // to kEmpty / 0 where they were used.
-template <int G>
+template <int G, typename TO>
 __device__ __forceinline__ void sorted_write(const Group<G>& g, int* ck, double* cv, int n,
-                                             int* out_ci, void* out_v, int vt, long long base) {
+                                             int* out_ci, TO* out_v, long long base) {
     const bool writes = base >= 0;
     const int nmax = __reduce_max_sync(kFull, n);
     if (nmax == 0) return;
@@ -270,9 +297,11 @@ __device__ __forceinline__ void sorted_write(const Group<G>& g, int* ck, double*
 #pragma unroll
         for (int m = 0; m < RM; ++m) {
             const int i = g.gl + m * G;
-            if (i < n && writes) {
-                out_ci[base + rk[m]] = mk[m];
-                stv(out_v, vt, base + rk[m], cv[i]);
+            if (i < n) {
+                if (writes) {
+                    out_ci[base + rk[m]] = mk[m];
+                    stv(out_v, base + rk[m], cv[i]);
+                }
             }
         }
         __syncwarp();
@@ -311,7 +340,7 @@ __device__ __forceinline__ void sorted_write(const Group<G>& g, int* ck, double*
     if (writes) {
         for (int i = g.gl; i < n; i += G) {
             out_ci[base + i] = ck[i];
-            stv(out_v, vt, base + i, cv[i]);
+            stv(out_v, base + i, cv[i]);
         }
     }
     __syncwarp();
@@ -383,22 +412,33 @@ __device__ __forceinline__ long long out_base(const Group<G>& g, const RowParams
     return b;
 }
 
-// ---------------------------------------------------------------------------
+// Per-group table region: shared memory, or the group's slice of gtab.
+template <bool GT>
+__device__ __forceinline__ unsigned char* group_region(unsigned char* smem, const RowParams& p,
+                                                       int gid, int gpc, long long bytes) {
+    if constexpr (GT) {
+        return p.gtab + (static_cast<long long>(blockIdx.x) * gpc + gid) * p.gstride;
+    } else {
+        (void)p;
+        return smem + static_cast<long long>(gid) * bytes;
+    }
+}
+
+template <int G> constexpr int prefetch_depth() { return G <= 4 ? 2 : (G <= 8 ? 1 : 0); }
+
 // Direct R*A*P.  Per-group region (numeric): vals1[S1] vals2[S2] keys1[S1]
 // keys2[S2] ord1[S1] ord2[S2]; symbolic: keys1 keys2 ord1 ord2.
-template <int G, int MODE>
+template <int G, int MODE, typename TV, typename TO, bool GT>
 __global__ void __launch_bounds__(256) k_direct_rows(DirectRowArgs a, RowParams p) {
     constexpr bool NUM = MODE != kSymb;
-    constexpr int EP = G <= 4 ? 2 : (G <= 8 ? 1 : 0);
+    constexpr int EP = prefetch_depth<G>();
     extern __shared__ __align__(16) unsigned char smem[];
     const Group<G> g;
     const int gpc = blockDim.x / G;
     const int gid = threadIdx.x / G;
     const int S1 = p.S1, S2 = p.S2;
     const long long bytes = static_cast<long long>(NUM ? 16 : 8) * (S1 + S2);
-    unsigned char* region = p.gtab
-        ? p.gtab + (static_cast<long long>(blockIdx.x) * gpc + gid) * p.gstride
-        : smem + static_cast<long long>(gid) * bytes;
+    unsigned char* region = group_region<GT>(smem, p, gid, gpc, bytes);
     double* vals1 = reinterpret_cast<double*>(region);
     double* vals2 = vals1 + S1;
     int* keys1 = NUM ? reinterpret_cast<int*>(vals2 + S2) : reinterpret_cast<int*>(region);
@@ -412,6 +452,10 @@ __global__ void __launch_bounds__(256) k_direct_rows(DirectRowArgs a, RowParams 
     clear_all<G, NUM>(g, keys1, vals1, S1);
     clear_all<G, NUM>(g, keys2, vals2, S2);
     __syncwarp();
+    const TV* rv = static_cast<const TV*>(a.R.v);
+    const TV* av = static_cast<const TV*>(a.A.v);
+    const TV* pv = static_cast<const TV*>(a.P.v);
+    const bool a_long = p.a_long, p_long = p.b_long;
 
     const int gpw = 32 / G;
     const long long warps = static_cast<long long>(gridDim.x) * (blockDim.x >> 5);
@@ -427,14 +471,13 @@ __global__ void __launch_bounds__(256) k_direct_rows(DirectRowArgs a, RowParams 
         }
         // Phase 1: the R*A row, first-touch order in ord1.
         bool fail1 = false, fail2 = false;
-        const LeftG L1{a.R.ci, a.R.v, a.R.vtype, rb};
-        const int n1 = accumulate<G, EP, NUM>(g, L1, rlen, a.A.rp, a.A.ci, a.A.v, a.A.vtype, T1,
-                                              fail1);
+        const LeftG<TV> L1{a.R.ci, rv, rb};
+        const int n1 = accumulate<G, EP, NUM>(g, L1, rlen, a.A.rp, a.A.ci, av, a_long, T1, fail1);
         __syncwarp();
         // Phase 2: forward the R*A row into P in first-touch order.
         const LeftT L2{keys1, vals1, ord1};
-        const int n2 = accumulate<G, EP, NUM>(g, L2, fail1 ? 0 : n1, a.P.rp, a.P.ci, a.P.v,
-                                              a.P.vtype, T2, fail2);
+        const int n2 = accumulate<G, EP, NUM>(g, L2, fail1 ? 0 : n1, a.P.rp, a.P.ci, pv, p_long,
+                                              T2, fail2);
         __syncwarp();
         clear_listed<G, NUM>(g, T1, n1);
         __syncwarp();
@@ -458,28 +501,25 @@ __global__ void __launch_bounds__(256) k_direct_rows(DirectRowArgs a, RowParams 
         if constexpr (NUM) {
             const long long base = out_base<G, MODE>(g, p, ok, row, n2);
             int* oc = MODE == kNumBook ? p.ub_ci : p.c_ci;
-            void* ov = MODE == kNumBook ? p.ub_v : p.c_v;
-            sorted_write(g, keys1, vals1, ok ? n2 : 0, oc, ov, p.c_vt, base);
+            TO* ov = static_cast<TO*>(MODE == kNumBook ? p.ub_v : p.c_v);
+            sorted_write<G, TO>(g, keys1, vals1, ok ? n2 : 0, oc, ov, base);
         }
     }
 }
 
-// ---------------------------------------------------------------------------
 // Pair-wise A*B.  Region (numeric): vals[S] cv[S] keys[S] ck[S] ord[S];
 // symbolic: keys[S] ord[S].
-template <int G, int MODE>
+template <int G, int MODE, typename TV, typename TO, bool GT>
 __global__ void __launch_bounds__(256) k_pair_rows(PairRowArgs a, RowParams p) {
     constexpr bool NUM = MODE != kSymb;
-    constexpr int EP = G <= 4 ? 2 : (G <= 8 ? 1 : 0);
+    constexpr int EP = prefetch_depth<G>();
     extern __shared__ __align__(16) unsigned char smem[];
     const Group<G> g;
     const int gpc = blockDim.x / G;
     const int gid = threadIdx.x / G;
     const int S = p.S1;
     const long long bytes = static_cast<long long>(NUM ? 28 : 8) * S;
-    unsigned char* region = p.gtab
-        ? p.gtab + (static_cast<long long>(blockIdx.x) * gpc + gid) * p.gstride
-        : smem + static_cast<long long>(gid) * bytes;
+    unsigned char* region = group_region<GT>(smem, p, gid, gpc, bytes);
     double* vals = reinterpret_cast<double*>(region);
     double* cv = vals + S;
     int* keys = NUM ? reinterpret_cast<int*>(cv + S) : reinterpret_cast<int*>(region);
@@ -490,6 +530,9 @@ __global__ void __launch_bounds__(256) k_pair_rows(PairRowArgs a, RowParams p) {
     clear_all<G, NUM>(g, keys, vals, S);
     if (NUM) clear_all<G, NUM>(g, ck, cv, S);
     __syncwarp();
+    const TV* avals = static_cast<const TV*>(a.A.v);
+    const TV* bvals = static_cast<const TV*>(a.B.v);
+    const bool b_long = p.b_long;
 
     const int gpw = 32 / G;
     const long long warps = static_cast<long long>(gridDim.x) * (blockDim.x >> 5);
@@ -504,9 +547,8 @@ __global__ void __launch_bounds__(256) k_pair_rows(PairRowArgs a, RowParams p) {
             alen = __ldg(a.A.rp + row + 1) - ab;
         }
         bool fail = false;
-        const LeftG L{a.A.ci, a.A.v, a.A.vtype, ab};
-        const int n = accumulate<G, EP, NUM>(g, L, alen, a.B.rp, a.B.ci, a.B.v, a.B.vtype, T,
-                                             fail);
+        const LeftG<TV> L{a.A.ci, avals, ab};
+        const int n = accumulate<G, EP, NUM>(g, L, alen, a.B.rp, a.B.ci, bvals, b_long, T, fail);
         __syncwarp();
         const bool ok = has && !fail;
         if (fail) {
@@ -524,27 +566,16 @@ __global__ void __launch_bounds__(256) k_pair_rows(PairRowArgs a, RowParams p) {
         if constexpr (NUM) {
             const long long base = out_base<G, MODE>(g, p, ok, row, n);
             int* oc = MODE == kNumBook ? p.ub_ci : p.c_ci;
-            void* ov = MODE == kNumBook ? p.ub_v : p.c_v;
-            sorted_write(g, ck, cv, ok ? n : 0, oc, ov, p.c_vt, base);
+            TO* ov = static_cast<TO*>(MODE == kNumBook ? p.ub_v : p.c_v);
+            sorted_write<G, TO>(g, ck, cv, ok ? n : 0, oc, ov, base);
         }
     }
 }
 
-// ---------------------------------------------------------------------------
-// Host side.
-
-size_t row_table_bytes(bool direct, int mode, int S1, int S2) {
-    const bool num = mode != kSymb;
-    if (direct) return static_cast<size_t>(num ? 16 : 8) * (S1 + S2);
-    return static_cast<size_t>(num ? 28 : 8) * S1;
-}
-
-int row_table_limit(int S, int G) { return table_limit(S, G); }
-
-template <int G, int MODE>
-static cudaError_t direct_g(const DirectRowArgs& a, const RowParams& p, const RowGeom& geo,
-                            cudaStream_t st) {
-    auto k = k_direct_rows<G, MODE>;
+// Launch one instantiation (sets the dynamic shared-memory limit first).
+template <typename K, typename Args>
+cudaError_t launch_row_kernel(K k, const Args& a, const RowParams& p, const RowGeom& geo,
+                              cudaStream_t st) {
     if (geo.smem > 48 * 1024) {
         cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                              static_cast<int>(geo.smem));
@@ -552,45 +583,6 @@ static cudaError_t direct_g(const DirectRowArgs& a, const RowParams& p, const Ro
     }
     k<<<geo.grid, geo.block, geo.smem, st>>>(a, p);
     return cudaGetLastError();
-}
-
-template <int G, int MODE>
-static cudaError_t pair_g(const PairRowArgs& a, const RowParams& p, const RowGeom& geo,
-                          cudaStream_t st) {
-    auto k = k_pair_rows<G, MODE>;
-    if (geo.smem > 48 * 1024) {
-        cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                             static_cast<int>(geo.smem));
-        if (e != cudaSuccess) return e;
-    }
-    k<<<geo.grid, geo.block, geo.smem, st>>>(a, p);
-    return cudaGetLastError();
-}
-
-#define SP3MM_G_SWITCH(G, CALL)                          \
-    switch (G) {                                         \
-        case 4: { constexpr int GG = 4; return CALL; }   \
-        case 8: { constexpr int GG = 8; return CALL; }   \
-        case 16: { constexpr int GG = 16; return CALL; } \
-        default: { constexpr int GG = 32; return CALL; } \
-    }
-
-cudaError_t launch_direct_rows(const DirectRowArgs& a, const RowParams& p, int mode,
-                               const RowGeom& geo, cudaStream_t st) {
-    if (p.nrows <= 0) return cudaSuccess;
-    note_launch();
-    if (mode == kSymb) SP3MM_G_SWITCH(geo.G, (direct_g<GG, kSymb>(a, p, geo, st)));
-    if (mode == kNumExact) SP3MM_G_SWITCH(geo.G, (direct_g<GG, kNumExact>(a, p, geo, st)));
-    SP3MM_G_SWITCH(geo.G, (direct_g<GG, kNumBook>(a, p, geo, st)));
-}
-
-cudaError_t launch_pair_rows(const PairRowArgs& a, const RowParams& p, int mode,
-                             const RowGeom& geo, cudaStream_t st) {
-    if (p.nrows <= 0) return cudaSuccess;
-    note_launch();
-    if (mode == kSymb) SP3MM_G_SWITCH(geo.G, (pair_g<GG, kSymb>(a, p, geo, st)));
-    if (mode == kNumExact) SP3MM_G_SWITCH(geo.G, (pair_g<GG, kNumExact>(a, p, geo, st)));
-    SP3MM_G_SWITCH(geo.G, (pair_g<GG, kNumBook>(a, p, geo, st)));
 }
 
 }  // namespace sp3mm

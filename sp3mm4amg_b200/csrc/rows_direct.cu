@@ -1,0 +1,66 @@
+// rows_direct.cu -- instantiations and launcher of the direct R*A*P row
+// kernel (rows.cuh).
+#include "rows.cuh"
+
+namespace sp3mm {
+
+template <int G, int MODE, bool GT>
+static cudaError_t direct_typed(const DirectRowArgs& a, const RowParams& p, const RowGeom& geo,
+                                cudaStream_t st) {
+    const int tv = a.R.vtype, to = p.c_vt;
+    if (MODE == kSymb)
+        return launch_row_kernel(k_direct_rows<G, kSymb, double, double, GT>, a, p, geo, st);
+    if (tv == SP3MM_F64 && to == SP3MM_F64)
+        return launch_row_kernel(k_direct_rows<G, MODE, double, double, GT>, a, p, geo, st);
+    if (tv == SP3MM_F64 && to == SP3MM_F32)
+        return launch_row_kernel(k_direct_rows<G, MODE, double, float, GT>, a, p, geo, st);
+    if (tv == SP3MM_F32 && to == SP3MM_F32)
+        return launch_row_kernel(k_direct_rows<G, MODE, float, float, GT>, a, p, geo, st);
+    return launch_row_kernel(k_direct_rows<G, MODE, float, double, GT>, a, p, geo, st);
+}
+
+template <int G, bool GT>
+static cudaError_t direct_mode(const DirectRowArgs& a, const RowParams& p, int mode,
+                               const RowGeom& geo, cudaStream_t st) {
+    if (mode == kSymb) return direct_typed<G, kSymb, GT>(a, p, geo, st);
+    if (mode == kNumExact) return direct_typed<G, kNumExact, GT>(a, p, geo, st);
+    return direct_typed<G, kNumBook, GT>(a, p, geo, st);
+}
+
+cudaError_t launch_direct_rows(const DirectRowArgs& a, const RowParams& p, int mode,
+                               const RowGeom& geo, cudaStream_t st) {
+    if (p.nrows <= 0) return cudaSuccess;
+    note_launch();
+    if (p.gtab) return direct_mode<32, true>(a, p, mode, geo, st);
+    switch (geo.G) {
+        case 4: return direct_mode<4, false>(a, p, mode, geo, st);
+        case 8: return direct_mode<8, false>(a, p, mode, geo, st);
+        case 16: return direct_mode<16, false>(a, p, mode, geo, st);
+        default: return direct_mode<32, false>(a, p, mode, geo, st);
+    }
+}
+
+}  // namespace sp3mm
+// Out-of-line helpers of the row kernels.
+#include "rows.cuh"
+
+namespace sp3mm {
+
+size_t row_table_bytes(bool direct, int mode, int S1, int S2) {
+    const bool num = mode != kSymb;
+    if (direct) return static_cast<size_t>(num ? 16 : 8) * (S1 + S2);
+    return static_cast<size_t>(num ? 28 : 8) * S1;
+}
+
+int row_table_limit(int S, int G) { return table_limit(S, G); }
+
+int row_prefetch_cover(int G) {
+    switch (G) {
+        case 4: return 4 * prefetch_depth<4>();
+        case 8: return 8 * prefetch_depth<8>();
+        case 16: return 16 * prefetch_depth<16>();
+        default: return 32 * prefetch_depth<32>();
+    }
+}
+
+}  // namespace sp3mm

@@ -152,6 +152,33 @@ def test_results_do_not_depend_on_tuning(golden, orc, lanes):
                     m.free()
 
 
+def test_fp32_value_storage(golden, orc):
+    # FP32 storage, FP64 accumulation: the pattern stays exact, values carry
+    # the FP32 rounding of the stored operands and result.
+    g = golden["poisson2d_64_agg2"]
+    with S.Context() as ctx:
+        d64 = [ctx.upload(m) for m in (g["R"], g["A"], g["P"])]
+        d32 = [ctx.upload(m, S.F32) for m in (g["R"], g["A"], g["P"])]
+        for variant, want in ((S.DIRECT, g["direct"]), (S.PAIR, g["pair"]),
+                              (S.PAIR_RIGHT, g["pair"])):
+            for fl in (S.UB, S.SYMBNUM):
+                # FP64 operands, FP32 result (the finest level of a mixed hierarchy).
+                C = ctx.rap(*d64, variant, fl, S.F32).download()
+                cmp = O.compare(C, want, rtol=1e-6)
+                assert cmp["col_idx"] and cmp["max_rel_err"] < 2 ** -23, (variant, fl, cmp)
+                # FP32 operands and result: errors of the FP32 operands,
+                # bounded relative to the largest entry (entries that cancel
+                # lose relative accuracy).
+                scale = np.abs(want.data).max()
+                for out in (S.F32, S.F64):
+                    C = ctx.rap(*d32, variant, fl, out).download()
+                    cmp = O.compare(C, want, rtol=1.0)
+                    assert cmp["col_idx"], (variant, fl, out, cmp)
+                    assert np.abs(C.data - want.data).max() <= 1e-5 * scale
+        with pytest.raises(S.Sp3mmError):
+            ctx.rap(d64[0], d32[1], d64[2], S.DIRECT, S.UB)
+
+
 @pytest.mark.parametrize("flavour", [0, 1])
 def test_long_rows_use_large_and_global_tables(orc, flavour):
     # Dense-ish rows push bounds past the shared-memory levels (up to 4096
