@@ -271,6 +271,25 @@ SP3MM_API int sp3mm_spmm_rowsizes(sp3mm_ctx *ctx, const sp3mm_dcsr *A, const sp3
                         int exact, int32_t *rows_dev, int64_t *total);
 /* Device transpose (R = P^T), values kept in their storage type. */
 SP3MM_API int sp3mm_transpose(sp3mm_ctx *ctx, const sp3mm_dcsr *A, sp3mm_dcsr *AT);
+/* C = R*A*P, direct variant, symbolic-numeric flavour, allocating nothing.
+ * No counterpart in the reference: it serves callers that cannot let a
+ * library allocate device memory while they run (their device memory is
+ * owned by another allocator, or the call sits in a latency-critical loop).
+ * Inputs are FP64 device CSRs; the caller passes C's arrays: c_row_ptr
+ * (R->M + 1 entries), c_col / c_val (c_capacity entries).  *c_nnz receives
+ * C's nonzero count; when it exceeds c_capacity the call returns
+ * SP3MM_ENOMEM having written only c_row_ptr (call again with larger
+ * arrays).  Temporaries live in a fixed 64 MiB device array inside the
+ * library (held on every device that uses it until the process exits), which
+ * bounds R->M to about 2.7 million rows (SP3MM_ELIMIT beyond) and requires
+ * every row's hash tables to fit in shared memory.  The first call on a
+ * device looks up that array's address; make it before any stream capture.
+ * Calls whose GPU work overlaps share the array and race: serialise them.
+ * `stream` is a cudaStream_t (NULL: the legacy default stream). */
+SP3MM_API int sp3mm_rap_direct_noalloc(const sp3mm_dcsr *R, const sp3mm_dcsr *A,
+                                       const sp3mm_dcsr *P, int32_t *c_row_ptr, int32_t *c_col,
+                                       double *c_val, int64_t c_capacity, int64_t *c_nnz,
+                                       void *stream);
 /* Upper bound of the device bytes a sp3mm_rap call may allocate. */
 SP3MM_API int sp3mm_rap_memory_estimate(const sp3mm_dcsr *R, const sp3mm_dcsr *A,
                               const sp3mm_dcsr *P, int variant, int flavour,

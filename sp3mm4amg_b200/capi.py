@@ -52,6 +52,9 @@ DEVICE_API = {
     "sp3mm_spmm_rowsizes": (_c.c_int, [_c.c_void_p, _c.c_void_p, _c.c_void_p, _c.c_int,
                                        _c.c_void_p, _c.POINTER(_c.c_int64)]),
     "sp3mm_transpose": (_c.c_int, [_c.c_void_p, _c.c_void_p, _c.c_void_p]),
+    "sp3mm_rap_direct_noalloc": (_c.c_int, [_c.c_void_p, _c.c_void_p, _c.c_void_p, _c.c_void_p,
+                                            _c.c_void_p, _c.c_void_p, _c.c_int64,
+                                            _c.POINTER(_c.c_int64), _c.c_void_p]),
     "sp3mm_rap_memory_estimate": (_c.c_int, [_c.c_void_p, _c.c_void_p, _c.c_void_p, _c.c_int,
                                              _c.c_int, _c.POINTER(_c.c_size_t)]),
 }
