@@ -223,12 +223,11 @@ int bin_rows(sp3mm_ctx* ctx, int M, const int* need, int shift, int G, Counters*
     return SP3MM_OK;
 }
 
-// Lanes per row from the right operand's mean row length (or the tuning).
+// Lanes per row: the tuning, else a whole warp (the warp kernels); the
+// mean row length of the right operand is kept for callers that tune by it.
 int pick_group(const sp3mm_ctx* ctx, double mean) {
+    (void)mean;
     if (ctx->tune_G) return ctx->tune_G;
-    if (mean <= 4.0) return 4;
-    if (mean <= 8.0) return 8;
-    if (mean <= 16.0) return 16;
     return 32;
 }
 
@@ -244,7 +243,7 @@ struct RowRunner {
     int a_max = -1, b_max = -1;
 
     int launch(RowParams p, int G, DevBuf& gtab) {
-        const size_t per_group = row_table_bytes(direct, mode, p.S1, p.S2);
+        const size_t per_group = row_table_bytes(direct, mode, G, p.S1, p.S2);
         const int gpw = 32 / G;
         int warps = static_cast<int>(ctx->smem_budget / (per_group * gpw));
         if (warps > 8) warps = 8;
@@ -262,7 +261,7 @@ struct RowRunner {
             // Tables in global memory, one warp per row; concurrency bounded
             // by a 2 GiB scratch budget.
             geo.G = G = 32;
-            const size_t stride = row_table_bytes(direct, mode, p.S1, p.S2);
+            const size_t stride = row_table_bytes(direct, mode, 32, p.S1, p.S2);
             size_t groups = static_cast<size_t>(p.nrows);
             const size_t cap = static_cast<size_t>(ctx->num_sms) * 8;
             if (groups > cap) groups = cap;
@@ -476,8 +475,8 @@ int direct_impl(sp3mm_ctx* ctx, const sp3mm_dcsr& R, const sp3mm_dcsr& A, const 
     const double mean = std::max(A.M ? static_cast<double>(A.nnz) / A.M : 1.0,
                                  P.M ? static_cast<double>(P.nnz) / P.M : 1.0);
     const int G = pick_group(ctx, mean);
-    const int d1 = ctx->tune_d1 >= 0 ? ctx->tune_d1 : 1;
-    const int d2 = ctx->tune_d2 >= 0 ? ctx->tune_d2 : 1;
+    const int d1 = ctx->tune_d1 >= 0 ? ctx->tune_d1 : 2;
+    const int d2 = ctx->tune_d2 >= 0 ? ctx->tune_d2 : 0;
     const int pmax = P.max_row >= 0 ? P.max_row : P.N;
     DevBuf cnt_buf, need;
     TRY(cnt_buf.alloc(ctx, sizeof(Counters)));

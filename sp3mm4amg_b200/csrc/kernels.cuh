@@ -63,7 +63,8 @@ struct RowGeom {
     size_t smem;  // dynamic shared memory per CTA
 };
 
-size_t row_table_bytes(bool direct, int mode, int S1, int S2);
+// Table bytes of one row (G lanes; G == 32: the warp kernels, incl. staging).
+size_t row_table_bytes(bool direct, int mode, int G, int S1, int S2);
 int row_table_limit(int S, int G);
 // Right-row entries a G-lane group prefetches per step (0: none).
 int row_prefetch_cover(int G);

@@ -144,7 +144,7 @@ int run_direct(const Layout& L, const DirectRowArgs& da, RowParams base, int mod
     launch_bin_scatter(M, L.level, L.head->cursors, L.lists, st);
 
     auto launch = [&](RowParams p, int g) -> int {
-        const size_t per_group = row_table_bytes(true, mode, p.S1, p.S2);
+        const size_t per_group = row_table_bytes(true, mode, g, p.S1, p.S2);
         const int gpw = 32 / g;
         int warps = static_cast<int>(geo.smem_budget / (per_group * gpw));
         if (warps > 8) warps = 8;

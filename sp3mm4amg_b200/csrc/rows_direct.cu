@@ -1,8 +1,31 @@
 // rows_direct.cu -- instantiations and launcher of the direct R*A*P row
 // kernel (rows.cuh).
-#include "rows.cuh"
+#include "rowwarp.cuh"
 
 namespace sp3mm {
+
+template <int MODE, bool GT>
+static cudaError_t direct_warp_typed(const DirectRowArgs& a, const RowParams& p,
+                                     const RowGeom& geo, cudaStream_t st) {
+    const int tv = a.R.vtype, to = p.c_vt;
+    if (MODE == kSymb)
+        return launch_row_kernel(k_direct_warp<kSymb, double, double, GT>, a, p, geo, st);
+    if (tv == SP3MM_F64 && to == SP3MM_F64)
+        return launch_row_kernel(k_direct_warp<MODE, double, double, GT>, a, p, geo, st);
+    if (tv == SP3MM_F64 && to == SP3MM_F32)
+        return launch_row_kernel(k_direct_warp<MODE, double, float, GT>, a, p, geo, st);
+    if (tv == SP3MM_F32 && to == SP3MM_F32)
+        return launch_row_kernel(k_direct_warp<MODE, float, float, GT>, a, p, geo, st);
+    return launch_row_kernel(k_direct_warp<MODE, float, double, GT>, a, p, geo, st);
+}
+
+template <bool GT>
+static cudaError_t direct_warp_mode(const DirectRowArgs& a, const RowParams& p, int mode,
+                                    const RowGeom& geo, cudaStream_t st) {
+    if (mode == kSymb) return direct_warp_typed<kSymb, GT>(a, p, geo, st);
+    if (mode == kNumExact) return direct_warp_typed<kNumExact, GT>(a, p, geo, st);
+    return direct_warp_typed<kNumBook, GT>(a, p, geo, st);
+}
 
 template <int G, int MODE, bool GT>
 static cudaError_t direct_typed(const DirectRowArgs& a, const RowParams& p, const RowGeom& geo,
@@ -31,23 +54,26 @@ cudaError_t launch_direct_rows(const DirectRowArgs& a, const RowParams& p, int m
                                const RowGeom& geo, cudaStream_t st) {
     if (p.nrows <= 0) return cudaSuccess;
     note_launch();
-    if (p.gtab) return direct_mode<32, true>(a, p, mode, geo, st);
+    // A whole warp per row (and every global-table launch): warp kernels;
+    // 4 / 8 / 16 lanes per row: the group kernels.
+    if (p.gtab) return direct_warp_mode<true>(a, p, mode, geo, st);
     switch (geo.G) {
         case 4: return direct_mode<4, false>(a, p, mode, geo, st);
         case 8: return direct_mode<8, false>(a, p, mode, geo, st);
         case 16: return direct_mode<16, false>(a, p, mode, geo, st);
-        default: return direct_mode<32, false>(a, p, mode, geo, st);
+        default: return direct_warp_mode<false>(a, p, mode, geo, st);
     }
 }
 
 }  // namespace sp3mm
 // Out-of-line helpers of the row kernels.
-#include "rows.cuh"
+#include "rowwarp.cuh"
 
 namespace sp3mm {
 
-size_t row_table_bytes(bool direct, int mode, int S1, int S2) {
+size_t row_table_bytes(bool direct, int mode, int G, int S1, int S2) {
     const bool num = mode != kSymb;
+    if (G == 32) return direct ? wdirect_bytes(num, S1, S2) : wpair_bytes(num, S1);
     if (direct) return static_cast<size_t>(num ? 16 : 8) * (S1 + S2);
     return static_cast<size_t>(num ? 28 : 8) * S1;
 }
