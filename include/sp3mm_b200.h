@@ -295,6 +295,38 @@ SP3MM_API int sp3mm_rap_memory_estimate(const sp3mm_dcsr *R, const sp3mm_dcsr *A
                               const sp3mm_dcsr *P, int variant, int flavour,
                               size_t *bytes);
 
+/* ---- Smoothed-aggregation setup around the product --------------------
+ * The level-by-level chain that produces the reference's test operators
+ * (code/scripts/getLevels3MMmatrixes.py:29-38) applied on the
+ * device.  A is a square operator on a box grid of ndim (1..3) dimensions
+ * dims[] with lexicographic numbering (x fastest) and a non-zero diagonal.
+ *
+ * sp3mm_block_prolongator: P = (I - omega D^-1 A) P0, P0 the aggregation of
+ * non-overlapping block^ndim grid blocks (partial blocks at the high edges),
+ * on the pattern of A*P0, values stored as out_val_type.  A row without a
+ * diagonal entry returns SP3MM_EINVAL. */
+SP3MM_API int sp3mm_block_prolongator(sp3mm_ctx *ctx, const sp3mm_dcsr *A, const int32_t *dims,
+                                      int ndim, int block, double omega, int out_val_type,
+                                      sp3mm_dcsr *P);
+
+/* A device-resident hierarchy A_0 (the caller's, borrowed) .. A_{L-1} with
+ * P_l = sp3mm_block_prolongator(A_l), R_l = P_l^T and
+ * A_{l+1} = R_l A_l P_l by sp3mm_rap(variant, flavour).  Coarsening stops
+ * at max_levels levels or once A_l has fewer than min_coarse rows.
+ * coarse_val_type SP3MM_F32 keeps level 0 in A_0's type and stores every
+ * coarse operator and coarse prolongator in FP32 (FP64 accumulation). */
+typedef struct sp3mm_hierarchy sp3mm_hierarchy;
+SP3MM_API int sp3mm_hierarchy_build(sp3mm_ctx *ctx, const sp3mm_dcsr *A0, const int32_t *dims,
+                                    int ndim, int block, double omega, int64_t min_coarse,
+                                    int max_levels, int variant, int flavour,
+                                    int coarse_val_type, sp3mm_hierarchy **out);
+SP3MM_API int sp3mm_hierarchy_levels(const sp3mm_hierarchy *h);
+/* Views of level `level`'s operator and (for all but the last level) its
+ * prolongator and restriction; owned by the hierarchy. */
+SP3MM_API int sp3mm_hierarchy_get(const sp3mm_hierarchy *h, int level, sp3mm_dcsr *A,
+                                  sp3mm_dcsr *P, sp3mm_dcsr *R);
+SP3MM_API int sp3mm_hierarchy_free(sp3mm_ctx *ctx, sp3mm_hierarchy *h);
+
 #ifdef __cplusplus
 }
 #endif

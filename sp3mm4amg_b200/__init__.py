@@ -140,9 +140,10 @@ def elapsed_internal() -> float:
 class DeviceCSR:
     """A CSR matrix resident in device memory (owned by its context)."""
 
-    def __init__(self, ctx: "Context", d: sp3mm_dcsr):
+    def __init__(self, ctx: "Context", d: sp3mm_dcsr, owned: bool = True):
         self.ctx = ctx
         self.d = d
+        self.owned = owned   # False: a view into a hierarchy, freed with it
 
     @property
     def shape(self):
@@ -174,7 +175,7 @@ class DeviceCSR:
         return CSR(rp, ci[:nnz], v[:nnz], self.shape)
 
     def free(self) -> None:
-        if self.d.row_ptr or self.d.col or self.d.val:
+        if self.owned and (self.d.row_ptr or self.d.col or self.d.val):
             self.ctx.lib.sp3mm_dcsr_free(self.ctx.h, self.ref)
 
     def bytes(self, idx_bytes: int = 4) -> int:
@@ -279,6 +280,27 @@ class Context:
                                                        ctypes.byref(b)))
         return int(b.value)
 
+    def block_prolongator(self, A: DeviceCSR, dims, block: int = 2, omega: float = 2.0 / 3.0,
+                          out_val_type: int = F64) -> DeviceCSR:
+        """P = (I - omega D^-1 A) P0 for the block^d aggregation of A's grid."""
+        dd = (ctypes.c_int32 * 3)(*(list(dims) + [1, 1])[:3])
+        d = sp3mm_dcsr()
+        self._check(self.lib.sp3mm_block_prolongator(self.h, A.ref, dd, len(dims), block,
+                                                     float(omega), out_val_type,
+                                                     ctypes.byref(d)))
+        return DeviceCSR(self, d)
+
+    def hierarchy(self, A0: DeviceCSR, dims, block: int = 2, omega: float = 2.0 / 3.0,
+                  min_coarse: int = 64, max_levels: int = 10, variant: int = DIRECT,
+                  flavour: int = UB, coarse_val_type: int = F64) -> "Hierarchy":
+        """Device-resident smoothed-aggregation hierarchy over A0 (borrowed)."""
+        dd = (ctypes.c_int32 * 3)(*(list(dims) + [1, 1])[:3])
+        h = ctypes.c_void_p()
+        self._check(self.lib.sp3mm_hierarchy_build(
+            self.h, A0.ref, dd, len(dims), block, float(omega), min_coarse, max_levels,
+            variant, flavour, coarse_val_type, ctypes.byref(h)))
+        return Hierarchy(self, h)
+
     def close(self) -> None:
         if self.h:
             self.lib.sp3mm_ctx_destroy(self.h)
@@ -289,3 +311,26 @@ class Context:
 
     def __exit__(self, *exc):
         self.close()
+
+
+class Hierarchy:
+    """Levels (A_l, P_l, R_l) of a device hierarchy; P/R are None on the last."""
+
+    def __init__(self, ctx: Context, h: ctypes.c_void_p):
+        self.ctx = ctx
+        self.h = h
+
+    def __len__(self) -> int:
+        return int(self.ctx.lib.sp3mm_hierarchy_levels(self.h))
+
+    def level(self, l: int):
+        a, p, r = sp3mm_dcsr(), sp3mm_dcsr(), sp3mm_dcsr()
+        self.ctx._check(self.ctx.lib.sp3mm_hierarchy_get(self.h, l, ctypes.byref(a),
+                                                         ctypes.byref(p), ctypes.byref(r)))
+        view = (lambda d: DeviceCSR(self.ctx, d, owned=False) if d.row_ptr else None)
+        return view(a), view(p), view(r)
+
+    def free(self) -> None:
+        if self.h:
+            self.ctx.lib.sp3mm_hierarchy_free(self.ctx.h, self.h)
+            self.h = None

@@ -57,6 +57,15 @@ DEVICE_API = {
                                             _c.POINTER(_c.c_int64), _c.c_void_p]),
     "sp3mm_rap_memory_estimate": (_c.c_int, [_c.c_void_p, _c.c_void_p, _c.c_void_p, _c.c_int,
                                              _c.c_int, _c.POINTER(_c.c_size_t)]),
+    "sp3mm_block_prolongator": (_c.c_int, [_c.c_void_p, _c.c_void_p, _c.c_void_p, _c.c_int,
+                                           _c.c_int, _c.c_double, _c.c_int, _c.c_void_p]),
+    "sp3mm_hierarchy_build": (_c.c_int, [_c.c_void_p, _c.c_void_p, _c.c_void_p, _c.c_int,
+                                         _c.c_int, _c.c_double, _c.c_int64, _c.c_int, _c.c_int,
+                                         _c.c_int, _c.c_int, _c.POINTER(_c.c_void_p)]),
+    "sp3mm_hierarchy_levels": (_c.c_int, [_c.c_void_p]),
+    "sp3mm_hierarchy_get": (_c.c_int, [_c.c_void_p, _c.c_int, _c.c_void_p, _c.c_void_p,
+                                       _c.c_void_p]),
+    "sp3mm_hierarchy_free": (_c.c_int, [_c.c_void_p, _c.c_void_p]),
 }
 
 # Error codes, flavours, variants, value types (include/sp3mm_b200.h).

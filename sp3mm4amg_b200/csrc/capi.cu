@@ -826,6 +826,12 @@ spmat* pair_driver(spmat* R, spmat* AC, spmat* P, CONFIG* cfg, SPMM_INTERF spmm,
 
 }  // namespace
 
+namespace sp3mm {
+int report_error(sp3mm_ctx* ctx, int code, const char* msg) {
+    return set_error(ctx, code, "%s", msg);
+}
+}  // namespace sp3mm
+
 // ---------------------------------------------------------------------------
 // Layer 2 C ABI.
 extern "C" {

@@ -133,3 +133,10 @@ void note_launch();
 uint64_t launch_count();
 
 }  // namespace sp3mm
+
+struct sp3mm_ctx;
+namespace sp3mm {
+// Record `msg` as the context's last error (and print it); returns `code`.
+int report_error(sp3mm_ctx* ctx, int code, const char* msg);
+
+}  // namespace sp3mm
