@@ -255,6 +255,9 @@ SP3MM_API int sp3mm_dcsr_download(sp3mm_ctx *ctx, const sp3mm_dcsr *m, int off_f
 SP3MM_API int sp3mm_dcsr_download_arrays(sp3mm_ctx *ctx, const sp3mm_dcsr *m, int64_t *row_ptr,
                                int64_t *col, double *val);
 SP3MM_API int sp3mm_dcsr_free(sp3mm_ctx *ctx, sp3mm_dcsr *m);
+/* Overwrite the values of m (same pattern) from host FP64 val[nnz],
+ * converted to m's value type; returns once the copy is complete. */
+SP3MM_API int sp3mm_dcsr_set_values(sp3mm_ctx *ctx, sp3mm_dcsr *m, const double *val);
 
 /* C = A*B on the device, flavour SP3MM_UB or SP3MM_SYMBNUM; C's values are
  * stored as out_val_type.  C is allocated by the library. */
@@ -294,6 +297,42 @@ SP3MM_API int sp3mm_rap_direct_noalloc(const sp3mm_dcsr *R, const sp3mm_dcsr *A,
 SP3MM_API int sp3mm_rap_memory_estimate(const sp3mm_dcsr *R, const sp3mm_dcsr *A,
                               const sp3mm_dcsr *P, int variant, int flavour,
                               size_t *bytes);
+
+/* ---- Batches: many independent products in one pass --------------------
+ * Product i is C_i = X_i*Y_i (SP3MM_BATCH_SPMM, the symbolic-numeric SpMM)
+ * or C_i = X_i*Y_i*Z_i (SP3MM_BATCH_RAP, the direct row-forwarding triple
+ * product); results equal the single-product calls bit for bit.  All
+ * operands share one value type; results are stored as out_val_type.
+ * The operands are borrowed: they must stay allocated, with unchanged
+ * patterns, while the batch is used.
+ *
+ * sp3mm_batch_plan runs the symbolic pass of every product at once (a few
+ * host round trips per batch), allocates the results and captures the
+ * numeric pass as a CUDA graph.  sp3mm_batch_execute replays that graph on
+ * the context stream without host synchronisation; it may be repeated
+ * after the operands' values change.  sp3mm_batch_run = plan (when needed)
+ * + execute + error check.  Results are views owned by the batch. */
+enum { SP3MM_BATCH_SPMM = 0, SP3MM_BATCH_RAP = 1 };
+typedef struct sp3mm_batch sp3mm_batch;
+SP3MM_API int sp3mm_batch_create(sp3mm_ctx *ctx, int n, const int *kinds, const sp3mm_dcsr *X,
+                                 const sp3mm_dcsr *Y, const sp3mm_dcsr *Z, int out_val_type,
+                                 sp3mm_batch **out);
+/* Symbolic table shifts d1, d2 (first table from its bound >> d1; second
+ * from its bound >> d2), numeric table slack (2^slack times the exact
+ * size), and the table levels at which a new numeric tier (one persistent
+ * launch) starts: nsplits < 0 for one tier per level, 0 for a single tier. */
+SP3MM_API int sp3mm_batch_set_tuning(sp3mm_batch *b, int d1, int d2, int slack, int nsplits,
+                                     const int32_t *splits);
+SP3MM_API int sp3mm_batch_plan(sp3mm_batch *b);
+SP3MM_API int sp3mm_batch_execute(sp3mm_batch *b);
+SP3MM_API int sp3mm_batch_run(sp3mm_batch *b);
+/* Times `reps` replays of each candidate tiering and slack, keeps the
+ * fastest; one line per candidate is written to report (may be NULL). */
+SP3MM_API int sp3mm_batch_autotune(sp3mm_batch *b, int reps, char *report, size_t len);
+SP3MM_API int sp3mm_batch_result(const sp3mm_batch *b, int i, sp3mm_dcsr *C);
+SP3MM_API int sp3mm_batch_info(const sp3mm_batch *b, int64_t *rows, int64_t *nnz, int *tiers,
+                               int *global_tiers);
+SP3MM_API int sp3mm_batch_free(sp3mm_batch *b);
 
 /* ---- Smoothed-aggregation setup around the product --------------------
  * The level-by-level chain that produces the reference's test operators

@@ -25,7 +25,8 @@ import ctypes
 import numpy as np
 
 from . import capi
-from .capi import (DIRECT, F32, F64, PAIR, PAIR_RIGHT, SYMBNUM, UB, sp3mm_dcsr)
+from .capi import (BATCH_RAP, BATCH_SPMM, DIRECT, F32, F64, PAIR, PAIR_RIGHT, SYMBNUM, UB,
+                   sp3mm_dcsr)
 from .problems import CSR, Problem
 from .spmat import (CONFIG, HostSpMat, IDXMAP, RBTREE, SPMAT_P, array_from_idx_ptr,
                     csr_from_spmat, idx_t, spmat)
@@ -34,6 +35,7 @@ __all__ = [
     "CSR", "Problem", "Context", "DeviceCSR", "Sp3mmError", "spmm", "sp3mm",
     "symb_rowsizes", "ub_rowsizes", "ub_colparts_rowsizes", "elapsed_internal",
     "UB", "SYMBNUM", "PAIR", "DIRECT", "PAIR_RIGHT", "F64", "F32", "RBTREE", "IDXMAP",
+    "BATCH_SPMM", "BATCH_RAP", "Batch", "Hierarchy",
 ]
 
 
@@ -174,6 +176,13 @@ class DeviceCSR:
             self.ctx.h, self.ref, rp.ctypes.data, ci.ctypes.data, v.ctypes.data))
         return CSR(rp, ci[:nnz], v[:nnz], self.shape)
 
+    def set_values(self, values: np.ndarray) -> None:
+        """Overwrite the values (same pattern) from host FP64 values."""
+        v = np.ascontiguousarray(values, np.float64)
+        if v.size != self.nnz:
+            raise ValueError("values must have one entry per nonzero")
+        self.ctx._check(self.ctx.lib.sp3mm_dcsr_set_values(self.ctx.h, self.ref, v.ctypes.data))
+
     def free(self) -> None:
         if self.owned and (self.d.row_ptr or self.d.col or self.d.val):
             self.ctx.lib.sp3mm_dcsr_free(self.ctx.h, self.ref)
@@ -301,6 +310,11 @@ class Context:
             variant, flavour, coarse_val_type, ctypes.byref(h)))
         return Hierarchy(self, h)
 
+    def batch(self, products, out_val_type: int = F64) -> "Batch":
+        """A batch of independent products: (X, Y) for X*Y, (X, Y, Z) for
+        the direct X*Y*Z."""
+        return Batch(self, products, out_val_type)
+
     def close(self) -> None:
         if self.h:
             self.lib.sp3mm_ctx_destroy(self.h)
@@ -333,4 +347,74 @@ class Hierarchy:
     def free(self) -> None:
         if self.h:
             self.ctx.lib.sp3mm_hierarchy_free(self.ctx.h, self.h)
+            self.h = None
+
+
+class Batch:
+    """Many independent products planned together and executed as one
+    captured CUDA graph (sp3mm_batch_*)."""
+
+    def __init__(self, ctx: Context, products, out_val_type: int = F64):
+        self.ctx = ctx
+        self.products = list(products)   # keep the operands alive
+        n = len(self.products)
+        kinds = (ctypes.c_int * max(n, 1))()
+        X = (sp3mm_dcsr * max(n, 1))()
+        Y = (sp3mm_dcsr * max(n, 1))()
+        Z = (sp3mm_dcsr * max(n, 1))()
+        for i, p in enumerate(self.products):
+            kinds[i] = BATCH_RAP if len(p) == 3 else BATCH_SPMM
+            X[i] = p[0].d
+            Y[i] = p[1].d
+            if len(p) == 3:
+                Z[i] = p[2].d
+        h = ctypes.c_void_p()
+        ctx._check(ctx.lib.sp3mm_batch_create(ctx.h, n, kinds, X, Y, Z, out_val_type,
+                                              ctypes.byref(h)))
+        self.h = h
+
+    def __len__(self) -> int:
+        return len(self.products)
+
+    def set_tuning(self, d1: int = 2, d2: int = 1, slack: int = 0, splits=None) -> None:
+        """splits None: one numeric tier per table level; [] one tier; else
+        a new tier starts at each listed level."""
+        if splits is None:
+            arr, ns = None, -1
+        else:
+            ns = len(splits)
+            arr = (ctypes.c_int32 * max(ns, 1))(*splits)
+        self.ctx._check(self.ctx.lib.sp3mm_batch_set_tuning(self.h, d1, d2, slack, ns, arr))
+
+    def plan(self) -> None:
+        self.ctx._check(self.ctx.lib.sp3mm_batch_plan(self.h))
+
+    def execute(self) -> None:
+        self.ctx._check(self.ctx.lib.sp3mm_batch_execute(self.h))
+
+    def run(self) -> None:
+        self.ctx._check(self.ctx.lib.sp3mm_batch_run(self.h))
+
+    def autotune(self, reps: int = 3) -> str:
+        buf = ctypes.create_string_buffer(1 << 14)
+        self.ctx._check(self.ctx.lib.sp3mm_batch_autotune(self.h, reps, buf, len(buf)))
+        return buf.value.decode()
+
+    def result(self, i: int) -> DeviceCSR:
+        d = sp3mm_dcsr()
+        self.ctx._check(self.ctx.lib.sp3mm_batch_result(self.h, i, ctypes.byref(d)))
+        return DeviceCSR(self.ctx, d, owned=False)
+
+    def info(self) -> dict:
+        rows, nnz = ctypes.c_int64(), ctypes.c_int64()
+        tiers, gt = ctypes.c_int(), ctypes.c_int()
+        self.ctx._check(self.ctx.lib.sp3mm_batch_info(self.h, ctypes.byref(rows),
+                                                      ctypes.byref(nnz), ctypes.byref(tiers),
+                                                      ctypes.byref(gt)))
+        return {"rows": rows.value, "nnz": nnz.value, "tiers": tiers.value,
+                "global_tiers": gt.value}
+
+    def free(self) -> None:
+        if self.h:
+            self.ctx.lib.sp3mm_batch_free(self.h)
             self.h = None

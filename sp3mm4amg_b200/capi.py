@@ -45,6 +45,7 @@ DEVICE_API = {
     "sp3mm_dcsr_download_arrays": (_c.c_int, [_c.c_void_p, _c.c_void_p, _c.c_void_p,
                                               _c.c_void_p, _c.c_void_p]),
     "sp3mm_dcsr_free": (_c.c_int, [_c.c_void_p, _c.c_void_p]),
+    "sp3mm_dcsr_set_values": (_c.c_int, [_c.c_void_p, _c.c_void_p, _c.c_void_p]),
     "sp3mm_spmm": (_c.c_int, [_c.c_void_p, _c.c_void_p, _c.c_void_p, _c.c_int, _c.c_int,
                               _c.c_void_p]),
     "sp3mm_rap": (_c.c_int, [_c.c_void_p, _c.c_void_p, _c.c_void_p, _c.c_void_p, _c.c_int,
@@ -66,11 +67,26 @@ DEVICE_API = {
     "sp3mm_hierarchy_get": (_c.c_int, [_c.c_void_p, _c.c_int, _c.c_void_p, _c.c_void_p,
                                        _c.c_void_p]),
     "sp3mm_hierarchy_free": (_c.c_int, [_c.c_void_p, _c.c_void_p]),
+    "sp3mm_batch_create": (_c.c_int, [_c.c_void_p, _c.c_int, _c.c_void_p, _c.c_void_p,
+                                      _c.c_void_p, _c.c_void_p, _c.c_int,
+                                      _c.POINTER(_c.c_void_p)]),
+    "sp3mm_batch_set_tuning": (_c.c_int, [_c.c_void_p, _c.c_int, _c.c_int, _c.c_int, _c.c_int,
+                                          _c.c_void_p]),
+    "sp3mm_batch_plan": (_c.c_int, [_c.c_void_p]),
+    "sp3mm_batch_execute": (_c.c_int, [_c.c_void_p]),
+    "sp3mm_batch_run": (_c.c_int, [_c.c_void_p]),
+    "sp3mm_batch_autotune": (_c.c_int, [_c.c_void_p, _c.c_int, _c.c_char_p, _c.c_size_t]),
+    "sp3mm_batch_result": (_c.c_int, [_c.c_void_p, _c.c_int, _c.c_void_p]),
+    "sp3mm_batch_info": (_c.c_int, [_c.c_void_p, _c.POINTER(_c.c_int64),
+                                    _c.POINTER(_c.c_int64), _c.POINTER(_c.c_int),
+                                    _c.POINTER(_c.c_int)]),
+    "sp3mm_batch_free": (_c.c_int, [_c.c_void_p]),
 }
 
 # Error codes, flavours, variants, value types (include/sp3mm_b200.h).
 SP3MM_OK, SP3MM_ECUDA, SP3MM_EINVAL, SP3MM_ENOMEM, SP3MM_ELIMIT, SP3MM_EDEVICE = range(6)
 UB, SYMBNUM = 0, 1
+BATCH_SPMM, BATCH_RAP = 0, 1
 PAIR, DIRECT, PAIR_RIGHT = 0, 1, 2
 F64, F32 = 0, 1
 

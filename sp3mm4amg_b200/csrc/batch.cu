@@ -1,0 +1,706 @@
+// batch.cu -- many independent products in one binned, persistent pass.
+//
+// The reference computes one product per call, each an OpenMP region over
+// that product's rows (code/src/Sp3MM_CSR_OMP_UB_Generic.c:498-573 for the
+// direct triple product, :56-124 and code/src/Sp3MM_CSR_OMP_Num_Generic.c:
+// 93-146 for SpMM).  An AMG setup over many operators (hierarchy levels,
+// independent systems) calls it once per product; on a GPU each small call
+// then pays its own launches and host round trips and fills a fraction of
+// the 148 SMs.  A batch instead concatenates the rows of all its products
+// into one row space and runs the whole set as one product:
+//
+//   plan     bounds of every row -> binning by table level -> persistent
+//            symbolic launches (optimistic tables, in-kernel retry with the
+//            proven size, global-memory tables for the rest) -> one scan of
+//            the row counts -> exact binning -> output allocation, and the
+//            numeric pass captured once as a CUDA graph;
+//   execute  one replay of that graph: each tier of table levels is one
+//            persistent launch, the tiers run as parallel graph branches.
+//
+// The plan needs four host round trips per batch, not per product; execute
+// needs none and can be replayed whenever the operands' values change but
+// their patterns and addresses do not (numeric re-setup).  Results are
+// bit-identical to the single-product entry points.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "batch.cuh"
+#include "context.cuh"
+#include "sp3mm_b200.h"
+
+using namespace sp3mm;
+
+namespace {
+
+// need[g] = distinct-key bound of the first table of global row g (the
+// product count of its row of X*Y, at most Y.N); row_item[g] = its product.
+__global__ void k_batch_bounds(const BItem* __restrict__ items, const long long* __restrict__ bases,
+                               int n, long long rows, int* need, int* row_item) {
+    for (long long g = blockIdx.x * (long long)blockDim.x + threadIdx.x; g < rows;
+         g += (long long)gridDim.x * blockDim.x) {
+        int lo = 0, hi = n;   // largest b with bases[b] <= g; bases[n] = rows
+        while (hi - lo > 1) {
+            const int mid = (lo + hi) >> 1;
+            if (__ldg(bases + mid) <= g) lo = mid;
+            else hi = mid;
+        }
+        const BItem* I = items + lo;
+        const int i = static_cast<int>(g - I->row_base);
+        const int* xrp = I->X.rp;
+        const int* xci = I->X.ci;
+        const int* yrp = I->Y.rp;
+        long long u = 0;
+        for (int t = __ldg(xrp + i); t < __ldg(xrp + i + 1); ++t) {
+            const int k = __ldg(xci + t);
+            u += __ldg(yrp + k + 1) - __ldg(yrp + k);
+        }
+        need[g] = static_cast<int>(u < I->Y.N ? u : I->Y.N);
+        row_item[g] = lo;
+    }
+}
+
+// Per-product output offset and length from the global row pointers.
+__global__ void k_batch_item_spans(const BItem* __restrict__ items, int n, const int* crp,
+                                   long long* span) {
+    const int b = blockIdx.x * blockDim.x + threadIdx.x;
+    if (b >= n) return;
+    const long long g0 = items[b].row_base, g1 = g0 + items[b].M;
+    span[2 * b] = crp[g0];
+    span[2 * b + 1] = static_cast<long long>(crp[g1]) - crp[g0];
+}
+
+// Local row pointers of every product: rp_local[rp_off[b] + i] =
+// crp[row_base + i] - crp[row_base] for i = 0..M (the arrays of empty
+// products are zeroed by the caller).
+__global__ void k_batch_local_rp(const BItem* __restrict__ items, const int* __restrict__ row_item,
+                                 const long long* __restrict__ rp_off, long long rows,
+                                 const int* crp, int* rp_local) {
+    for (long long g = blockIdx.x * (long long)blockDim.x + threadIdx.x; g < rows;
+         g += (long long)gridDim.x * blockDim.x) {
+        const int b = row_item[g];
+        const long long base = items[b].row_base;
+        const int i = static_cast<int>(g - base);
+        const int c0 = crp[base];
+        int* out = rp_local + rp_off[b];
+        out[i] = crp[g] - c0;
+        if (i == items[b].M - 1) out[i + 1] = crp[g + 1] - c0;
+    }
+}
+
+int grid_for_rows(long long rows) {
+    long long g = (rows + 255) / 256;
+    return static_cast<int>(std::max<long long>(1, std::min<long long>(g, 148LL * 32)));
+}
+
+}  // namespace
+
+// A tier: a contiguous range of table levels run by one persistent launch.
+struct BatchTier {
+    int lo = 0, hi = 0;      // levels [lo, hi]
+    int first = 0, count = 0;   // rows: lists[first, first + count)
+    int scap = 0;
+    bool gt = false;
+    int block = 0, grid = 0;
+    size_t smem = 0;
+};
+
+struct sp3mm_batch {
+    sp3mm_ctx* ctx = nullptr;
+    std::vector<BItem> items;
+    std::vector<long long> bases;   // n + 1 row offsets
+    long long rows = 0;
+    int tv = SP3MM_F64, to = SP3MM_F64;
+    // Tuning: symbolic shifts, numeric slack, tier split levels (a new tier
+    // starts at each listed level; empty: one tier per non-empty level).
+    int d1 = 2, d2 = 1, slack = 0;
+    std::vector<int> splits;
+    bool auto_split = true;
+    int warps_cap = 8;
+    // Device state.
+    DevBuf d_items, d_bases, d_row_item, d_need, d_cnt1, d_cnt2, d_crp;
+    DevBuf d_ci, d_v, d_rp, d_rp_off, d_counters;
+    DevBuf num_gtab;
+    Bins nbins;
+    std::vector<BatchTier> tiers;
+    std::vector<long long> rp_off;
+    std::vector<sp3mm_dcsr> results;
+    long long nnz = 0;
+    bool planned = false;
+    // Numeric graph (tiers as parallel branches).
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t exec = nullptr;
+    std::vector<cudaStream_t> branch;
+    std::vector<cudaEvent_t> events;
+    int graph_kernels = 0;
+
+    ~sp3mm_batch() { drop_graph(); }
+    void drop_graph() {
+        if (exec) cudaGraphExecDestroy(exec);
+        if (graph) cudaGraphDestroy(graph);
+        exec = nullptr;
+        graph = nullptr;
+        for (auto s : branch) cudaStreamDestroy(s);
+        for (auto e : events) cudaEventDestroy(e);
+        branch.clear();
+        events.clear();
+    }
+};
+
+namespace {
+
+int batch_fail(sp3mm_batch* b, int code, const char* msg) {
+    return set_error(b ? b->ctx : nullptr, code, "batch: %s", msg);
+}
+
+}  // namespace
+
+namespace {
+
+// Tiers over the non-empty levels of `bins`.  A tier's tables hold
+// 32 << (its top level + extra) slots per warp (extra: the numeric slack,
+// or the symbolic shift d1 so that a proven-size retry still fits).  Tiers
+// whose region does not fit one CTA's shared memory merge into one
+// global-memory tier.
+int make_tiers(sp3mm_batch* b, const Bins& bins, bool num, int extra, int tv, int to,
+               std::vector<BatchTier>& out) {
+    sp3mm_ctx* ctx = b->ctx;
+    out.clear();
+    const int mode = num ? kNumExact : kSymb;
+    BatchTier gt;
+    gt.gt = true;
+    gt.lo = kLevels;
+    gt.hi = -1;
+    auto tier_of = [&](int L) {
+        if (b->auto_split) return L;
+        int t = 0;
+        for (int s : b->splits)
+            if (L >= s) ++t;
+        return t;
+    };
+    int L = 0;
+    while (L < kLevels) {
+        if (!bins.counts[L]) {
+            ++L;
+            continue;
+        }
+        BatchTier t;
+        t.lo = t.hi = L;
+        const int id = tier_of(L);
+        int M = L + 1;
+        while (M < kLevels && tier_of(M) == id) {
+            if (bins.counts[M]) t.hi = M;
+            ++M;
+        }
+        t.first = bins.offsets[t.lo];
+        t.count = bins.offsets[t.hi] + bins.counts[t.hi] - t.first;
+        const int top = std::min(t.hi + extra, 30 - 5);
+        t.scap = 32 << top;
+        const size_t bytes = batch_row_region_bytes(num, t.scap);
+        if (bytes > ctx->smem_optin) {
+            // Global-memory tier: extend it (levels are visited ascending).
+            if (gt.hi < 0) {
+                gt.lo = t.lo;
+                gt.first = t.first;
+            }
+            gt.hi = t.hi;
+            gt.count = bins.offsets[t.hi] + bins.counts[t.hi] - gt.first;
+            gt.scap = t.scap;
+            L = M;
+            continue;
+        }
+        int w = static_cast<int>(std::min<size_t>(b->warps_cap, ctx->smem_optin / bytes));
+        w = std::max(1, w);
+        t.block = 32 * w;
+        t.smem = bytes * w;
+        int per_sm = 0;
+        CK(ctx, batch_rows_configure(mode, false, tv, to, t.block, t.smem, ctx->smem_optin,
+                                     &per_sm));
+        per_sm = std::max(1, per_sm);
+        const long long need_ctas = (t.count + w - 1) / w;
+        t.grid = static_cast<int>(std::min<long long>(need_ctas, 1LL * per_sm * ctx->num_sms));
+        out.push_back(t);
+        L = M;
+    }
+    if (gt.hi >= 0) {
+        const size_t stride = (batch_row_region_bytes(num, gt.scap) + 255) / 256 * 256;
+        long long warps = std::min<long long>(gt.count, 8LL * ctx->num_sms);
+        const size_t budget = size_t(2) << 30;
+        while (warps > 1 && static_cast<size_t>(warps) * stride > budget) warps >>= 1;
+        const int w = static_cast<int>(std::min<long long>(8, warps));
+        gt.block = 32 * w;
+        gt.grid = static_cast<int>((warps + w - 1) / w);
+        gt.smem = stride;   // per-warp stride (the launch uses no shared memory)
+        out.push_back(gt);
+    }
+    return SP3MM_OK;
+}
+
+size_t gt_bytes(const BatchTier& t) {
+    return static_cast<size_t>(t.grid) * (t.block / 32) * t.smem;
+}
+
+// Launch the tiers; with several, tier 0 runs on the context stream and the
+// others on branch streams forked from it and joined back (parallel graph
+// branches when captured).
+int run_tiers(sp3mm_batch* b, int mode, const std::vector<BatchTier>& tiers, const int* lists,
+              BatchRowParams base, unsigned char* gtab) {
+    sp3mm_ctx* ctx = b->ctx;
+    const cudaStream_t st = ctx->stream;
+    const int nt = static_cast<int>(tiers.size());
+    while (static_cast<int>(b->branch.size()) < nt - 1) {
+        cudaStream_t s;
+        CK(ctx, cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking));
+        b->branch.push_back(s);
+    }
+    while (static_cast<int>(b->events.size()) < nt) {
+        cudaEvent_t e;
+        CK(ctx, cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+        b->events.push_back(e);
+    }
+    if (nt > 1) CK(ctx, cudaEventRecord(b->events[0], st));
+    for (int k = 0; k < nt; ++k) {
+        const BatchTier& t = tiers[k];
+        const cudaStream_t s = k == 0 ? st : b->branch[k - 1];
+        if (k > 0) CK(ctx, cudaStreamWaitEvent(s, b->events[0], 0));
+        BatchRowParams p = base;
+        p.rows = lists + t.first;
+        p.nrows = t.count;
+        p.scap = t.scap;
+        p.reverse = t.hi > t.lo ? 1 : 0;
+        size_t smem = t.smem;
+        if (t.gt) {
+            p.gtab = gtab;
+            p.gstride = static_cast<long long>(t.smem);
+            smem = 0;
+        }
+        CK(ctx, launch_batch_rows(mode, t.gt, b->tv, b->to, t.grid, t.block, smem, s,
+                                  b->d_items.as<BItem>(), b->d_row_item.as<int>(), p));
+        if (k > 0) {
+            CK(ctx, cudaEventRecord(b->events[k], s));
+            CK(ctx, cudaStreamWaitEvent(st, b->events[k], 0));
+        }
+    }
+    return SP3MM_OK;
+}
+
+// Numeric tiers, their global-memory tables and the captured graph.
+int build_numeric(sp3mm_batch* b) {
+    sp3mm_ctx* ctx = b->ctx;
+    const cudaStream_t st = ctx->stream;
+    if (b->exec) cudaGraphExecDestroy(b->exec);
+    if (b->graph) cudaGraphDestroy(b->graph);
+    b->exec = nullptr;
+    b->graph = nullptr;
+    TRY(make_tiers(b, b->nbins, true, b->slack, b->tv, b->to, b->tiers));
+    size_t need_gt = 0;
+    for (const auto& t : b->tiers)
+        if (t.gt) need_gt = gt_bytes(t);
+    b->num_gtab.release();
+    if (need_gt) TRY(b->num_gtab.alloc(ctx, need_gt));
+    BatchRowParams p{};
+    p.slack = b->slack;
+    p.cnt1 = b->d_cnt1.as<int>();
+    p.cnt2 = b->d_cnt2.as<int>();
+    p.c_rp = b->d_crp.as<int>();
+    p.c_ci = b->d_ci.as<int>();
+    p.c_v = b->d_v.p;
+    p.err = ctx->d_err;
+    // Create branch streams and events before capture begins.
+    const int nt = static_cast<int>(b->tiers.size());
+    while (static_cast<int>(b->branch.size()) < nt - 1) {
+        cudaStream_t s;
+        CK(ctx, cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking));
+        b->branch.push_back(s);
+    }
+    while (static_cast<int>(b->events.size()) < nt) {
+        cudaEvent_t e;
+        CK(ctx, cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+        b->events.push_back(e);
+    }
+    CK(ctx, cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
+    const int rc = run_tiers(b, kNumExact, b->tiers, b->nbins.lists.as<int>(), p,
+                             b->num_gtab.as<unsigned char>());
+    cudaGraph_t g = nullptr;
+    const cudaError_t e = cudaStreamEndCapture(st, &g);
+    if (rc != SP3MM_OK) {
+        if (g) cudaGraphDestroy(g);
+        return rc;
+    }
+    CK(ctx, e);
+    b->graph = g;
+    CK(ctx, cudaGraphInstantiate(&b->exec, g, 0));
+    b->graph_kernels = nt;
+    return SP3MM_OK;
+}
+
+}  // namespace
+
+namespace {
+
+int batch_plan(sp3mm_batch* b) {
+    sp3mm_ctx* ctx = b->ctx;
+    const cudaStream_t st = ctx->stream;
+    const int n = static_cast<int>(b->items.size());
+    const long long rows = b->rows;
+    const int M = static_cast<int>(rows);
+    const size_t R1 = static_cast<size_t>(rows) + 1;
+    b->planned = false;
+    b->results.assign(n, sp3mm_dcsr{});
+    TRY(b->d_items.alloc(ctx, sizeof(BItem) * n));
+    TRY(b->d_bases.alloc(ctx, sizeof(long long) * (n + 1)));
+    CK(ctx, cudaMemcpyAsync(b->d_items.p, b->items.data(), sizeof(BItem) * n,
+                            cudaMemcpyHostToDevice, st));
+    CK(ctx, cudaMemcpyAsync(b->d_bases.p, b->bases.data(), sizeof(long long) * (n + 1),
+                            cudaMemcpyHostToDevice, st));
+    TRY(b->d_row_item.alloc(ctx, sizeof(int) * R1));
+    TRY(b->d_need.alloc(ctx, sizeof(int) * R1));
+    TRY(b->d_cnt1.alloc(ctx, sizeof(int) * R1));
+    TRY(b->d_cnt2.alloc(ctx, sizeof(int) * R1));
+    TRY(b->d_crp.alloc(ctx, sizeof(int) * R1));
+    const size_t cbytes = sizeof(Counters) * 2 + 4 * sizeof(int);
+    TRY(b->d_counters.alloc(ctx, cbytes));
+    Counters* dc = b->d_counters.as<Counters>();
+    int* rinfo = reinterpret_cast<int*>(dc + 2);   // retry count, retry need
+    CK(ctx, cudaMemsetAsync(b->d_cnt1.p, 0, sizeof(int) * R1, st));
+    CK(ctx, cudaMemsetAsync(b->d_cnt2.p, 0, sizeof(int) * R1, st));
+    CK(ctx, cudaMemsetAsync(b->d_counters.p, 0, cbytes, st));
+    if (rows > 0) {
+        prof(ctx, "batch.bounds", [&] {
+            k_batch_bounds<<<grid_for_rows(rows), 256, 0, st>>>(
+                b->d_items.as<BItem>(), b->d_bases.as<long long>(), n, rows, b->d_need.as<int>(),
+                b->d_row_item.as<int>());
+        });
+        note_launch();
+        CK(ctx, cudaGetLastError());
+    }
+
+    // Symbolic pass: tiers of the optimistic levels (need >> d1).
+    Bins sb;
+    TRY(bin_rows(ctx, M, b->d_need.as<int>(), b->d1, 32, dc, nullptr, sb));
+    std::vector<BatchTier> stiers;
+    TRY(make_tiers(b, sb, false, b->d1, b->tv, b->to, stiers));
+    DevBuf retry_a, retry_b, sgtab;
+    TRY(retry_a.alloc(ctx, sizeof(int) * R1));
+    TRY(retry_b.alloc(ctx, sizeof(int) * R1));
+    size_t sgt = 0;
+    for (const auto& t : stiers)
+        if (t.gt) sgt = gt_bytes(t);
+    if (sgt) TRY(sgtab.alloc(ctx, sgt));
+    BatchRowParams p{};
+    p.d1 = b->d1;
+    p.d2 = b->d2;
+    p.need = b->d_need.as<int>();
+    p.cnt1 = b->d_cnt1.as<int>();
+    p.cnt2 = b->d_cnt2.as<int>();
+    p.retry_rows = retry_a.as<int>();
+    p.retry_count = rinfo;
+    p.retry_need = rinfo + 1;
+    p.err = ctx->d_err;
+    if (!stiers.empty()) {
+        int rc = SP3MM_OK;
+        prof(ctx, "batch.symbolic", [&] {
+            rc = run_tiers(b, kSymb, stiers, sb.lists.as<int>(), p, sgtab.as<unsigned char>());
+        });
+        TRY(rc);
+    }
+    // Rows whose proven tables exceed their tier: global-memory tables
+    // sized from the largest proven bound, at most three rounds (a direct
+    // row learns its second bound only once its first table is complete).
+    int* cur = retry_a.as<int>();
+    int* nxt = retry_b.as<int>();
+    for (int round = 0;; ++round) {
+        int h[2] = {0, 0};
+        CK(ctx, cudaMemcpyAsync(h, rinfo, sizeof h, cudaMemcpyDeviceToHost, st));
+        CK(ctx, cudaStreamSynchronize(st));
+        if (h[0] == 0) break;
+        if (round == 3) return batch_fail(b, SP3MM_EDEVICE, "symbolic retries did not converge");
+        CK(ctx, cudaMemsetAsync(rinfo, 0, 2 * sizeof(int), st));
+        BatchTier t;
+        t.gt = true;
+        t.first = 0;
+        t.count = h[0];
+        t.scap = batch_slots_for(h[1]);
+        const size_t stride = (batch_row_region_bytes(false, t.scap) + 255) / 256 * 256;
+        long long warps = std::min<long long>(h[0], 8LL * ctx->num_sms);
+        while (warps > 1 && static_cast<size_t>(warps) * stride > (size_t(2) << 30)) warps >>= 1;
+        const int w = static_cast<int>(std::min<long long>(8, warps));
+        t.block = 32 * w;
+        t.grid = static_cast<int>((warps + w - 1) / w);
+        t.smem = stride;
+        DevBuf g;
+        TRY(g.alloc(ctx, gt_bytes(t)));
+        BatchRowParams q = p;
+        q.retry_rows = nxt;
+        std::vector<BatchTier> one{t};
+        int rc = SP3MM_OK;
+        prof(ctx, "batch.symbolic.global", [&] {
+            rc = run_tiers(b, kSymb, one, cur, q, g.as<unsigned char>());
+        });
+        TRY(rc);
+        std::swap(cur, nxt);
+    }
+
+    // Row pointers of the whole batch, product spans, exact binning.
+    DevBuf tmp, span;
+    const size_t tb = scan_temp_bytes(M);
+    TRY(tmp.alloc(ctx, tb));
+    TRY(span.alloc(ctx, sizeof(long long) * 2 * (n + 1)));
+    if (rows > 0) {
+        prof(ctx, "batch.scan", [&] {
+            launch_scan(M, b->d_cnt2.as<int>(), b->d_crp.as<int>(), tmp.p, tb, st);
+        });
+    } else {
+        CK(ctx, cudaMemsetAsync(b->d_crp.p, 0, sizeof(int), st));
+    }
+    CK(ctx, cudaGetLastError());
+    std::vector<long long> hspan(2 * static_cast<size_t>(n) + 2, 0);
+    if (n > 0) {
+        k_batch_item_spans<<<(n + 255) / 256, 256, 0, st>>>(b->d_items.as<BItem>(), n,
+                                                           b->d_crp.as<int>(),
+                                                           span.as<long long>());
+        note_launch();
+        CK(ctx, cudaGetLastError());
+        CK(ctx, cudaMemcpyAsync(hspan.data(), span.p, sizeof(long long) * 2 * n,
+                                cudaMemcpyDeviceToHost, st));
+    }
+    if (rows > 0)
+        launch_need_from_counts(M, b->d_cnt2.as<int>(), b->d_cnt1.as<int>(), b->d_need.as<int>(),
+                                st);
+    TRY(bin_rows(ctx, M, b->d_need.as<int>(), 0, 32, dc + 1, nullptr, b->nbins));
+    TRY(check_device_err(ctx));
+    long long nnz = 0;
+    for (int i = 0; i < n; ++i) nnz += hspan[2 * i + 1];
+    if (nnz >= INT32_MAX) return batch_fail(b, SP3MM_ELIMIT, "the batch has too many nonzeros");
+    b->nnz = nnz;
+
+    // Outputs: one array of columns and values for the batch, one array of
+    // local row pointers per product.
+    TRY(b->d_ci.alloc(ctx, sizeof(int) * static_cast<size_t>(nnz)));
+    TRY(b->d_v.alloc(ctx, vbytes(b->to) * static_cast<size_t>(nnz)));
+    b->rp_off.assign(n, 0);
+    long long rp_total = 0;
+    for (int i = 0; i < n; ++i) {
+        b->rp_off[i] = rp_total;
+        rp_total += b->items[i].M + 1;
+    }
+    TRY(b->d_rp.alloc(ctx, sizeof(int) * static_cast<size_t>(rp_total)));
+    TRY(b->d_rp_off.alloc(ctx, sizeof(long long) * std::max(n, 1)));
+    CK(ctx, cudaMemsetAsync(b->d_rp.p, 0, sizeof(int) * static_cast<size_t>(rp_total), st));
+    if (n > 0)
+        CK(ctx, cudaMemcpyAsync(b->d_rp_off.p, b->rp_off.data(), sizeof(long long) * n,
+                                cudaMemcpyHostToDevice, st));
+    if (rows > 0) {
+        k_batch_local_rp<<<grid_for_rows(rows), 256, 0, st>>>(
+            b->d_items.as<BItem>(), b->d_row_item.as<int>(), b->d_rp_off.as<long long>(), rows,
+            b->d_crp.as<int>(), b->d_rp.as<int>());
+        note_launch();
+        CK(ctx, cudaGetLastError());
+    }
+    for (int i = 0; i < n; ++i) {
+        sp3mm_dcsr& C = b->results[i];
+        C.M = b->items[i].M;
+        C.N = b->items[i].N;
+        C.nnz = hspan[2 * i + 1];
+        C.row_ptr = b->d_rp.as<int>() + b->rp_off[i];
+        C.col = b->d_ci.as<int>() + hspan[2 * i];
+        C.val = static_cast<unsigned char*>(b->d_v.p) + vbytes(b->to) * hspan[2 * i];
+        C.val_type = b->to;
+        C.max_row = -1;
+    }
+    TRY(build_numeric(b));
+    b->planned = true;
+    return SP3MM_OK;
+}
+
+int check_operand(sp3mm_ctx* ctx, const sp3mm_dcsr& m, int tv, const char* what) {
+    TRY(check_dcsr(ctx, &m, what));
+    if (m.val_type != tv)
+        return set_error(ctx, SP3MM_EINVAL, "batch: %s has another value type", what);
+    return SP3MM_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int sp3mm_batch_create(sp3mm_ctx* ctx, int n, const int* kinds, const sp3mm_dcsr* X,
+                       const sp3mm_dcsr* Y, const sp3mm_dcsr* Z, int out_val_type,
+                       sp3mm_batch** out) {
+    if (!ctx || !out || n < 0 || (n > 0 && (!kinds || !X || !Y)))
+        return set_error(ctx, SP3MM_EINVAL, "batch: invalid arguments");
+    if (out_val_type != SP3MM_F64 && out_val_type != SP3MM_F32)
+        return set_error(ctx, SP3MM_EINVAL, "batch: unknown output value type");
+    auto* b = new sp3mm_batch();
+    b->ctx = ctx;
+    b->to = out_val_type;
+    b->tv = n > 0 ? X[0].val_type : SP3MM_F64;
+    b->items.resize(n);
+    b->bases.assign(n + 1, 0);
+    long long rows = 0;
+    for (int i = 0; i < n; ++i) {
+        BItem& I = b->items[i];
+        int rc = SP3MM_OK;
+        if (kinds[i] != SP3MM_BATCH_SPMM && kinds[i] != SP3MM_BATCH_RAP)
+            rc = set_error(ctx, SP3MM_EINVAL, "batch: product %d has an unknown kind", i);
+        if (rc == SP3MM_OK) rc = check_operand(ctx, X[i], b->tv, "X");
+        if (rc == SP3MM_OK) rc = check_operand(ctx, Y[i], b->tv, "Y");
+        if (rc == SP3MM_OK && X[i].N != Y[i].M)
+            rc = set_error(ctx, SP3MM_EINVAL, "batch: product %d: X.N != Y.M", i);
+        if (rc == SP3MM_OK && kinds[i] == SP3MM_BATCH_RAP) {
+            if (!Z) rc = set_error(ctx, SP3MM_EINVAL, "batch: product %d needs Z", i);
+            if (rc == SP3MM_OK) rc = check_operand(ctx, Z[i], b->tv, "Z");
+            if (rc == SP3MM_OK && Y[i].N != Z[i].M)
+                rc = set_error(ctx, SP3MM_EINVAL, "batch: product %d: Y.N != Z.M", i);
+        }
+        if (rc != SP3MM_OK) {
+            delete b;
+            return rc;
+        }
+        I.X = view(X[i]);
+        I.Y = view(Y[i]);
+        I.kind = kinds[i] == SP3MM_BATCH_RAP ? kBatchDirect : kBatchPair;
+        if (I.kind == kBatchDirect) I.Z = view(Z[i]);
+        else I.Z = CsrView{};
+        I.M = X[i].M;
+        I.N = I.kind == kBatchDirect ? Z[i].N : Y[i].N;
+        I.row_base = rows;
+        b->bases[i] = rows;
+        rows += X[i].M;
+    }
+    b->bases[n] = rows;
+    if (rows >= INT32_MAX) {
+        delete b;
+        return set_error(ctx, SP3MM_ELIMIT, "batch: too many rows");
+    }
+    b->rows = rows;
+    *out = b;
+    return SP3MM_OK;
+}
+
+int sp3mm_batch_set_tuning(sp3mm_batch* b, int d1, int d2, int slack, int nsplits,
+                           const int32_t* splits) {
+    if (!b || d1 < 0 || d1 > 8 || d2 < 0 || d2 > 8 || slack < 0 || slack > 3 ||
+        (nsplits > 0 && !splits))
+        return batch_fail(b, SP3MM_EINVAL, "invalid tuning");
+    b->d1 = d1;
+    b->d2 = d2;
+    const bool numeric_changed =
+        slack != b->slack || (nsplits < 0) != b->auto_split ||
+        (nsplits >= 0 && std::vector<int>(splits, splits + nsplits) != b->splits);
+    b->slack = slack;
+    b->auto_split = nsplits < 0;
+    b->splits.assign(splits && nsplits > 0 ? splits : nullptr,
+                     splits && nsplits > 0 ? splits + nsplits : nullptr);
+    if (b->planned && numeric_changed) return build_numeric(b);
+    return SP3MM_OK;
+}
+
+int sp3mm_batch_plan(sp3mm_batch* b) {
+    if (!b) return SP3MM_EINVAL;
+    return batch_plan(b);
+}
+
+int sp3mm_batch_execute(sp3mm_batch* b) {
+    if (!b) return SP3MM_EINVAL;
+    if (!b->planned) return batch_fail(b, SP3MM_EINVAL, "execute before plan");
+    sp3mm_ctx* ctx = b->ctx;
+    cudaError_t e = cudaSuccess;
+    prof(ctx, "batch.numeric", [&] { e = cudaGraphLaunch(b->exec, ctx->stream); });
+    CK(ctx, e);
+    return SP3MM_OK;
+}
+
+int sp3mm_batch_run(sp3mm_batch* b) {
+    if (!b) return SP3MM_EINVAL;
+    if (!b->planned) TRY(batch_plan(b));
+    TRY(sp3mm_batch_execute(b));
+    return check_device_err(b->ctx);
+}
+
+int sp3mm_batch_result(const sp3mm_batch* b, int i, sp3mm_dcsr* C) {
+    if (!b || !C || !b->planned || i < 0 || i >= static_cast<int>(b->results.size()))
+        return SP3MM_EINVAL;
+    *C = b->results[i];
+    return SP3MM_OK;
+}
+
+int sp3mm_batch_info(const sp3mm_batch* b, int64_t* rows, int64_t* nnz, int* tiers,
+                     int* global_tiers) {
+    if (!b) return SP3MM_EINVAL;
+    if (rows) *rows = b->rows;
+    if (nnz) *nnz = b->nnz;
+    int t = 0, g = 0;
+    for (const auto& x : b->tiers) (x.gt ? g : t)++;
+    if (tiers) *tiers = t + g;
+    if (global_tiers) *global_tiers = g;
+    return SP3MM_OK;
+}
+
+int sp3mm_batch_free(sp3mm_batch* b) {
+    if (!b) return SP3MM_EINVAL;
+    cudaStreamSynchronize(b->ctx->stream);
+    delete b;
+    return SP3MM_OK;
+}
+
+int sp3mm_batch_autotune(sp3mm_batch* b, int reps, char* report, size_t len) {
+    if (!b || reps < 1) return SP3MM_EINVAL;
+    sp3mm_ctx* ctx = b->ctx;
+    const cudaStream_t st = ctx->stream;
+    if (!b->planned) TRY(batch_plan(b));
+    struct Cand {
+        bool autos;
+        std::vector<int> splits;
+        int slack;
+        float ms;
+    };
+    std::vector<int> present;
+    for (int L = 0; L < kLevels; ++L)
+        if (b->nbins.counts[L]) present.push_back(L);
+    std::vector<Cand> cands;
+    for (int slack = 0; slack <= 1; ++slack) {
+        cands.push_back({true, {}, slack, 0.f});
+        cands.push_back({false, {}, slack, 0.f});
+        for (size_t k = 1; k < present.size() && k <= 4; ++k)
+            cands.push_back({false, {present[k]}, slack, 0.f});
+    }
+    std::string rep;
+    size_t best = 0;
+    for (size_t c = 0; c < cands.size(); ++c) {
+        Cand& k = cands[c];
+        b->auto_split = k.autos;
+        b->splits = k.splits;
+        b->slack = k.slack;
+        TRY(build_numeric(b));
+        CK(ctx, cudaGraphLaunch(b->exec, st));   // warm-up
+        CK(ctx, cudaEventRecord(ctx->ev0, st));
+        for (int r = 0; r < reps; ++r) CK(ctx, cudaGraphLaunch(b->exec, st));
+        CK(ctx, cudaEventRecord(ctx->ev1, st));
+        CK(ctx, cudaEventSynchronize(ctx->ev1));
+        float ms = 0.f;
+        CK(ctx, cudaEventElapsedTime(&ms, ctx->ev0, ctx->ev1));
+        k.ms = ms / reps;
+        char line[160];
+        snprintf(line, sizeof line, "%s split=%d slack=%d tiers=%zu ms=%.4f\n",
+                 k.autos ? "per-level" : (k.splits.empty() ? "one-tier" : "two-tier"),
+                 k.splits.empty() ? -1 : k.splits[0], k.slack, b->tiers.size(), k.ms);
+        rep += line;
+        if (k.ms < cands[best].ms || c == 0) best = c;
+    }
+    TRY(check_device_err(ctx));
+    b->auto_split = cands[best].autos;
+    b->splits = cands[best].splits;
+    b->slack = cands[best].slack;
+    TRY(build_numeric(b));
+    if (report && len) {
+        snprintf(report, len, "%s", rep.c_str());
+    }
+    return SP3MM_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,52 @@
+// batch.cuh -- descriptors and launchers of the batch row kernels.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include "kernels.cuh"
+
+namespace sp3mm {
+
+enum : int { kBatchPair = 0, kBatchDirect = 1 };
+
+// One product of a batch: C = X*Y (pair) or C = X*Y*Z (direct).
+struct BItem {
+    CsrView X, Y, Z;
+    int kind;
+    int M, N;              // shape of C
+    long long row_base;    // first global row
+};
+
+struct BatchRowParams {
+    const int* rows;        // global rows of this launch
+    const int* nrows_dev;   // when set, the row count is read from here
+    int nrows;
+    int scap;               // slots per table in each warp's region
+    int d1, d2;             // symbolic: optimistic table shifts
+    int slack;              // numeric: tables 2^slack times the exact size
+    int reverse;            // walk the list from its end (largest rows first)
+    const int* need;        // symbolic: first-table bound per global row
+    int* cnt1;              // direct R*A distinct count (out: symbolic, in: numeric)
+    int* cnt2;              // C row length (out: symbolic, in: numeric)
+    const int* c_rp;        // numeric: global row pointers into c_ci / c_v
+    int* c_ci;
+    void* c_v;
+    int* retry_rows;        // rows whose proven tables exceed scap
+    int* retry_count;
+    int* retry_need;        // largest proven table bound among them
+    unsigned char* gtab;    // global-memory regions (GT), gstride bytes each
+    long long gstride;
+    unsigned* err;
+};
+
+// Sets the kernel's dynamic shared memory limit to `max_smem` and returns
+// how many CTAs of `block` threads with `smem` bytes each fit one SM.
+cudaError_t batch_rows_configure(int mode, bool gt, int tv, int to, int block, size_t smem,
+                                 size_t max_smem, int* ctas_per_sm);
+cudaError_t launch_batch_rows(int mode, bool gt, int tv, int to, int grid, int block,
+                              size_t smem, cudaStream_t st, const BItem* items,
+                              const int* row_item, const BatchRowParams& p);
+size_t batch_row_region_bytes(bool num, int scap);
+int batch_slots_for(long long need);
+
+}  // namespace sp3mm

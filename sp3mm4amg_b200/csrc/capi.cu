@@ -17,6 +17,7 @@
 #include <string>
 #include <vector>
 
+#include "context.cuh"
 #include "kernels.cuh"
 #include "sp3mm_b200.h"
 #include "sp3mm_internal.cuh"
@@ -25,60 +26,7 @@ using namespace sp3mm;
 
 double Start = 0.0, End = 0.0, Elapsed = 0.0, ElapsedInternal = 0.0;
 
-struct sp3mm_ctx {
-    int device = 0;
-    int num_sms = 148;
-    cudaStream_t own_stream = nullptr;
-    cudaStream_t stream = nullptr;
-    unsigned* d_err = nullptr;           // sticky device error word
-    size_t ws_limit = 0;
-    size_t smem_budget = 110 * 1024;
-    // Row-kernel tuning: lanes per row (0: from the operands' mean row
-    // length), table-size shifts d1 (first table from bound >> d1; < 0:
-    // default) and d2 (direct second table = first >> d2).
-    int tune_G = 0, tune_d1 = -1, tune_d2 = -1;
-    std::string last_error;
-    cudaEvent_t ev0 = nullptr, ev1 = nullptr;
-    // Optional per-launch timing (events on the context stream).
-    struct ProfRec {
-        const char* label;
-        cudaEvent_t a, b;
-    };
-    bool profiling = false;
-    std::vector<ProfRec> prof;
-};
-
-namespace {
-
-void prof_clear(sp3mm_ctx* ctx) {
-    for (auto& r : ctx->prof) {
-        cudaEventDestroy(r.a);
-        cudaEventDestroy(r.b);
-    }
-    ctx->prof.clear();
-}
-
-// Run `f` (which launches kernels on ctx->stream), bracketed by events when
-// profiling is on.
-template <typename F>
-void prof(sp3mm_ctx* ctx, const char* label, F&& f) {
-    if (!ctx->profiling) {
-        f();
-        return;
-    }
-    sp3mm_ctx::ProfRec r{label, nullptr, nullptr};
-    cudaEventCreate(&r.a);
-    cudaEventCreate(&r.b);
-    cudaEventRecord(r.a, ctx->stream);
-    f();
-    cudaEventRecord(r.b, ctx->stream);
-    ctx->prof.push_back(r);
-}
-
-double wall_seconds() {
-    using namespace std::chrono;
-    return duration<double>(steady_clock::now().time_since_epoch()).count();
-}
+namespace sp3mm {
 
 int set_error(sp3mm_ctx* ctx, int code, const char* fmt, ...) {
     char buf[512];
@@ -91,59 +39,6 @@ int set_error(sp3mm_ctx* ctx, int code, const char* fmt, ...) {
     return code;
 }
 
-#define CK(ctx, call)                                                                   \
-    do {                                                                                \
-        cudaError_t e_ = (call);                                                        \
-        if (e_ != cudaSuccess)                                                          \
-            return set_error((ctx), SP3MM_ECUDA, "%s failed: %s (%s:%d)", #call,        \
-                             cudaGetErrorString(e_), __FILE__, __LINE__);               \
-    } while (0)
-
-#define TRY(expr)                 \
-    do {                          \
-        int rc_ = (expr);         \
-        if (rc_ != SP3MM_OK) return rc_; \
-    } while (0)
-
-// Stream-ordered device allocation from the device's memory pool.
-struct DevBuf {
-    sp3mm_ctx* ctx = nullptr;
-    void* p = nullptr;
-    DevBuf() = default;
-    DevBuf(const DevBuf&) = delete;
-    DevBuf& operator=(const DevBuf&) = delete;
-    ~DevBuf() { release(); }
-    int alloc(sp3mm_ctx* c, size_t bytes) {
-        release();
-        ctx = c;
-        if (bytes == 0) bytes = 16;
-        cudaError_t e = cudaMallocAsync(&p, bytes, c->stream);
-        if (e != cudaSuccess) {
-            p = nullptr;
-            cudaGetLastError();
-            return set_error(c, SP3MM_ENOMEM, "device allocation of %zu bytes failed: %s", bytes,
-                             cudaGetErrorString(e));
-        }
-        return SP3MM_OK;
-    }
-    void release() {
-        if (p && ctx) cudaFreeAsync(p, ctx->stream);
-        p = nullptr;
-    }
-    void* detach() {
-        void* q = p;
-        p = nullptr;
-        return q;
-    }
-    template <typename T> T* as() const { return static_cast<T*>(p); }
-};
-
-CsrView view(const sp3mm_dcsr& m) {
-    return CsrView{m.M, m.N, m.nnz, m.row_ptr, m.col, m.val, m.val_type};
-}
-
-size_t vbytes(int vt) { return vt == SP3MM_F32 ? 4 : 8; }
-
 int check_dcsr(sp3mm_ctx* ctx, const sp3mm_dcsr* m, const char* what) {
     if (!m) return set_error(ctx, SP3MM_EINVAL, "%s is NULL", what);
     if (m->M < 0 || m->N < 0 || m->nnz < 0 || !m->row_ptr || (m->nnz > 0 && (!m->col || !m->val)))
@@ -152,25 +47,6 @@ int check_dcsr(sp3mm_ctx* ctx, const sp3mm_dcsr* m, const char* what) {
         return set_error(ctx, SP3MM_EINVAL, "%s has an unknown value type", what);
     return SP3MM_OK;
 }
-
-// Small device block of counters used by one binning pass.
-struct Counters {
-    int counts[kLevels + 1];
-    int cursors[kLevels];
-    int nmax;
-    int retry_count;
-    unsigned long long total;
-    unsigned long long cursor;
-};
-
-// Row lists by level, built from per-row `need`.
-struct Bins {
-    int counts[kLevels + 1] = {};
-    int offsets[kLevels] = {};
-    int nmax = 0;
-    unsigned long long total = 0;
-    DevBuf level, lists;
-};
 
 int read_err(sp3mm_ctx* ctx, unsigned* out) {
     CK(ctx, cudaMemcpyAsync(out, ctx->d_err, sizeof(unsigned), cudaMemcpyDeviceToHost,
@@ -190,9 +66,6 @@ int check_device_err(sp3mm_ctx* ctx) {
     return SP3MM_OK;
 }
 
-// Bin M rows by need[i] >> shift for groups of G lanes; `dcnt` is the
-// device counter block (its `total` was accumulated by the bounds kernel);
-// row_cnt of empty rows is zeroed when given.
 int bin_rows(sp3mm_ctx* ctx, int M, const int* need, int shift, int G, Counters* dcnt,
              int* row_cnt, Bins& b) {
     TRY(b.level.alloc(ctx, static_cast<size_t>(M) + 1));
@@ -221,6 +94,23 @@ int bin_rows(sp3mm_ctx* ctx, int M, const int* need, int shift, int G, Counters*
                            ctx->stream);
     });
     return SP3MM_OK;
+}
+
+}  // namespace sp3mm
+
+namespace {
+
+void prof_clear(sp3mm_ctx* ctx) {
+    for (auto& r : ctx->prof) {
+        cudaEventDestroy(r.a);
+        cudaEventDestroy(r.b);
+    }
+    ctx->prof.clear();
+}
+
+double wall_seconds() {
+    using namespace std::chrono;
+    return duration<double>(steady_clock::now().time_since_epoch()).count();
 }
 
 // Lanes per row: the tuning, else a whole warp (the warp kernels); the
@@ -600,6 +490,7 @@ int ctx_init(sp3mm_ctx* c, int device) {
         return set_error(c, SP3MM_ECUDA, "device %d (sm_%d%d) is not a Blackwell sm_100 GPU",
                          device, prop.major, prop.minor);
     c->num_sms = prop.multiProcessorCount;
+    c->smem_optin = prop.sharedMemPerBlockOptin;
     CK(c, cudaStreamCreateWithFlags(&c->own_stream, cudaStreamNonBlocking));
     c->stream = c->own_stream;
     CK(c, cudaMalloc(&c->d_err, sizeof(unsigned)));
@@ -980,6 +871,26 @@ int sp3mm_dcsr_download_arrays(sp3mm_ctx* ctx, const sp3mm_dcsr* m, int64_t* row
     TRY(check_dcsr(ctx, m, "matrix"));
     return download_u64(ctx, *m, 0, reinterpret_cast<uint64_t*>(row_ptr),
                         reinterpret_cast<uint64_t*>(col), val);
+}
+
+int sp3mm_dcsr_set_values(sp3mm_ctx* ctx, sp3mm_dcsr* m, const double* val) {
+    if (!ctx || !m) return SP3MM_EINVAL;
+    TRY(check_dcsr(ctx, m, "matrix"));
+    if (m->nnz > 0 && !val) return set_error(ctx, SP3MM_EINVAL, "values are NULL");
+    if (m->nnz == 0) return SP3MM_OK;
+    const cudaStream_t st = ctx->stream;
+    if (m->val_type == SP3MM_F64) {
+        CK(ctx, cudaMemcpyAsync(m->val, val, sizeof(double) * m->nnz, cudaMemcpyHostToDevice, st));
+    } else {
+        DevBuf stage;
+        TRY(stage.alloc(ctx, sizeof(double) * m->nnz));
+        CK(ctx, cudaMemcpyAsync(stage.p, val, sizeof(double) * m->nnz, cudaMemcpyHostToDevice,
+                                st));
+        launch_convert_values(m->nnz, stage.p, SP3MM_F64, m->val, m->val_type, st);
+        CK(ctx, cudaGetLastError());
+    }
+    CK(ctx, cudaStreamSynchronize(st));
+    return SP3MM_OK;
 }
 
 int sp3mm_dcsr_free(sp3mm_ctx* ctx, sp3mm_dcsr* m) {
