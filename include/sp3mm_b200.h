@@ -365,6 +365,15 @@ SP3MM_API int sp3mm_hierarchy_levels(const sp3mm_hierarchy *h);
 SP3MM_API int sp3mm_hierarchy_get(const sp3mm_hierarchy *h, int level, sp3mm_dcsr *A,
                                   sp3mm_dcsr *P, sp3mm_dcsr *R);
 SP3MM_API int sp3mm_hierarchy_free(sp3mm_ctx *ctx, sp3mm_hierarchy *h);
+/* n hierarchies built level-synchronously: each step forms the next level
+ * of every unfinished hierarchy with batched launches (one SpMM batch for
+ * the A*P0 products, one batch of direct triple products), so results equal
+ * n calls of sp3mm_hierarchy_build with variant SP3MM_DIRECT.  dims holds
+ * 3 entries per hierarchy (the first ndims[i] are used). */
+SP3MM_API int sp3mm_hierarchy_build_batch(sp3mm_ctx *ctx, int n, const sp3mm_dcsr *A0,
+                                          const int32_t *dims, const int32_t *ndims, int block,
+                                          double omega, int64_t min_coarse, int max_levels,
+                                          int coarse_val_type, sp3mm_hierarchy **out);
 
 #ifdef __cplusplus
 }

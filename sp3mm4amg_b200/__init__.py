@@ -310,6 +310,25 @@ class Context:
             variant, flavour, coarse_val_type, ctypes.byref(h)))
         return Hierarchy(self, h)
 
+    def hierarchies(self, A0s, dims_list, block: int = 2, omega: float = 2.0 / 3.0,
+                    min_coarse: int = 64, max_levels: int = 10,
+                    coarse_val_type: int = F64) -> list:
+        """Hierarchies over each A0 (borrowed), built level-synchronously with
+        batched launches (direct products)."""
+        n = len(A0s)
+        arr = (sp3mm_dcsr * max(n, 1))(*[a.d for a in A0s])
+        dims = (ctypes.c_int32 * max(3 * n, 1))()
+        nd = (ctypes.c_int32 * max(n, 1))()
+        for i, dm in enumerate(dims_list):
+            nd[i] = len(dm)
+            for j, x in enumerate((list(dm) + [1, 1])[:3]):
+                dims[3 * i + j] = x
+        out = (ctypes.c_void_p * max(n, 1))()
+        self._check(self.lib.sp3mm_hierarchy_build_batch(
+            self.h, n, arr, dims, nd, block, float(omega), min_coarse, max_levels,
+            coarse_val_type, out))
+        return [Hierarchy(self, ctypes.c_void_p(out[i])) for i in range(n)]
+
     def batch(self, products, out_val_type: int = F64) -> "Batch":
         """A batch of independent products: (X, Y) for X*Y, (X, Y, Z) for
         the direct X*Y*Z."""

@@ -67,6 +67,9 @@ DEVICE_API = {
     "sp3mm_hierarchy_get": (_c.c_int, [_c.c_void_p, _c.c_int, _c.c_void_p, _c.c_void_p,
                                        _c.c_void_p]),
     "sp3mm_hierarchy_free": (_c.c_int, [_c.c_void_p, _c.c_void_p]),
+    "sp3mm_hierarchy_build_batch": (_c.c_int, [_c.c_void_p, _c.c_int, _c.c_void_p, _c.c_void_p,
+                                               _c.c_void_p, _c.c_int, _c.c_double, _c.c_int64,
+                                               _c.c_int, _c.c_int, _c.c_void_p]),
     "sp3mm_batch_create": (_c.c_int, [_c.c_void_p, _c.c_int, _c.c_void_p, _c.c_void_p,
                                       _c.c_void_p, _c.c_void_p, _c.c_int,
                                       _c.POINTER(_c.c_void_p)]),

@@ -526,6 +526,27 @@ int check_operand(sp3mm_ctx* ctx, const sp3mm_dcsr& m, int tv, const char* what)
 
 }  // namespace
 
+namespace sp3mm {
+
+void batch_trim(sp3mm_batch* b) {
+    b->drop_graph();
+    b->tiers.clear();
+    b->d_items.release();
+    b->d_bases.release();
+    b->d_row_item.release();
+    b->d_need.release();
+    b->d_cnt1.release();
+    b->d_cnt2.release();
+    b->d_crp.release();
+    b->d_rp_off.release();
+    b->d_counters.release();
+    b->num_gtab.release();
+    b->nbins.level.release();
+    b->nbins.lists.release();
+}
+
+}  // namespace sp3mm
+
 extern "C" {
 
 int sp3mm_batch_create(sp3mm_ctx* ctx, int n, const int* kinds, const sp3mm_dcsr* X,
@@ -608,6 +629,7 @@ int sp3mm_batch_plan(sp3mm_batch* b) {
 int sp3mm_batch_execute(sp3mm_batch* b) {
     if (!b) return SP3MM_EINVAL;
     if (!b->planned) return batch_fail(b, SP3MM_EINVAL, "execute before plan");
+    if (!b->exec) return batch_fail(b, SP3MM_EINVAL, "the batch was trimmed");
     sp3mm_ctx* ctx = b->ctx;
     cudaError_t e = cudaSuccess;
     prof(ctx, "batch.numeric", [&] { e = cudaGraphLaunch(b->exec, ctx->stream); });

@@ -5,6 +5,8 @@
 
 #include "kernels.cuh"
 
+struct sp3mm_batch;
+
 namespace sp3mm {
 
 enum : int { kBatchPair = 0, kBatchDirect = 1 };
@@ -47,6 +49,9 @@ cudaError_t launch_batch_rows(int mode, bool gt, int tv, int to, int grid, int b
                               size_t smem, cudaStream_t st, const BItem* items,
                               const int* row_item, const BatchRowParams& p);
 size_t batch_row_region_bytes(bool num, int scap);
+// Release a planned, executed batch's planning state and graph; its
+// results stay valid, execute is no longer possible.
+void batch_trim(::sp3mm_batch* b);
 int batch_slots_for(long long need);
 
 }  // namespace sp3mm

@@ -1,0 +1,457 @@
+// hbatch.cu -- level-synchronous construction of many hierarchies.
+//
+// Every step advances a set of hierarchies by one level with the same
+// arithmetic as the single build (hierarchy.cu): P = (I - omega D^-1 A) P0
+// on the pattern of A*P0, R = P^T, A_c = R A P (direct product).  Instead of
+// a dozen launches and several host round trips per hierarchy, a step runs
+//
+//   labels + diagonals        one launch over the rows of all hierarchies
+//   A*P0                      one batch (sp3mm_batch, SpMM products)
+//   Jacobi combine            one launch
+//   transpose                 column counts, scan, scatter, row sort and
+//                             local row pointers over the block-diagonal
+//                             concatenation of all P (five launches)
+//   R*A*P                     one batch (direct triple products)
+//
+// Matrices built by a step live in arenas shared by the step's hierarchies
+// (the two batches' result arrays and the restriction arrays); each
+// hierarchy keeps them alive.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <climits>
+#include <memory>
+#include <vector>
+
+#include "batch.cuh"
+#include "context.cuh"
+#include "hierarchy.cuh"
+#include "sp3mm_b200.h"
+
+using namespace sp3mm;
+
+namespace {
+
+// One hierarchy of a step (device descriptor).
+struct HStep {
+    CsrView A;             // the hierarchy's coarsest operator
+    int nx, ny, nz, block;
+    int nc;                // coarse size
+    long long row_base;    // first global fine row
+    long long col_base;    // first global coarse column
+    double omega;
+    CsrView AP0;           // A*P0: the pattern of P, FP64 values
+    void* pv;              // P values (AP0's array when FP64)
+    int pvt;
+    long long r_base;      // first entry of this R in the step's R arrays
+};
+
+__device__ __forceinline__ int find_base(const long long* __restrict__ bases, int n, long long g) {
+    int lo = 0, hi = n;   // largest b with bases[b] <= g (bases[n] = total)
+    while (hi - lo > 1) {
+        const int mid = (lo + hi) >> 1;
+        if (__ldg(bases + mid) <= g) lo = mid;
+        else hi = mid;
+    }
+    return lo;
+}
+
+__device__ __forceinline__ double vload(const void* p, int vt, long long i) {
+    return vt == SP3MM_F32 ? static_cast<double>(static_cast<const float*>(p)[i])
+                           : static_cast<const double*>(p)[i];
+}
+__device__ __forceinline__ void vstore(void* p, int vt, long long i, double v) {
+    if (vt == SP3MM_F32) static_cast<float*>(p)[i] = __double2float_rn(v);
+    else static_cast<double*>(p)[i] = v;
+}
+
+// agg[g] = block of fine point g on its hierarchy's coarse grid (local
+// coarse index); d[g] = diagonal entry (flag when missing or zero).
+__global__ void k_hs_labels(const HStep* __restrict__ hs, const long long* __restrict__ bases,
+                            int n, long long rows, int* agg, double* d, unsigned* err) {
+    for (long long g = blockIdx.x * (long long)blockDim.x + threadIdx.x; g < rows;
+         g += (long long)gridDim.x * blockDim.x) {
+        const HStep& h = hs[find_base(bases, n, g)];
+        const long long i = g - h.row_base;
+        const int b = h.block;
+        const int cx = (h.nx + b - 1) / b, cy = (h.ny + b - 1) / b;
+        const long long x = i % h.nx, y = (i / h.nx) % h.ny,
+                        z = i / (static_cast<long long>(h.nx) * h.ny);
+        agg[g] = static_cast<int>(x / b + cx * (y / b + static_cast<long long>(cy) * (z / b)));
+        int lo = h.A.rp[i], hi = h.A.rp[i + 1];
+        double v = 0.0;
+        while (lo < hi) {
+            const int mid = (lo + hi) >> 1;
+            const int c = h.A.ci[mid];
+            if (c == i) {
+                v = vload(h.A.v, h.A.vtype, mid);
+                break;
+            }
+            if (c < i) lo = mid + 1;
+            else hi = mid;
+        }
+        if (v == 0.0) atomicOr(err, kErrInput);
+        d[g] = v;
+    }
+}
+
+// P = (I - omega D^-1 A) P0 on the pattern of A*P0: s = omega / d_i, then
+// [j == agg(i)] - s * (A P0)_ij, separately rounded (the single build's
+// arithmetic).
+__global__ void k_hs_jacobi(const HStep* __restrict__ hs, const long long* __restrict__ bases,
+                            int n, long long rows, const int* agg, const double* d) {
+    for (long long g = blockIdx.x * (long long)blockDim.x + threadIdx.x; g < rows;
+         g += (long long)gridDim.x * blockDim.x) {
+        const HStep& h = hs[find_base(bases, n, g)];
+        const int i = static_cast<int>(g - h.row_base);
+        const double s = __ddiv_rn(h.omega, d[g]);
+        const int a = agg[g];
+        const double* x = static_cast<const double*>(h.AP0.v);
+        for (int j = h.AP0.rp[i]; j < h.AP0.rp[i + 1]; ++j) {
+            const double y = __dmul_rn(s, x[j]);
+            vstore(h.pv, h.pvt, j, h.AP0.ci[j] == a ? __dsub_rn(1.0, y) : -y);
+        }
+    }
+}
+
+// Transpose of the block-diagonal concatenation of all P: entries per
+// global coarse column.
+__global__ void k_hs_colcount(const HStep* __restrict__ hs, const long long* __restrict__ bases,
+                              int n, long long rows, int* cnt) {
+    for (long long g = blockIdx.x * (long long)blockDim.x + threadIdx.x; g < rows;
+         g += (long long)gridDim.x * blockDim.x) {
+        const HStep& h = hs[find_base(bases, n, g)];
+        const int i = static_cast<int>(g - h.row_base);
+        for (int j = h.AP0.rp[i]; j < h.AP0.rp[i + 1]; ++j)
+            atomicAdd(cnt + h.col_base + h.AP0.ci[j], 1);
+    }
+}
+
+__global__ void k_hs_scatter(const HStep* __restrict__ hs, const long long* __restrict__ bases,
+                             int n, long long rows, const int* grp, int* cursor, int* r_ci,
+                             void* r_v, int vt) {
+    for (long long g = blockIdx.x * (long long)blockDim.x + threadIdx.x; g < rows;
+         g += (long long)gridDim.x * blockDim.x) {
+        const HStep& h = hs[find_base(bases, n, g)];
+        const int i = static_cast<int>(g - h.row_base);
+        for (int j = h.AP0.rp[i]; j < h.AP0.rp[i + 1]; ++j) {
+            const long long c = h.col_base + h.AP0.ci[j];
+            const long long pos = grp[c] + atomicAdd(cursor + c, 1);
+            r_ci[pos] = i;
+            vstore(r_v, vt, pos, vload(h.pv, h.pvt, j));
+        }
+    }
+}
+
+// Local row pointers of every R: r_rp[r_rp_off[h] + j] = grp[col_base + j]
+// - grp[col_base] for j = 0..nc.
+__global__ void k_hs_local_rp(const HStep* __restrict__ hs, const long long* __restrict__ cbases,
+                              int n, long long cols, const int* grp, const long long* r_rp_off,
+                              int* r_rp) {
+    for (long long c = blockIdx.x * (long long)blockDim.x + threadIdx.x; c < cols;
+         c += (long long)gridDim.x * blockDim.x) {
+        const int b = find_base(cbases, n, c);
+        const HStep& h = hs[b];
+        const int j = static_cast<int>(c - h.col_base);
+        const int c0 = grp[h.col_base];
+        int* out = r_rp + r_rp_off[b];
+        out[j] = grp[c] - c0;
+        if (j == h.nc - 1) out[j + 1] = grp[c + 1] - c0;
+    }
+}
+
+__global__ void k_hs_fill(long long n, int* iota, void* ones, int vt) {
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i <= n;
+         i += (long long)gridDim.x * blockDim.x) {
+        iota[i] = static_cast<int>(i);
+        if (i < n) vstore(ones, vt, i, 1.0);
+    }
+}
+
+int grid_of(long long work) {
+    const long long g = (work + 255) / 256;
+    return static_cast<int>(std::max<long long>(1, std::min<long long>(g, 148LL * 32)));
+}
+
+// Device memory released when the last hierarchy holding it is freed.
+struct Arena {
+    sp3mm_ctx* ctx;
+    std::vector<void*> ptrs;
+    explicit Arena(sp3mm_ctx* c) : ctx(c) {}
+    ~Arena() {
+        for (void* p : ptrs) cudaFreeAsync(p, ctx->stream);
+    }
+    void* take(DevBuf& b) {
+        void* p = b.detach();
+        ptrs.push_back(p);
+        return p;
+    }
+};
+
+std::shared_ptr<sp3mm_batch> hold(sp3mm_batch* b) {
+    return std::shared_ptr<sp3mm_batch>(b, [](sp3mm_batch* p) { sp3mm_batch_free(p); });
+}
+
+}  // namespace
+
+namespace {
+
+// One step for hierarchies whose coarsest operators share a value type
+// and whose coarse levels share a storage type.
+int step_group(sp3mm_ctx* ctx, const std::vector<sp3mm_hierarchy*>& hs) {
+    const cudaStream_t st = ctx->stream;
+    const int k = static_cast<int>(hs.size());
+    const int tv = hs[0]->A.back().val_type;
+    const int cvt = hs[0]->coarse_val_type;
+    const size_t vb = vbytes(tv);
+    std::vector<HStep> H(k);
+    std::vector<long long> bases(k + 1), cbases(k + 1);
+    long long rows = 0, cols = 0, maxn = 0;
+    for (int t = 0; t < k; ++t) {
+        const sp3mm_hierarchy* h = hs[t];
+        const sp3mm_dcsr& A = h->A.back();
+        const int nx = h->nx.back(), ny = h->ny.back(), nz = h->nz.back(), b = h->block;
+        if (static_cast<long long>(nx) * ny * nz != A.M || A.M != A.N)
+            return set_error(ctx, SP3MM_EINVAL, "hierarchy step: grid does not match operator");
+        HStep& s = H[t];
+        s = HStep{};
+        s.A = view(A);
+        s.nx = nx;
+        s.ny = ny;
+        s.nz = nz;
+        s.block = b;
+        s.nc = ((nx + b - 1) / b) * ((ny + b - 1) / b) * ((nz + b - 1) / b);
+        s.row_base = rows;
+        s.col_base = cols;
+        s.omega = h->omega;
+        s.pvt = tv;
+        bases[t] = rows;
+        cbases[t] = cols;
+        rows += A.M;
+        cols += s.nc;
+        maxn = std::max<long long>(maxn, A.M);
+    }
+    bases[k] = rows;
+    cbases[k] = cols;
+    if (rows >= INT32_MAX || cols >= INT32_MAX)
+        return set_error(ctx, SP3MM_ELIMIT, "hierarchy step: too many rows");
+
+    DevBuf dH, dB, dCB, agg, d, iota, ones, cnt, cursor, grp, tmp, rrp_off;
+    TRY(dH.alloc(ctx, sizeof(HStep) * k));
+    TRY(dB.alloc(ctx, sizeof(long long) * (k + 1)));
+    TRY(dCB.alloc(ctx, sizeof(long long) * (k + 1)));
+    TRY(agg.alloc(ctx, sizeof(int) * rows));
+    TRY(d.alloc(ctx, sizeof(double) * rows));
+    TRY(iota.alloc(ctx, sizeof(int) * (maxn + 1)));
+    TRY(ones.alloc(ctx, vb * maxn));
+    CK(ctx, cudaMemcpyAsync(dH.p, H.data(), sizeof(HStep) * k, cudaMemcpyHostToDevice, st));
+    CK(ctx, cudaMemcpyAsync(dB.p, bases.data(), sizeof(long long) * (k + 1),
+                            cudaMemcpyHostToDevice, st));
+    CK(ctx, cudaMemcpyAsync(dCB.p, cbases.data(), sizeof(long long) * (k + 1),
+                            cudaMemcpyHostToDevice, st));
+    k_hs_fill<<<grid_of(maxn + 1), 256, 0, st>>>(maxn, iota.as<int>(), ones.p, tv);
+    k_hs_labels<<<grid_of(rows), 256, 0, st>>>(dH.as<HStep>(), dB.as<long long>(), k, rows,
+                                               agg.as<int>(), d.as<double>(), ctx->d_err);
+    note_launch();
+    note_launch();
+    CK(ctx, cudaGetLastError());
+
+    // A*P0 for every hierarchy: one SpMM batch.
+    std::vector<int> kinds(k, SP3MM_BATCH_SPMM);
+    std::vector<sp3mm_dcsr> X(k), Y(k), Z(k);
+    for (int t = 0; t < k; ++t) {
+        X[t] = hs[t]->A.back();
+        sp3mm_dcsr& p0 = Y[t];
+        p0.M = static_cast<int>(bases[t + 1] - bases[t]);
+        p0.N = H[t].nc;
+        p0.nnz = p0.M;
+        p0.row_ptr = iota.as<int>();
+        p0.col = agg.as<int>() + bases[t];
+        p0.val = ones.p;
+        p0.val_type = tv;
+        p0.max_row = 1;
+    }
+    sp3mm_batch* raw = nullptr;
+    TRY(sp3mm_batch_create(ctx, k, kinds.data(), X.data(), Y.data(), nullptr, SP3MM_F64, &raw));
+    auto b1 = hold(raw);
+    TRY(sp3mm_batch_run(b1.get()));
+    batch_trim(b1.get());
+
+    // P values (in place when FP64) and the restriction arrays.
+    auto arena = std::make_shared<Arena>(ctx);
+    std::vector<sp3mm_dcsr> AP0(k), P(k), R(k);
+    long long nnz_p = 0;
+    std::vector<long long> r_base(k), rrp(k);
+    long long rrp_total = 0;
+    for (int t = 0; t < k; ++t) {
+        TRY(sp3mm_batch_result(b1.get(), t, &AP0[t]));
+        r_base[t] = nnz_p;
+        nnz_p += AP0[t].nnz;
+        rrp[t] = rrp_total;
+        rrp_total += H[t].nc + 1;
+    }
+    if (nnz_p >= INT32_MAX) return set_error(ctx, SP3MM_ELIMIT, "hierarchy step: P too large");
+    void* p32 = nullptr;
+    if (tv != SP3MM_F64) {
+        DevBuf pv;
+        TRY(pv.alloc(ctx, vb * nnz_p));
+        p32 = arena->take(pv);
+    }
+    for (int t = 0; t < k; ++t) {
+        H[t].AP0 = view(AP0[t]);
+        H[t].pv = p32 ? static_cast<unsigned char*>(p32) + vb * r_base[t] : AP0[t].val;
+        H[t].r_base = r_base[t];
+    }
+    CK(ctx, cudaMemcpyAsync(dH.p, H.data(), sizeof(HStep) * k, cudaMemcpyHostToDevice, st));
+    k_hs_jacobi<<<grid_of(rows), 256, 0, st>>>(dH.as<HStep>(), dB.as<long long>(), k, rows,
+                                               agg.as<int>(), d.as<double>());
+    note_launch();
+    CK(ctx, cudaGetLastError());
+
+    // R = P^T of the block-diagonal concatenation.
+    TRY(cnt.alloc(ctx, sizeof(int) * (cols + 1)));
+    TRY(cursor.alloc(ctx, sizeof(int) * (cols + 1)));
+    TRY(grp.alloc(ctx, sizeof(int) * (cols + 1)));
+    CK(ctx, cudaMemsetAsync(cnt.p, 0, sizeof(int) * (cols + 1), st));
+    CK(ctx, cudaMemsetAsync(cursor.p, 0, sizeof(int) * (cols + 1), st));
+    k_hs_colcount<<<grid_of(rows), 256, 0, st>>>(dH.as<HStep>(), dB.as<long long>(), k, rows,
+                                                 cnt.as<int>());
+    note_launch();
+    const size_t tb = scan_temp_bytes(static_cast<int>(cols));
+    TRY(tmp.alloc(ctx, tb));
+    launch_scan(static_cast<int>(cols), cnt.as<int>(), grp.as<int>(), tmp.p, tb, st);
+    DevBuf rci, rv, rrpb;
+    TRY(rci.alloc(ctx, sizeof(int) * nnz_p));
+    TRY(rv.alloc(ctx, vb * nnz_p));
+    TRY(rrpb.alloc(ctx, sizeof(int) * rrp_total));
+    TRY(rrp_off.alloc(ctx, sizeof(long long) * k));
+    CK(ctx, cudaMemcpyAsync(rrp_off.p, rrp.data(), sizeof(long long) * k, cudaMemcpyHostToDevice,
+                            st));
+    k_hs_scatter<<<grid_of(rows), 256, 0, st>>>(dH.as<HStep>(), dB.as<long long>(), k, rows,
+                                                grp.as<int>(), cursor.as<int>(), rci.as<int>(),
+                                                rv.p, tv);
+    note_launch();
+    launch_sort_rows(static_cast<int>(cols), grp.as<int>(), rci.as<int>(), rv.p, tv, INT_MAX, st);
+    k_hs_local_rp<<<grid_of(cols), 256, 0, st>>>(dH.as<HStep>(), dCB.as<long long>(), k, cols,
+                                                 grp.as<int>(), rrp_off.as<long long>(),
+                                                 rrpb.as<int>());
+    note_launch();
+    CK(ctx, cudaGetLastError());
+    int* r_ci = static_cast<int*>(arena->take(rci));
+    unsigned char* r_v = static_cast<unsigned char*>(arena->take(rv));
+    int* r_rp = static_cast<int*>(arena->take(rrpb));
+    for (int t = 0; t < k; ++t) {
+        const int n = static_cast<int>(bases[t + 1] - bases[t]);
+        P[t] = sp3mm_dcsr{n, H[t].nc, AP0[t].nnz, AP0[t].row_ptr, AP0[t].col,
+                          H[t].pv, tv, -1};
+        R[t] = sp3mm_dcsr{H[t].nc, n, AP0[t].nnz, r_rp + rrp[t], r_ci + r_base[t],
+                          r_v + vb * r_base[t], tv, -1};
+    }
+
+    // A_c = R*A*P for every hierarchy: one batch of direct products.
+    std::vector<int> rk(k, SP3MM_BATCH_RAP);
+    for (int t = 0; t < k; ++t) X[t] = R[t];
+    raw = nullptr;
+    std::vector<sp3mm_dcsr> Aop(k);
+    for (int t = 0; t < k; ++t) Aop[t] = hs[t]->A.back();
+    TRY(sp3mm_batch_create(ctx, k, rk.data(), X.data(), Aop.data(), P.data(), cvt, &raw));
+    auto b2 = hold(raw);
+    TRY(sp3mm_batch_run(b2.get()));
+    batch_trim(b2.get());
+    for (int t = 0; t < k; ++t) {
+        sp3mm_hierarchy* h = hs[t];
+        sp3mm_dcsr Ac{};
+        TRY(sp3mm_batch_result(b2.get(), t, &Ac));
+        const int b = h->block;
+        h->P.push_back(P[t]);
+        h->R.push_back(R[t]);
+        h->A.push_back(Ac);
+        h->nx.push_back((h->nx.back() + b - 1) / b);
+        h->ny.push_back((h->ny.back() + b - 1) / b);
+        h->nz.push_back((h->nz.back() + b - 1) / b);
+        h->nlev = static_cast<int>(h->A.size());
+        h->keep.push_back(b1);
+        h->keep.push_back(b2);
+        h->keep.push_back(arena);
+    }
+    return SP3MM_OK;
+}
+
+}  // namespace
+
+namespace sp3mm {
+
+int hierarchy_step(sp3mm_ctx* ctx, const std::vector<sp3mm_hierarchy*>& all) {
+    // Group by (operator value type, coarse storage type).
+    std::vector<sp3mm_hierarchy*> groups[4];
+    for (sp3mm_hierarchy* h : all)
+        if (h->wants_level())
+            groups[(h->A.back().val_type == SP3MM_F32 ? 2 : 0) +
+                   (h->coarse_val_type == SP3MM_F32 ? 1 : 0)]
+                .push_back(h);
+    for (auto& g : groups)
+        if (!g.empty()) TRY(step_group(ctx, g));
+    return SP3MM_OK;
+}
+
+}  // namespace sp3mm
+
+extern "C" {
+
+int sp3mm_hierarchy_build_batch(sp3mm_ctx* ctx, int n, const sp3mm_dcsr* A0, const int32_t* dims,
+                                const int32_t* ndims, int block, double omega,
+                                int64_t min_coarse, int max_levels, int coarse_val_type,
+                                sp3mm_hierarchy** out) {
+    if (!ctx || n < 0 || (n > 0 && (!A0 || !dims || !ndims || !out)) || block < 2 ||
+        max_levels < 1 || (coarse_val_type != SP3MM_F64 && coarse_val_type != SP3MM_F32))
+        return set_error(ctx, SP3MM_EINVAL, "hierarchy_build_batch: invalid arguments");
+    std::vector<sp3mm_hierarchy*> hs(n, nullptr);
+    auto free_all = [&] {
+        for (auto* h : hs)
+            if (h) sp3mm_hierarchy_free(ctx, h);
+    };
+    for (int i = 0; i < n; ++i) {
+        const int nd = ndims[i];
+        const int32_t* dm = dims + 3 * i;
+        int rc = check_dcsr(ctx, &A0[i], "A0");
+        if (rc == SP3MM_OK && (nd < 1 || nd > 3))
+            rc = set_error(ctx, SP3MM_EINVAL, "hierarchy_build_batch: bad dimension count");
+        const int nx = dm[0], ny = nd > 1 ? dm[1] : 1, nz = nd > 2 ? dm[2] : 1;
+        if (rc == SP3MM_OK && (nx < 1 || ny < 1 || nz < 1 ||
+                               static_cast<long long>(nx) * ny * nz != A0[i].M ||
+                               A0[i].M != A0[i].N))
+            rc = set_error(ctx, SP3MM_EINVAL, "hierarchy_build_batch: grid does not match A0");
+        if (rc != SP3MM_OK) {
+            free_all();
+            return rc;
+        }
+        auto* h = new sp3mm_hierarchy();
+        h->ndim = nd;
+        h->block = block;
+        h->omega = omega;
+        h->min_coarse = min_coarse;
+        h->max_levels = max_levels;
+        h->coarse_val_type = coarse_val_type;
+        h->owns_arrays = false;
+        h->A.push_back(A0[i]);
+        h->nx.push_back(nx);
+        h->ny.push_back(ny);
+        h->nz.push_back(nz);
+        h->nlev = 1;
+        hs[i] = h;
+    }
+    for (;;) {
+        bool any = false;
+        for (auto* h : hs) any = any || h->wants_level();
+        if (!any) break;
+        const int rc = hierarchy_step(ctx, hs);
+        if (rc != SP3MM_OK) {
+            free_all();
+            return rc;
+        }
+    }
+    for (int i = 0; i < n; ++i) out[i] = hs[i];
+    return SP3MM_OK;
+}
+
+}  // extern "C"

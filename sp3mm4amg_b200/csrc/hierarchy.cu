@@ -29,6 +29,7 @@
 #include <cstdio>
 #include <vector>
 
+#include "hierarchy.cuh"
 #include "kernels.cuh"
 #include "sp3mm_b200.h"
 #include "sp3mm_internal.cuh"
@@ -156,12 +157,6 @@ struct Scratch {
 
 using namespace sp3mm;
 
-struct sp3mm_hierarchy {
-    int nlev = 0;
-    std::vector<sp3mm_dcsr> A, P, R;   // A[0] is the caller's (borrowed)
-    std::vector<int> nx, ny, nz;
-};
-
 extern "C" {
 
 int sp3mm_block_prolongator(sp3mm_ctx* ctx, const sp3mm_dcsr* A, const int32_t* dims, int ndim,
@@ -237,12 +232,14 @@ int sp3mm_block_prolongator(sp3mm_ctx* ctx, const sp3mm_dcsr* A, const int32_t* 
 
 int sp3mm_hierarchy_free(sp3mm_ctx* ctx, sp3mm_hierarchy* h) {
     if (!ctx || !h) return SP3MM_EINVAL;
-    for (size_t l = 0; l < h->P.size(); ++l) {
-        sp3mm_dcsr_free(ctx, &h->P[l]);
-        sp3mm_dcsr_free(ctx, &h->R[l]);
+    if (h->owns_arrays) {
+        for (size_t l = 0; l < h->P.size(); ++l) {
+            sp3mm_dcsr_free(ctx, &h->P[l]);
+            sp3mm_dcsr_free(ctx, &h->R[l]);
+        }
+        for (size_t l = 1; l < h->A.size(); ++l) sp3mm_dcsr_free(ctx, &h->A[l]);
     }
-    for (size_t l = 1; l < h->A.size(); ++l) sp3mm_dcsr_free(ctx, &h->A[l]);
-    delete h;
+    delete h;   // releases the shared arenas of a batched build
     return SP3MM_OK;
 }
 
@@ -254,6 +251,12 @@ int sp3mm_hierarchy_build(sp3mm_ctx* ctx, const sp3mm_dcsr* A0, const int32_t* d
         (coarse_val_type != SP3MM_F64 && coarse_val_type != SP3MM_F32))
         return fail(ctx, SP3MM_EINVAL, "hierarchy_build: invalid arguments");
     sp3mm_hierarchy* h = new sp3mm_hierarchy();
+    h->ndim = ndim;
+    h->block = block;
+    h->omega = omega;
+    h->min_coarse = min_coarse;
+    h->max_levels = max_levels;
+    h->coarse_val_type = coarse_val_type;
     h->A.push_back(*A0);
     int nx = dims[0], ny = ndim > 1 ? dims[1] : 1, nz = ndim > 2 ? dims[2] : 1;
     h->nx.push_back(nx);

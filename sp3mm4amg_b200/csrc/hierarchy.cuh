@@ -1,0 +1,39 @@
+// hierarchy.cuh -- the device hierarchy object shared by the single and the
+// batched (level-synchronous) builds and the request server.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <memory>
+#include <vector>
+
+#include "sp3mm_b200.h"
+
+struct sp3mm_hierarchy {
+    int nlev = 0;
+    std::vector<sp3mm_dcsr> A, P, R;   // A[0] is the caller's (borrowed)
+    std::vector<int> nx, ny, nz;
+    // Build parameters.
+    int ndim = 3, block = 2, max_levels = 1, coarse_val_type = SP3MM_F64;
+    long long min_coarse = 0;
+    double omega = 2.0 / 3.0;
+    // Matrices built by the batched build live in shared device arenas
+    // (kept alive here) instead of owning their arrays.
+    bool owns_arrays = true;
+    std::vector<std::shared_ptr<void>> keep;
+
+    // Whether another level should be built.
+    bool wants_level() const {
+        const sp3mm_dcsr& a = A.back();
+        return static_cast<int>(A.size()) < max_levels && a.M >= min_coarse && a.M > 1;
+    }
+};
+
+namespace sp3mm {
+
+// Advance every hierarchy of hs that wants another level by one level,
+// level-synchronously: all their prolongators, restrictions and Galerkin
+// products are formed by a few batched launches (direct triple product).
+int hierarchy_step(sp3mm_ctx* ctx, const std::vector<sp3mm_hierarchy*>& hs);
+
+}  // namespace sp3mm

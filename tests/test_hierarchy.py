@@ -167,3 +167,60 @@ def test_device_hierarchy_max_levels_and_grid_check(orc):
         with pytest.raises(S.Sp3mmError):
             ctx.hierarchy(dA0, (20, 21))
         dA0.free()
+
+
+# ---------------------------------------------------------------- batched build
+
+def _instances():
+    return [(12, 12, 12), (40, 33), (7, 9, 5), (64, 64), (3, 4), (21, 18, 10)]
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("coarse", [S.F64, S.F32])
+def test_device_hierarchies_batched(orc, coarse):
+    """Level-synchronous batched build: every level of every hierarchy
+    equals the oracle chain bit for bit (and so the single build)."""
+    dims_list = _instances()
+    A0s = [pb.poisson3d(*d) if len(d) == 3 else pb.poisson2d(*d) for d in dims_list]
+    wants = [H.chain(orc, A, d, min_coarse=30, max_levels=5, coarse_f32=(coarse == S.F32))
+             for A, d in zip(A0s, dims_list)]
+    with S.Context() as ctx:
+        dA0 = [ctx.upload(A) for A in A0s]
+        hs = ctx.hierarchies(dA0, dims_list, min_coarse=30, max_levels=5,
+                             coarse_val_type=coarse)
+        for h, want in zip(hs, wants):
+            assert len(h) == len(want)
+            for l, (wA, wP, wR) in enumerate(want):
+                A, P, R = h.level(l)
+                _same(A.download(), wA)
+                if wP is None:
+                    assert P is None
+                    continue
+                _same(P.download(), wP)
+                _same(R.download(), wR)
+        # Freeing in any order keeps the others' shared arrays valid.
+        hs[1].free()
+        A, _, _ = hs[0].level(len(hs[0]) - 1)
+        _same(A.download(), wants[0][-1][0])
+        for h in hs:
+            h.free()
+        for a in dA0:
+            a.free()
+
+
+@pytest.mark.gpu
+def test_device_hierarchies_batched_errors():
+    A = pb.poisson2d(6, 6)
+    a = A.to_scipy().tolil()
+    a[2, 2] = 0.0
+    a = a.tocsr()
+    a.eliminate_zeros()
+    with S.Context() as ctx:
+        good, bad = ctx.upload(A), ctx.upload(pb.CSR.from_scipy(a))
+        with pytest.raises(S.Sp3mmError):
+            ctx.hierarchies([good, good], [(6, 6), (6, 5)])
+        with pytest.raises(S.Sp3mmError):
+            ctx.hierarchies([good, bad], [(6, 6), (6, 6)], min_coarse=2)
+        hs = ctx.hierarchies([good], [(6, 6)], min_coarse=2)
+        assert len(hs[0]) >= 2
+        hs[0].free()
