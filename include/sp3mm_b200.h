@@ -306,12 +306,12 @@ SP3MM_API int sp3mm_rap_memory_estimate(const sp3mm_dcsr *R, const sp3mm_dcsr *A
  * The operands are borrowed: they must stay allocated, with unchanged
  * patterns, while the batch is used.
  *
- * sp3mm_batch_plan runs the symbolic pass of every product at once (a few
- * host round trips per batch), allocates the results and captures the
- * numeric pass as a CUDA graph.  sp3mm_batch_execute replays that graph on
- * the context stream without host synchronisation; it may be repeated
- * after the operands' values change.  sp3mm_batch_run = plan (when needed)
- * + execute + error check.  Results are views owned by the batch. */
+ * sp3mm_batch_plan sizes every product at once (a few host round trips
+ * per batch) and allocates the results.  sp3mm_batch_execute replays the
+ * numeric pass, captured as a CUDA graph, on the context stream without
+ * host synchronisation; it may be repeated after the operands' values
+ * change.  sp3mm_batch_run = plan (when needed; values computed) or
+ * execute, then an error check.  Results are views owned by the batch. */
 enum { SP3MM_BATCH_SPMM = 0, SP3MM_BATCH_RAP = 1 };
 typedef struct sp3mm_batch sp3mm_batch;
 SP3MM_API int sp3mm_batch_create(sp3mm_ctx *ctx, int n, const int *kinds, const sp3mm_dcsr *X,
@@ -323,6 +323,12 @@ SP3MM_API int sp3mm_batch_create(sp3mm_ctx *ctx, int n, const int *kinds, const 
  * launch) starts: nsplits < 0 for one tier per level, 0 for a single tier. */
 SP3MM_API int sp3mm_batch_set_tuning(sp3mm_batch *b, int d1, int d2, int slack, int nsplits,
                                      const int32_t *splits);
+/* SP3MM_UB (default): the plan runs one numeric pass in which every row
+ * books its exact length from one cursor, then compacts (the plan computes
+ * the values; the replay graph is built at the first execute).
+ * SP3MM_SYMBNUM: the plan runs a symbolic pass and builds the graph; values
+ * come from execute.  Both give the same results. */
+SP3MM_API int sp3mm_batch_set_flavour(sp3mm_batch *b, int flavour);
 SP3MM_API int sp3mm_batch_plan(sp3mm_batch *b);
 SP3MM_API int sp3mm_batch_execute(sp3mm_batch *b);
 SP3MM_API int sp3mm_batch_run(sp3mm_batch *b);

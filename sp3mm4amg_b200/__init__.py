@@ -329,10 +329,13 @@ class Context:
             coarse_val_type, out))
         return [Hierarchy(self, ctypes.c_void_p(out[i])) for i in range(n)]
 
-    def batch(self, products, out_val_type: int = F64) -> "Batch":
+    def batch(self, products, out_val_type: int = F64, flavour: int = UB) -> "Batch":
         """A batch of independent products: (X, Y) for X*Y, (X, Y, Z) for
         the direct X*Y*Z."""
-        return Batch(self, products, out_val_type)
+        b = Batch(self, products, out_val_type)
+        if flavour != UB:
+            b.set_flavour(flavour)
+        return b
 
     def close(self) -> None:
         if self.h:
@@ -404,6 +407,10 @@ class Batch:
             ns = len(splits)
             arr = (ctypes.c_int32 * max(ns, 1))(*splits)
         self.ctx._check(self.ctx.lib.sp3mm_batch_set_tuning(self.h, d1, d2, slack, ns, arr))
+
+    def set_flavour(self, flavour: int) -> None:
+        """UB: booked single numeric pass in the plan; SYMBNUM: symbolic plan."""
+        self.ctx._check(self.ctx.lib.sp3mm_batch_set_flavour(self.h, flavour))
 
     def plan(self) -> None:
         self.ctx._check(self.ctx.lib.sp3mm_batch_plan(self.h))

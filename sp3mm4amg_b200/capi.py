@@ -75,6 +75,7 @@ DEVICE_API = {
                                       _c.POINTER(_c.c_void_p)]),
     "sp3mm_batch_set_tuning": (_c.c_int, [_c.c_void_p, _c.c_int, _c.c_int, _c.c_int, _c.c_int,
                                           _c.c_void_p]),
+    "sp3mm_batch_set_flavour": (_c.c_int, [_c.c_void_p, _c.c_int]),
     "sp3mm_batch_plan": (_c.c_int, [_c.c_void_p]),
     "sp3mm_batch_execute": (_c.c_int, [_c.c_void_p]),
     "sp3mm_batch_run": (_c.c_int, [_c.c_void_p]),

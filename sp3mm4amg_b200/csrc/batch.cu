@@ -39,8 +39,12 @@ namespace {
 
 // need[g] = distinct-key bound of the first table of global row g (the
 // product count of its row of X*Y, at most Y.N); row_item[g] = its product.
+// *total += the output-size bound of every row (SpMM: need; direct:
+// min(R*A products times Z's longest row, Z.N)).
 __global__ void k_batch_bounds(const BItem* __restrict__ items, const long long* __restrict__ bases,
-                               int n, long long rows, int* need, int* row_item) {
+                               int n, long long rows, int* need, int* row_item,
+                               unsigned long long* total) {
+    unsigned long long ub = 0;
     for (long long g = blockIdx.x * (long long)blockDim.x + threadIdx.x; g < rows;
          g += (long long)gridDim.x * blockDim.x) {
         int lo = 0, hi = n;   // largest b with bases[b] <= g; bases[n] = rows
@@ -61,7 +65,17 @@ __global__ void k_batch_bounds(const BItem* __restrict__ items, const long long*
         }
         need[g] = static_cast<int>(u < I->Y.N ? u : I->Y.N);
         row_item[g] = lo;
+        if (I->kind == kBatchDirect) {
+            const long long zm = I->zmax >= 0 ? I->zmax : I->Z.N;
+            const long long b2 = u * zm;
+            ub += static_cast<unsigned long long>(b2 < I->Z.N ? b2 : I->Z.N);
+        } else {
+            ub += static_cast<unsigned long long>(u < I->Y.N ? u : I->Y.N);
+        }
     }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) ub += __shfl_xor_sync(0xffffffffu, ub, o);
+    if ((threadIdx.x & 31) == 0 && ub) atomicAdd(total, ub);
 }
 
 // Per-product output offset and length from the global row pointers.
@@ -72,6 +86,23 @@ __global__ void k_batch_item_spans(const BItem* __restrict__ items, int n, const
     const long long g0 = items[b].row_base, g1 = g0 + items[b].M;
     span[2 * b] = crp[g0];
     span[2 * b + 1] = static_cast<long long>(crp[g1]) - crp[g0];
+}
+
+// Longest C row of every product (span[2n + b]), from the row counts.
+__global__ void k_batch_item_max(const int* __restrict__ row_item, long long rows,
+                                 const int* cnt, long long* span_max) {
+    for (long long g = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+         g - threadIdx.x % 32 < rows; g += (long long)gridDim.x * blockDim.x) {
+        const bool in = g < rows;
+        const int b = in ? row_item[g] : -1;
+        int m = in ? cnt[g] : 0;
+        // Lanes of one product reduce together; one atomic per product.
+        const unsigned same = __match_any_sync(0xffffffffu, b);
+        m = static_cast<int>(__reduce_max_sync(same, static_cast<unsigned>(m)));
+        if (in && (threadIdx.x & 31) == __ffs(same) - 1 && m > 0)
+            atomicMax(reinterpret_cast<unsigned long long*>(span_max + b),
+                      static_cast<unsigned long long>(m));
+    }
 }
 
 // Local row pointers of every product: rp_local[rp_off[b] + i] =
@@ -118,6 +149,9 @@ struct sp3mm_batch {
     // Tuning: symbolic shifts, numeric slack, tier split levels (a new tier
     // starts at each listed level; empty: one tier per non-empty level).
     int d1 = 2, d2 = 1, slack = 0;
+    int flavour = SP3MM_UB;        // UB: booked numeric plan; SYMBNUM: symbolic plan
+    bool values_ready = false;     // the plan computed the values (UB)
+    bool trimmed = false;
     std::vector<int> splits;
     bool auto_split = true;
     int warps_cap = 8;
@@ -166,11 +200,11 @@ namespace {
 // or the symbolic shift d1 so that a proven-size retry still fits).  Tiers
 // whose region does not fit one CTA's shared memory merge into one
 // global-memory tier.
-int make_tiers(sp3mm_batch* b, const Bins& bins, bool num, int extra, int tv, int to,
+int make_tiers(sp3mm_batch* b, const Bins& bins, int mode, int extra, int tv, int to,
                std::vector<BatchTier>& out) {
     sp3mm_ctx* ctx = b->ctx;
     out.clear();
-    const int mode = num ? kNumExact : kSymb;
+    const bool num = mode != kSymb;
     BatchTier gt;
     gt.gt = true;
     gt.lo = kLevels;
@@ -296,7 +330,7 @@ int build_numeric(sp3mm_batch* b) {
     if (b->graph) cudaGraphDestroy(b->graph);
     b->exec = nullptr;
     b->graph = nullptr;
-    TRY(make_tiers(b, b->nbins, true, b->slack, b->tv, b->to, b->tiers));
+    TRY(make_tiers(b, b->nbins, kNumExact, b->slack, b->tv, b->to, b->tiers));
     size_t need_gt = 0;
     for (const auto& t : b->tiers)
         if (t.gt) need_gt = gt_bytes(t);
@@ -342,6 +376,85 @@ int build_numeric(sp3mm_batch* b) {
 
 namespace {
 
+// The row pass of a plan -- symbolic (kSymb) or booked numeric (kNumBook):
+// tiers of the optimistic levels of `sb`, then rounds for the rows whose
+// proven tables exceed their tier, with global-memory tables sized from the
+// largest proven bound (a direct row learns its second bound only once its
+// first table is complete, hence up to three rounds).
+int row_pass(sp3mm_batch* b, int mode, const Bins& sb, BatchRowParams p, int* rinfo,
+             const char* label) {
+    sp3mm_ctx* ctx = b->ctx;
+    const cudaStream_t st = ctx->stream;
+    const bool num = mode != kSymb;
+    const size_t R1 = static_cast<size_t>(b->rows) + 1;
+    std::vector<BatchTier> tiers;
+    TRY(make_tiers(b, sb, mode, num ? 0 : b->d1, b->tv, b->to, tiers));
+    DevBuf retry_a, retry_b, gtab;
+    TRY(retry_a.alloc(ctx, sizeof(int) * R1));
+    TRY(retry_b.alloc(ctx, sizeof(int) * R1));
+    size_t gb = 0;
+    for (const auto& t : tiers)
+        if (t.gt) gb = gt_bytes(t);
+    if (gb) TRY(gtab.alloc(ctx, gb));
+    CK(ctx, cudaMemsetAsync(rinfo, 0, 2 * sizeof(int), st));
+    p.retry_rows = retry_a.as<int>();
+    p.retry_count = rinfo;
+    p.retry_need = rinfo + 1;
+    if (!tiers.empty()) {
+        int rc = SP3MM_OK;
+        prof(ctx, label, [&] {
+            rc = run_tiers(b, mode, tiers, sb.lists.as<int>(), p, gtab.as<unsigned char>());
+        });
+        TRY(rc);
+    }
+    int* cur = retry_a.as<int>();
+    int* nxt = retry_b.as<int>();
+    for (int round = 0;; ++round) {
+        int h[2] = {0, 0};
+        CK(ctx, cudaMemcpyAsync(h, rinfo, sizeof h, cudaMemcpyDeviceToHost, st));
+        CK(ctx, cudaStreamSynchronize(st));
+        if (h[0] == 0) break;
+        if (round == 3) return batch_fail(b, SP3MM_EDEVICE, "row retries did not converge");
+        CK(ctx, cudaMemsetAsync(rinfo, 0, 2 * sizeof(int), st));
+        BatchTier t;
+        t.gt = true;
+        t.first = 0;
+        t.count = h[0];
+        t.scap = batch_slots_for(h[1]);
+        const size_t stride = (batch_row_region_bytes(num, t.scap) + 255) / 256 * 256;
+        long long warps = std::min<long long>(h[0], 8LL * ctx->num_sms);
+        while (warps > 1 && static_cast<size_t>(warps) * stride > (size_t(2) << 30)) warps >>= 1;
+        const int w = static_cast<int>(std::min<long long>(8, warps));
+        t.block = 32 * w;
+        t.grid = static_cast<int>((warps + w - 1) / w);
+        t.smem = stride;
+        DevBuf g;
+        TRY(g.alloc(ctx, gt_bytes(t)));
+        BatchRowParams q = p;
+        q.retry_rows = nxt;
+        std::vector<BatchTier> one{t};
+        int rc = SP3MM_OK;
+        prof(ctx, label, [&] { rc = run_tiers(b, mode, one, cur, q, g.as<unsigned char>()); });
+        TRY(rc);
+        std::swap(cur, nxt);
+    }
+    return SP3MM_OK;
+}
+
+// Exact binning of the rows by max(R*A, C) row counts and the numeric graph.
+int ensure_numeric(sp3mm_batch* b) {
+    if (b->exec) return SP3MM_OK;
+    sp3mm_ctx* ctx = b->ctx;
+    Counters* dc = b->d_counters.as<Counters>() + 1;
+    CK(ctx, cudaMemsetAsync(dc, 0, sizeof(Counters), ctx->stream));
+    const int M = static_cast<int>(b->rows);
+    if (M > 0)
+        launch_need_from_counts(M, b->d_cnt2.as<int>(), b->d_cnt1.as<int>(), b->d_need.as<int>(),
+                                ctx->stream);
+    TRY(bin_rows(ctx, M, b->d_need.as<int>(), 0, 32, dc, nullptr, b->nbins));
+    return build_numeric(b);
+}
+
 int batch_plan(sp3mm_batch* b) {
     sp3mm_ctx* ctx = b->ctx;
     const cudaStream_t st = ctx->stream;
@@ -350,6 +463,11 @@ int batch_plan(sp3mm_batch* b) {
     const int M = static_cast<int>(rows);
     const size_t R1 = static_cast<size_t>(rows) + 1;
     b->planned = false;
+    b->values_ready = false;
+    if (b->exec) cudaGraphExecDestroy(b->exec);
+    if (b->graph) cudaGraphDestroy(b->graph);
+    b->exec = nullptr;
+    b->graph = nullptr;
     b->results.assign(n, sp3mm_dcsr{});
     TRY(b->d_items.alloc(ctx, sizeof(BItem) * n));
     TRY(b->d_bases.alloc(ctx, sizeof(long long) * (n + 1)));
@@ -373,83 +491,63 @@ int batch_plan(sp3mm_batch* b) {
         prof(ctx, "batch.bounds", [&] {
             k_batch_bounds<<<grid_for_rows(rows), 256, 0, st>>>(
                 b->d_items.as<BItem>(), b->d_bases.as<long long>(), n, rows, b->d_need.as<int>(),
-                b->d_row_item.as<int>());
+                b->d_row_item.as<int>(), &dc->total);
         });
         note_launch();
         CK(ctx, cudaGetLastError());
     }
-
-    // Symbolic pass: tiers of the optimistic levels (need >> d1).
     Bins sb;
     TRY(bin_rows(ctx, M, b->d_need.as<int>(), b->d1, 32, dc, nullptr, sb));
-    std::vector<BatchTier> stiers;
-    TRY(make_tiers(b, sb, false, b->d1, b->tv, b->to, stiers));
-    DevBuf retry_a, retry_b, sgtab;
-    TRY(retry_a.alloc(ctx, sizeof(int) * R1));
-    TRY(retry_b.alloc(ctx, sizeof(int) * R1));
-    size_t sgt = 0;
-    for (const auto& t : stiers)
-        if (t.gt) sgt = gt_bytes(t);
-    if (sgt) TRY(sgtab.alloc(ctx, sgt));
+
     BatchRowParams p{};
     p.d1 = b->d1;
     p.d2 = b->d2;
     p.need = b->d_need.as<int>();
     p.cnt1 = b->d_cnt1.as<int>();
     p.cnt2 = b->d_cnt2.as<int>();
-    p.retry_rows = retry_a.as<int>();
-    p.retry_count = rinfo;
-    p.retry_need = rinfo + 1;
     p.err = ctx->d_err;
-    if (!stiers.empty()) {
-        int rc = SP3MM_OK;
-        prof(ctx, "batch.symbolic", [&] {
-            rc = run_tiers(b, kSymb, stiers, sb.lists.as<int>(), p, sgtab.as<unsigned char>());
-        });
-        TRY(rc);
-    }
-    // Rows whose proven tables exceed their tier: global-memory tables
-    // sized from the largest proven bound, at most three rounds (a direct
-    // row learns its second bound only once its first table is complete).
-    int* cur = retry_a.as<int>();
-    int* nxt = retry_b.as<int>();
-    for (int round = 0;; ++round) {
-        int h[2] = {0, 0};
-        CK(ctx, cudaMemcpyAsync(h, rinfo, sizeof h, cudaMemcpyDeviceToHost, st));
-        CK(ctx, cudaStreamSynchronize(st));
-        if (h[0] == 0) break;
-        if (round == 3) return batch_fail(b, SP3MM_EDEVICE, "symbolic retries did not converge");
-        CK(ctx, cudaMemsetAsync(rinfo, 0, 2 * sizeof(int), st));
-        BatchTier t;
-        t.gt = true;
-        t.first = 0;
-        t.count = h[0];
-        t.scap = batch_slots_for(h[1]);
-        const size_t stride = (batch_row_region_bytes(false, t.scap) + 255) / 256 * 256;
-        long long warps = std::min<long long>(h[0], 8LL * ctx->num_sms);
-        while (warps > 1 && static_cast<size_t>(warps) * stride > (size_t(2) << 30)) warps >>= 1;
-        const int w = static_cast<int>(std::min<long long>(8, warps));
-        t.block = 32 * w;
-        t.grid = static_cast<int>((warps + w - 1) / w);
-        t.smem = stride;
-        DevBuf g;
-        TRY(g.alloc(ctx, gt_bytes(t)));
+    bool booked = false;
+    DevBuf ub_ci, ub_v, row_off, cursor;
+    if (b->flavour == SP3MM_UB && rows > 0) {
+        // One numeric pass: every row books its exact length from one
+        // cursor, bounded by the output bound and by half the free memory.
+        size_t fr = 0, tot = 0;
+        CK(ctx, cudaMemGetInfo(&fr, &tot));
+        const size_t eb = sizeof(int) + vbytes(b->to);
+        const unsigned long long budget =
+            std::max<unsigned long long>(1ULL << 20, fr / 2 / eb);
+        const unsigned long long cap = std::min<unsigned long long>(sb.total, budget);
+        TRY(ub_ci.alloc(ctx, sizeof(int) * std::max<unsigned long long>(cap, 1)));
+        TRY(ub_v.alloc(ctx, vbytes(b->to) * std::max<unsigned long long>(cap, 1)));
+        TRY(row_off.alloc(ctx, sizeof(long long) * R1));
+        TRY(cursor.alloc(ctx, sizeof(unsigned long long)));
+        CK(ctx, cudaMemsetAsync(cursor.p, 0, sizeof(unsigned long long), st));
         BatchRowParams q = p;
-        q.retry_rows = nxt;
-        std::vector<BatchTier> one{t};
-        int rc = SP3MM_OK;
-        prof(ctx, "batch.symbolic.global", [&] {
-            rc = run_tiers(b, kSymb, one, cur, q, g.as<unsigned char>());
-        });
-        TRY(rc);
-        std::swap(cur, nxt);
+        q.cursor = cursor.as<unsigned long long>();
+        q.cap = cap;
+        q.row_off = row_off.as<long long>();
+        q.ub_ci = ub_ci.as<int>();
+        q.ub_v = ub_v.p;
+        TRY(row_pass(b, kNumBook, sb, q, rinfo, "batch.book"));
+        unsigned e = 0;
+        TRY(read_err(ctx, &e));
+        if (e != 0 && e != kErrBook) return check_device_err(ctx);
+        if (e == kErrBook) {
+            // The booking space ran out: plan this batch symbolically.
+            CK(ctx, cudaMemsetAsync(ctx->d_err, 0, sizeof(unsigned), st));
+            CK(ctx, cudaMemsetAsync(b->d_cnt1.p, 0, sizeof(int) * R1, st));
+            CK(ctx, cudaMemsetAsync(b->d_cnt2.p, 0, sizeof(int) * R1, st));
+        } else {
+            booked = true;
+        }
     }
+    if (!booked && rows > 0) TRY(row_pass(b, kSymb, sb, p, rinfo, "batch.symbolic"));
 
-    // Row pointers of the whole batch, product spans, exact binning.
+    // Row pointers of the whole batch, product spans and longest rows.
     DevBuf tmp, span;
     const size_t tb = scan_temp_bytes(M);
     TRY(tmp.alloc(ctx, tb));
-    TRY(span.alloc(ctx, sizeof(long long) * 2 * (n + 1)));
+    TRY(span.alloc(ctx, sizeof(long long) * 3 * (n + 1)));
     if (rows > 0) {
         prof(ctx, "batch.scan", [&] {
             launch_scan(M, b->d_cnt2.as<int>(), b->d_crp.as<int>(), tmp.p, tb, st);
@@ -458,21 +556,22 @@ int batch_plan(sp3mm_batch* b) {
         CK(ctx, cudaMemsetAsync(b->d_crp.p, 0, sizeof(int), st));
     }
     CK(ctx, cudaGetLastError());
-    std::vector<long long> hspan(2 * static_cast<size_t>(n) + 2, 0);
+    std::vector<long long> hspan(3 * static_cast<size_t>(n) + 3, 0);
     if (n > 0) {
         k_batch_item_spans<<<(n + 255) / 256, 256, 0, st>>>(b->d_items.as<BItem>(), n,
                                                            b->d_crp.as<int>(),
                                                            span.as<long long>());
+        CK(ctx, cudaMemsetAsync(span.as<long long>() + 2 * n, 0, sizeof(long long) * n, st));
+        if (rows > 0)
+            k_batch_item_max<<<grid_for_rows(rows), 256, 0, st>>>(
+                b->d_row_item.as<int>(), rows, b->d_cnt2.as<int>(), span.as<long long>() + 2 * n);
+        note_launch();
         note_launch();
         CK(ctx, cudaGetLastError());
-        CK(ctx, cudaMemcpyAsync(hspan.data(), span.p, sizeof(long long) * 2 * n,
+        CK(ctx, cudaMemcpyAsync(hspan.data(), span.p, sizeof(long long) * 3 * n,
                                 cudaMemcpyDeviceToHost, st));
     }
-    if (rows > 0)
-        launch_need_from_counts(M, b->d_cnt2.as<int>(), b->d_cnt1.as<int>(), b->d_need.as<int>(),
-                                st);
-    TRY(bin_rows(ctx, M, b->d_need.as<int>(), 0, 32, dc + 1, nullptr, b->nbins));
-    TRY(check_device_err(ctx));
+    TRY(check_device_err(ctx));   // synchronises: hspan is complete
     long long nnz = 0;
     for (int i = 0; i < n; ++i) nnz += hspan[2 * i + 1];
     if (nnz >= INT32_MAX) return batch_fail(b, SP3MM_ELIMIT, "the batch has too many nonzeros");
@@ -501,6 +600,13 @@ int batch_plan(sp3mm_batch* b) {
         note_launch();
         CK(ctx, cudaGetLastError());
     }
+    if (booked) {
+        prof(ctx, "batch.compact", [&] {
+            launch_compact(M, b->d_cnt2.as<int>(), row_off.as<long long>(), ub_ci.as<int>(),
+                           ub_v.p, b->d_crp.as<int>(), b->d_ci.as<int>(), b->d_v.p, b->to, st);
+        });
+        CK(ctx, cudaGetLastError());
+    }
     for (int i = 0; i < n; ++i) {
         sp3mm_dcsr& C = b->results[i];
         C.M = b->items[i].M;
@@ -510,9 +616,10 @@ int batch_plan(sp3mm_batch* b) {
         C.col = b->d_ci.as<int>() + hspan[2 * i];
         C.val = static_cast<unsigned char*>(b->d_v.p) + vbytes(b->to) * hspan[2 * i];
         C.val_type = b->to;
-        C.max_row = -1;
+        C.max_row = static_cast<int>(hspan[2 * static_cast<size_t>(n) + i]);
     }
-    TRY(build_numeric(b));
+    b->values_ready = booked || rows == 0;
+    if (!booked) TRY(ensure_numeric(b));
     b->planned = true;
     return SP3MM_OK;
 }
@@ -529,6 +636,7 @@ int check_operand(sp3mm_ctx* ctx, const sp3mm_dcsr& m, int tv, const char* what)
 namespace sp3mm {
 
 void batch_trim(sp3mm_batch* b) {
+    b->trimmed = true;
     b->drop_graph();
     b->tiers.clear();
     b->d_items.release();
@@ -587,6 +695,7 @@ int sp3mm_batch_create(sp3mm_ctx* ctx, int n, const int* kinds, const sp3mm_dcsr
         I.kind = kinds[i] == SP3MM_BATCH_RAP ? kBatchDirect : kBatchPair;
         if (I.kind == kBatchDirect) I.Z = view(Z[i]);
         else I.Z = CsrView{};
+        I.zmax = I.kind == kBatchDirect ? Z[i].max_row : -1;
         I.M = X[i].M;
         I.N = I.kind == kBatchDirect ? Z[i].N : Y[i].N;
         I.row_base = rows;
@@ -617,7 +726,14 @@ int sp3mm_batch_set_tuning(sp3mm_batch* b, int d1, int d2, int slack, int nsplit
     b->auto_split = nsplits < 0;
     b->splits.assign(splits && nsplits > 0 ? splits : nullptr,
                      splits && nsplits > 0 ? splits + nsplits : nullptr);
-    if (b->planned && numeric_changed) return build_numeric(b);
+    if (b->exec && numeric_changed) return build_numeric(b);
+    return SP3MM_OK;
+}
+
+int sp3mm_batch_set_flavour(sp3mm_batch* b, int flavour) {
+    if (!b || (flavour != SP3MM_UB && flavour != SP3MM_SYMBNUM))
+        return batch_fail(b, SP3MM_EINVAL, "unknown flavour");
+    b->flavour = flavour;
     return SP3MM_OK;
 }
 
@@ -629,7 +745,8 @@ int sp3mm_batch_plan(sp3mm_batch* b) {
 int sp3mm_batch_execute(sp3mm_batch* b) {
     if (!b) return SP3MM_EINVAL;
     if (!b->planned) return batch_fail(b, SP3MM_EINVAL, "execute before plan");
-    if (!b->exec) return batch_fail(b, SP3MM_EINVAL, "the batch was trimmed");
+    if (b->trimmed) return batch_fail(b, SP3MM_EINVAL, "the batch was trimmed");
+    TRY(ensure_numeric(b));
     sp3mm_ctx* ctx = b->ctx;
     cudaError_t e = cudaSuccess;
     prof(ctx, "batch.numeric", [&] { e = cudaGraphLaunch(b->exec, ctx->stream); });
@@ -639,7 +756,10 @@ int sp3mm_batch_execute(sp3mm_batch* b) {
 
 int sp3mm_batch_run(sp3mm_batch* b) {
     if (!b) return SP3MM_EINVAL;
-    if (!b->planned) TRY(batch_plan(b));
+    if (!b->planned) {
+        TRY(batch_plan(b));
+        if (b->values_ready) return SP3MM_OK;   // the booked plan computed them
+    }
     TRY(sp3mm_batch_execute(b));
     return check_device_err(b->ctx);
 }
@@ -675,6 +795,8 @@ int sp3mm_batch_autotune(sp3mm_batch* b, int reps, char* report, size_t len) {
     sp3mm_ctx* ctx = b->ctx;
     const cudaStream_t st = ctx->stream;
     if (!b->planned) TRY(batch_plan(b));
+    if (b->trimmed) return batch_fail(b, SP3MM_EINVAL, "the batch was trimmed");
+    TRY(ensure_numeric(b));
     struct Cand {
         bool autos;
         std::vector<int> splits;

@@ -17,6 +17,7 @@ struct BItem {
     int kind;
     int M, N;              // shape of C
     long long row_base;    // first global row
+    int zmax;              // direct: longest row of Z (-1: unknown)
 };
 
 struct BatchRowParams {
@@ -39,6 +40,13 @@ struct BatchRowParams {
     unsigned char* gtab;    // global-memory regions (GT), gstride bytes each
     long long gstride;
     unsigned* err;
+    // Booking (upper-bound flavour): each finished row books its exact
+    // length from `cursor` (capacity `cap` entries) and is written there.
+    unsigned long long* cursor;
+    unsigned long long cap;
+    long long* row_off;
+    int* ub_ci;
+    void* ub_v;
 };
 
 // Sets the kernel's dynamic shared memory limit to `max_smem` and returns

@@ -24,6 +24,8 @@ KFn pick_types(int tv, int to) {
 
 KFn pick(int mode, bool gt, int tv, int to) {
     if (mode == kSymb) return gt ? pick_types<kSymb, true>(tv, to) : pick_types<kSymb, false>(tv, to);
+    if (mode == kNumBook)
+        return gt ? pick_types<kNumBook, true>(tv, to) : pick_types<kNumBook, false>(tv, to);
     return gt ? pick_types<kNumExact, true>(tv, to) : pick_types<kNumExact, false>(tv, to);
 }
 

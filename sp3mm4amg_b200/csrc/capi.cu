@@ -231,18 +231,39 @@ int finish_matrix(sp3mm_dcsr* C, DevBuf& rp, DevBuf& ci, DevBuf& v) {
 }
 
 // Scan row counts into a fresh row_ptr; returns the total.
-int scan_counts(sp3mm_ctx* ctx, int M, const int* row_cnt, DevBuf& rp, long long* total) {
-    TRY(rp.alloc(ctx, sizeof(int) * (static_cast<size_t>(M) + 1)));
+int scan_counts(sp3mm_ctx* ctx, int M, const int* row_cnt, DevBuf& rp, long long* total,
+                int* max_row = nullptr) {
+    TRY(rp.alloc(ctx, sizeof(int) * (static_cast<size_t>(M) + 2)));
     DevBuf tmp;
     const size_t tb = scan_temp_bytes(M);
     TRY(tmp.alloc(ctx, tb));
     prof(ctx, "scan", [&] { launch_scan(M, row_cnt, rp.as<int>(), tmp.p, tb, ctx->stream); });
     CK(ctx, cudaGetLastError());
-    int t = 0;
-    CK(ctx, cudaMemcpyAsync(&t, rp.as<int>() + M, sizeof(int), cudaMemcpyDeviceToHost,
+    // The longest row rides in the slot after row_ptr[M].
+    int* mr = rp.as<int>() + M + 1;
+    CK(ctx, cudaMemsetAsync(mr, 0, sizeof(int), ctx->stream));
+    launch_count_max(M, row_cnt, nullptr, mr, ctx->stream);
+    int t[2] = {0, 0};
+    CK(ctx, cudaMemcpyAsync(t, rp.as<int>() + M, 2 * sizeof(int), cudaMemcpyDeviceToHost,
                             ctx->stream));
     CK(ctx, cudaStreamSynchronize(ctx->stream));
-    *total = t;
+    *total = t[0];
+    if (max_row) *max_row = t[1];
+    return SP3MM_OK;
+}
+
+// Longest row of m, computed on the device when not recorded.
+int known_max_row(sp3mm_ctx* ctx, const sp3mm_dcsr& m, int* out) {
+    if (m.max_row >= 0) {
+        *out = m.max_row;
+        return SP3MM_OK;
+    }
+    DevBuf b;
+    TRY(b.alloc(ctx, sizeof(int)));
+    CK(ctx, cudaMemsetAsync(b.p, 0, sizeof(int), ctx->stream));
+    launch_count_max(m.M, nullptr, m.row_ptr, b.as<int>(), ctx->stream);
+    CK(ctx, cudaMemcpyAsync(out, b.p, sizeof(int), cudaMemcpyDeviceToHost, ctx->stream));
+    CK(ctx, cudaStreamSynchronize(ctx->stream));
     return SP3MM_OK;
 }
 
@@ -267,6 +288,7 @@ int product_rows(sp3mm_ctx* ctx, RowRunner& rr, int M, int N, int flavour, int o
     p.err = ctx->d_err;
     p.c_vt = out_vt;
     long long nnz = 0;
+    int cmax = -1;
     if (flavour == SP3MM_SYMBNUM) {
         if (rr.direct) {
             TRY(row_cnt1.alloc(ctx, sizeof(int) * (static_cast<size_t>(M) + 1)));
@@ -275,7 +297,7 @@ int product_rows(sp3mm_ctx* ctx, RowRunner& rr, int M, int N, int flavour, int o
         }
         rr.mode = kSymb;
         TRY(rr.run(bins, p, G, d2, s1_max, s2_max, dc));
-        TRY(scan_counts(ctx, M, row_cnt.as<int>(), rp, &nnz));
+        TRY(scan_counts(ctx, M, row_cnt.as<int>(), rp, &nnz, &cmax));
         TRY(check_device_err(ctx));
         if (nnz < 0 || nnz >= INT32_MAX)
             return set_error(ctx, SP3MM_ELIMIT, "result has too many nonzeros");
@@ -309,7 +331,7 @@ int product_rows(sp3mm_ctx* ctx, RowRunner& rr, int M, int N, int flavour, int o
         p.ub_v = ub_v.p;
         rr.mode = kNumBook;
         TRY(rr.run(bins, p, G, d2, s1_max, s2_max, dc));
-        TRY(scan_counts(ctx, M, row_cnt.as<int>(), rp, &nnz));
+        TRY(scan_counts(ctx, M, row_cnt.as<int>(), rp, &nnz, &cmax));
         TRY(check_device_err(ctx));
         if (nnz < 0 || nnz >= INT32_MAX)
             return set_error(ctx, SP3MM_ELIMIT, "result has too many nonzeros");
@@ -325,7 +347,7 @@ int product_rows(sp3mm_ctx* ctx, RowRunner& rr, int M, int N, int flavour, int o
     C->N = N;
     C->nnz = nnz;
     C->val_type = out_vt;
-    C->max_row = -1;
+    C->max_row = cmax;
     return finish_matrix(C, rp, ci, v);
 }
 
@@ -367,7 +389,8 @@ int direct_impl(sp3mm_ctx* ctx, const sp3mm_dcsr& R, const sp3mm_dcsr& A, const 
     const int G = pick_group(ctx, mean);
     const int d1 = ctx->tune_d1 >= 0 ? ctx->tune_d1 : 2;
     const int d2 = ctx->tune_d2 >= 0 ? ctx->tune_d2 : 0;
-    const int pmax = P.max_row >= 0 ? P.max_row : P.N;
+    int pmax = 0;
+    TRY(known_max_row(ctx, P, &pmax));
     DevBuf cnt_buf, need;
     TRY(cnt_buf.alloc(ctx, sizeof(Counters)));
     TRY(need.alloc(ctx, sizeof(int) * (static_cast<size_t>(M) + 1)));

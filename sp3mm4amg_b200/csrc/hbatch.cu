@@ -343,7 +343,7 @@ int step_group(sp3mm_ctx* ctx, const std::vector<sp3mm_hierarchy*>& hs) {
     for (int t = 0; t < k; ++t) {
         const int n = static_cast<int>(bases[t + 1] - bases[t]);
         P[t] = sp3mm_dcsr{n, H[t].nc, AP0[t].nnz, AP0[t].row_ptr, AP0[t].col,
-                          H[t].pv, tv, -1};
+                          H[t].pv, tv, AP0[t].max_row};
         R[t] = sp3mm_dcsr{H[t].nc, n, AP0[t].nnz, r_rp + rrp[t], r_ci + r_base[t],
                           r_v + vb * r_base[t], tv, -1};
     }

@@ -226,7 +226,6 @@ int sp3mm_block_prolongator(sp3mm_ctx* ctx, const sp3mm_dcsr* A, const int32_t* 
         return fail(ctx, SP3MM_EINVAL, "block_prolongator: a row of A has no diagonal entry");
     }
     *P = AP0;
-    P->max_row = -1;
     return SP3MM_OK;
 }
 

@@ -380,6 +380,21 @@ void launch_direct_bounds(const CsrView& R, const CsrView& A, int p_max_row, int
     note_launch();
 }
 
+__global__ void k_count_max(int M, const int* cnt, const int* rp, int* out) {
+    int m = 0;
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < M; i += gridDim.x * blockDim.x)
+        m = max(m, cnt ? cnt[i] : rp[i + 1] - rp[i]);
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) m = max(m, __shfl_xor_sync(0xffffffffu, m, o));
+    if ((threadIdx.x & 31) == 0 && m > 0) atomicMax(out, m);
+}
+
+void launch_count_max(int M, const int* cnt, const int* rp, int* out, cudaStream_t st) {
+    if (M == 0) return;
+    k_count_max<<<grid_for(M, 256), 256, 0, st>>>(M, cnt, rp, out);
+    note_launch();
+}
+
 void launch_need_from_counts(int M, const int* cnt, const int* cnt1, int* need,
                              cudaStream_t st) {
     if (M == 0) return;

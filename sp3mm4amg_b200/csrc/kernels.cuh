@@ -80,6 +80,8 @@ void launch_pair_bounds(const CsrView& A, const CsrView& B, int* need,
                         unsigned long long* total, cudaStream_t st);
 void launch_direct_bounds(const CsrView& R, const CsrView& A, int p_max_row, int* need,
                           unsigned long long* total, cudaStream_t st);
+// *out = max(*out, largest cnt[i]) (cnt null: largest row length of rp).
+void launch_count_max(int M, const int* cnt, const int* rp, int* out, cudaStream_t st);
 // need from exact counts: max(cnt[i], cnt1[i]) (cnt1 may be null).
 void launch_need_from_counts(int M, const int* cnt, const int* cnt1, int* need,
                              cudaStream_t st);

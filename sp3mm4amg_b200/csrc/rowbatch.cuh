@@ -67,6 +67,20 @@ __device__ __forceinline__ void batch_retry(const BatchRowParams& p, int g, long
     }
 }
 
+// Book n entries for row g; -1 when the capacity is exhausted (flagged).
+__device__ __forceinline__ long long batch_book(const BatchRowParams& p, int g, int n) {
+    const int lane = threadIdx.x & 31;
+    unsigned long long off = 0;
+    if (lane == 0 && n > 0) off = atomicAdd(p.cursor, static_cast<unsigned long long>(n));
+    off = __shfl_sync(kFull, off, 0);
+    if (off + n > p.cap) {
+        if (lane == 0) atomicOr(p.err, kErrBook);
+        return -1;
+    }
+    if (lane == 0) p.row_off[g] = static_cast<long long>(off);
+    return static_cast<long long>(off);
+}
+
 // Accumulate with an optimistic table of S slots, then (on overflow) once
 // more with the proven size Sp when it fits the region.  Returns the size
 // used, or 0 when the row does not fit (the table is left clear).
@@ -135,7 +149,7 @@ __global__ void __launch_bounds__(256, 4)
         if (kind == kBatchDirect) {
             const CsrView Z = I->Z;
             long long need2 = 0;
-            if constexpr (MODE == kSymb) {
+            if constexpr (MODE != kNumExact) {
                 const int need1 = __ldg(p.need + g);
                 S1 = batch_accumulate<NUM>(L1, xlen, Y.rp, Y.ci, static_cast<const TV*>(Y.v),
                                            keys1, vals1, ord1, batch_slots(need1 >> p.d1),
@@ -161,8 +175,14 @@ __global__ void __launch_bounds__(256, 4)
                     p.cnt1[g] = n1;
                     p.cnt2[g] = n2;
                 }
-                wclear(make_wtab(keys2, vals2, ord2, S2), n2, NUM);
-                __syncwarp();
+                if constexpr (MODE == kSymb) {
+                    wclear(make_wtab(keys2, vals2, ord2, S2), n2, NUM);
+                    __syncwarp();
+                } else {
+                    wextract(make_wtab(keys2, vals2, ord2, S2), n2, keys1, vals1);
+                    const long long base = batch_book(p, g, n2);
+                    wsorted_write<TO>(keys1, vals1, n2, p.ub_ci, static_cast<TO*>(p.ub_v), base);
+                }
             } else {
                 const int e1 = __ldg(p.cnt1 + g), e2 = __ldg(p.cnt2 + g);
                 S1 = batch_slots(e1);
@@ -192,7 +212,7 @@ __global__ void __launch_bounds__(256, 4)
                 wsorted_write<TO>(keys1, vals1, n2, p.c_ci, static_cast<TO*>(p.c_v), base);
             }
         } else {
-            if constexpr (MODE == kSymb) {
+            if constexpr (MODE != kNumExact) {
                 const int need1 = __ldg(p.need + g);
                 S1 = batch_accumulate<NUM>(L1, xlen, Y.rp, Y.ci, static_cast<const TV*>(Y.v),
                                            keys1, vals1, ord1, batch_slots(need1 >> p.d1),
@@ -202,8 +222,14 @@ __global__ void __launch_bounds__(256, 4)
                     continue;
                 }
                 if (lane == 0) p.cnt2[g] = n1;
-                wclear(make_wtab(keys1, vals1, ord1, S1), n1, NUM);
-                __syncwarp();
+                if constexpr (MODE == kSymb) {
+                    wclear(make_wtab(keys1, vals1, ord1, S1), n1, NUM);
+                    __syncwarp();
+                } else {
+                    wextract(make_wtab(keys1, vals1, ord1, S1), n1, keys2, vals2);
+                    const long long base = batch_book(p, g, n1);
+                    wsorted_write<TO>(keys2, vals2, n1, p.ub_ci, static_cast<TO*>(p.ub_v), base);
+                }
             } else {
                 const int e = __ldg(p.cnt2 + g);
                 S1 = batch_slots(e);

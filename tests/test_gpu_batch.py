@@ -49,9 +49,9 @@ def mixed(orc):
     return specs, wants
 
 
-def _run(ctx, specs, tuning=None, out_vt=S.F64, in_vt=S.F64):
+def _run(ctx, specs, tuning=None, out_vt=S.F64, in_vt=S.F64, flavour=S.UB):
     dev = [tuple(ctx.upload(m, in_vt) for m in s) for s in specs]
-    b = ctx.batch(dev, out_vt)
+    b = ctx.batch(dev, out_vt, flavour)
     if tuning is not None:
         b.set_tuning(**tuning)
     b.run()
@@ -64,10 +64,11 @@ def _run(ctx, specs, tuning=None, out_vt=S.F64, in_vt=S.F64):
     return got, info
 
 
-def test_batch_mixed_bit_exact(mixed):
+@pytest.mark.parametrize("flavour", [S.UB, S.SYMBNUM])
+def test_batch_mixed_bit_exact(mixed, flavour):
     specs, wants = mixed
     with S.Context() as ctx:
-        got, info = _run(ctx, specs)
+        got, info = _run(ctx, specs, flavour=flavour)
     assert info["nnz"] == sum(w.nnz for w in wants)
     for g, w in zip(got, wants):
         _same(g, w)
@@ -82,9 +83,10 @@ def test_batch_mixed_bit_exact(mixed):
 def test_batch_tuning_invariance(mixed, tuning):
     specs, wants = mixed
     with S.Context() as ctx:
-        got, _ = _run(ctx, specs, tuning)
-    for g, w in zip(got, wants):
-        _same(g, w)
+        for flavour in (S.UB, S.SYMBNUM):
+            got, _ = _run(ctx, specs, tuning, flavour=flavour)
+            for g, w in zip(got, wants):
+                _same(g, w)
 
 
 def test_batch_value_types(mixed, orc):
@@ -141,7 +143,25 @@ def test_batch_autotune_keeps_results(mixed):
         b.free()
 
 
-def test_batch_long_rows_global_tables(orc):
+def test_batch_replay_after_booked_plan(mixed):
+    """A booked plan computes the values; the first execute builds the exact
+    replay graph and reproduces them."""
+    specs, wants = mixed
+    with S.Context() as ctx:
+        dev = [tuple(ctx.upload(m) for m in s) for s in specs]
+        b = ctx.batch(dev)
+        b.run()
+        first = [b.result(i).download() for i in range(len(specs))]
+        b.execute()
+        ctx.sync()
+        for i, w in enumerate(wants):
+            _same(first[i], w)
+            _same(b.result(i).download(), w)
+        b.free()
+
+
+@pytest.mark.parametrize("flavour", [S.UB, S.SYMBNUM])
+def test_batch_long_rows_global_tables(orc, flavour):
     """Rows with thousands of distinct columns exceed every shared-memory
     tier: symbolic retries and the global-memory tiers take them."""
     X = pb.random_sparse(40, 2000, 0.12, seed=11)
@@ -152,8 +172,9 @@ def test_batch_long_rows_global_tables(orc):
     wants = [orc.spmm(X, Y), orc.sp3mm_direct(X, Y, Z), orc.sp3mm_direct(*small)]
     assert int(np.diff(wants[0].indptr).max()) > 4000
     with S.Context() as ctx:
-        got, info = _run(ctx, specs)
-    assert info["global_tiers"] >= 1
+        got, info = _run(ctx, specs, flavour=flavour)
+        if flavour == S.SYMBNUM:
+            assert info["global_tiers"] >= 1
     for g, w in zip(got, wants):
         _same(g, w)
 
@@ -166,9 +187,10 @@ def test_batch_degenerate(orc):
     specs = [(Z0, B), (E, A), (A, A, A), (A, A)]
     wants = [orc.spmm(Z0, B), orc.spmm(E, A), orc.sp3mm_direct(A, A, A), orc.spmm(A, A)]
     with S.Context() as ctx:
-        got, _ = _run(ctx, specs)
-        for g, w in zip(got, wants):
-            _same(g, w)
+        for flavour in (S.UB, S.SYMBNUM):
+            got, _ = _run(ctx, specs, flavour=flavour)
+            for g, w in zip(got, wants):
+                _same(g, w)
         empty = ctx.batch([])
         empty.run()
         assert empty.info()["nnz"] == 0
