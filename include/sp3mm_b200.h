@@ -381,6 +381,39 @@ SP3MM_API int sp3mm_hierarchy_build_batch(sp3mm_ctx *ctx, int n, const sp3mm_dcs
                                           double omega, int64_t min_coarse, int max_levels,
                                           int coarse_val_type, sp3mm_hierarchy **out);
 
+/* ---- Request server: continuous batching of hierarchy setups ------------
+ * Each request is a host CSR operator A0 (0-based int64 row_ptr/col, FP64
+ * values; borrowed until the request is admitted) on a box grid.  Every
+ * sp3mm_server_step admits queued requests first come first served while
+ * fewer than max_active are in flight and the request's device-memory
+ * estimate fits both the budget (mem_fraction of the HBM free at creation,
+ * less what admitted requests reserve) and the HBM free now; then advances
+ * every admitted hierarchy by one level with batched launches shared by all
+ * of them (results equal the single build's); then retires complete ones.
+ * Times are seconds on the server's clock (sp3mm_server_now); a request's
+ * latency runs from its arrival (given, or its submission) to the end of
+ * the step that completed it.  Status: 0 queued, 1 active, 2 done,
+ * 3 failed (poll returns the error), 4 taken. */
+typedef struct sp3mm_server sp3mm_server;
+SP3MM_API int sp3mm_server_create(sp3mm_ctx *ctx, int max_active, double mem_fraction,
+                                  sp3mm_server **out);
+SP3MM_API double sp3mm_server_now(const sp3mm_server *s);
+SP3MM_API int sp3mm_server_submit(sp3mm_server *s, int64_t M, int64_t nnz,
+                                  const int64_t *row_ptr, const int64_t *col, const double *val,
+                                  const int32_t *dims, int ndim, int block, double omega,
+                                  int64_t min_coarse, int max_levels, int coarse_val_type,
+                                  double arrival, int64_t *id);
+SP3MM_API int sp3mm_server_step(sp3mm_server *s, int *pending);
+SP3MM_API int sp3mm_server_poll(const sp3mm_server *s, int64_t id, int *status,
+                                double *latency, double *queued);
+/* Hand a done request's hierarchy (with its uploaded A0) to the caller,
+ * who frees it with sp3mm_hierarchy_free. */
+SP3MM_API int sp3mm_server_take(sp3mm_server *s, int64_t id, sp3mm_hierarchy **h);
+SP3MM_API int sp3mm_server_stats(const sp3mm_server *s, int64_t *completed, int64_t *products,
+                                 double *p50, double *p99, double *busy_s, int64_t *steps,
+                                 int *peak_active, int64_t *deferred);
+SP3MM_API int sp3mm_server_free(sp3mm_server *s);
+
 #ifdef __cplusplus
 }
 #endif

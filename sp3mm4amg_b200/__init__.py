@@ -35,7 +35,7 @@ __all__ = [
     "CSR", "Problem", "Context", "DeviceCSR", "Sp3mmError", "spmm", "sp3mm",
     "symb_rowsizes", "ub_rowsizes", "ub_colparts_rowsizes", "elapsed_internal",
     "UB", "SYMBNUM", "PAIR", "DIRECT", "PAIR_RIGHT", "F64", "F32", "RBTREE", "IDXMAP",
-    "BATCH_SPMM", "BATCH_RAP", "Batch", "Hierarchy",
+    "BATCH_SPMM", "BATCH_RAP", "Batch", "Hierarchy", "Server",
 ]
 
 
@@ -443,4 +443,71 @@ class Batch:
     def free(self) -> None:
         if self.h:
             self.ctx.lib.sp3mm_batch_free(self.h)
+            self.h = None
+
+
+class Server:
+    """Continuous-batching hierarchy-setup server (sp3mm_server_*)."""
+
+    QUEUED, ACTIVE, DONE, FAILED, TAKEN = range(5)
+
+    def __init__(self, ctx: Context, max_active: int = 64, mem_fraction: float = 0.5):
+        self.ctx = ctx
+        h = ctypes.c_void_p()
+        ctx._check(ctx.lib.sp3mm_server_create(ctx.h, max_active, float(mem_fraction),
+                                               ctypes.byref(h)))
+        self.h = h
+        self._inputs = {}   # host arrays must outlive admission
+
+    def now(self) -> float:
+        return float(self.ctx.lib.sp3mm_server_now(self.h))
+
+    def submit(self, A0: CSR, dims, block: int = 2, omega: float = 2.0 / 3.0,
+               min_coarse: int = 1000, max_levels: int = 20, coarse_val_type: int = F64,
+               arrival: float = -1.0) -> int:
+        rp = np.ascontiguousarray(A0.indptr, np.int64)
+        ci = np.ascontiguousarray(A0.indices, np.int64)
+        v = np.ascontiguousarray(A0.data, np.float64)
+        dd = (ctypes.c_int32 * 3)(*(list(dims) + [1, 1])[:3])
+        rid = ctypes.c_int64()
+        self.ctx._check(self.ctx.lib.sp3mm_server_submit(
+            self.h, A0.M, A0.nnz, rp.ctypes.data, ci.ctypes.data, v.ctypes.data, dd, len(dims),
+            block, float(omega), min_coarse, max_levels, coarse_val_type, float(arrival),
+            ctypes.byref(rid)))
+        self._inputs[rid.value] = (rp, ci, v)
+        return rid.value
+
+    def step(self) -> int:
+        pending = ctypes.c_int()
+        self.ctx._check(self.ctx.lib.sp3mm_server_step(self.h, ctypes.byref(pending)))
+        for rid in [r for r in self._inputs if self.poll(r)[0] != self.QUEUED]:
+            del self._inputs[rid]
+        return pending.value
+
+    def poll(self, rid: int):
+        """(status, latency_s, queued_s)."""
+        st, lat, q = ctypes.c_int(), ctypes.c_double(), ctypes.c_double()
+        self.ctx.lib.sp3mm_server_poll(self.h, rid, ctypes.byref(st), ctypes.byref(lat),
+                                       ctypes.byref(q))
+        return st.value, lat.value, q.value
+
+    def take(self, rid: int) -> Hierarchy:
+        h = ctypes.c_void_p()
+        self.ctx._check(self.ctx.lib.sp3mm_server_take(self.h, rid, ctypes.byref(h)))
+        return Hierarchy(self.ctx, h)
+
+    def stats(self) -> dict:
+        c, pr, st, de = ctypes.c_int64(), ctypes.c_int64(), ctypes.c_int64(), ctypes.c_int64()
+        p50, p99, busy = ctypes.c_double(), ctypes.c_double(), ctypes.c_double()
+        peak = ctypes.c_int()
+        self.ctx._check(self.ctx.lib.sp3mm_server_stats(
+            self.h, ctypes.byref(c), ctypes.byref(pr), ctypes.byref(p50), ctypes.byref(p99),
+            ctypes.byref(busy), ctypes.byref(st), ctypes.byref(peak), ctypes.byref(de)))
+        return {"completed": c.value, "products": pr.value, "p50_s": p50.value,
+                "p99_s": p99.value, "busy_s": busy.value, "steps": st.value,
+                "peak_active": peak.value, "deferred": de.value}
+
+    def free(self) -> None:
+        if self.h:
+            self.ctx.lib.sp3mm_server_free(self.h)
             self.h = None

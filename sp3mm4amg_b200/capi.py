@@ -85,6 +85,23 @@ DEVICE_API = {
                                     _c.POINTER(_c.c_int64), _c.POINTER(_c.c_int),
                                     _c.POINTER(_c.c_int)]),
     "sp3mm_batch_free": (_c.c_int, [_c.c_void_p]),
+    "sp3mm_server_create": (_c.c_int, [_c.c_void_p, _c.c_int, _c.c_double,
+                                       _c.POINTER(_c.c_void_p)]),
+    "sp3mm_server_now": (_c.c_double, [_c.c_void_p]),
+    "sp3mm_server_submit": (_c.c_int, [_c.c_void_p, _c.c_int64, _c.c_int64, _c.c_void_p,
+                                       _c.c_void_p, _c.c_void_p, _c.c_void_p, _c.c_int,
+                                       _c.c_int, _c.c_double, _c.c_int64, _c.c_int, _c.c_int,
+                                       _c.c_double, _c.POINTER(_c.c_int64)]),
+    "sp3mm_server_step": (_c.c_int, [_c.c_void_p, _c.POINTER(_c.c_int)]),
+    "sp3mm_server_poll": (_c.c_int, [_c.c_void_p, _c.c_int64, _c.POINTER(_c.c_int),
+                                     _c.POINTER(_c.c_double), _c.POINTER(_c.c_double)]),
+    "sp3mm_server_take": (_c.c_int, [_c.c_void_p, _c.c_int64, _c.POINTER(_c.c_void_p)]),
+    "sp3mm_server_stats": (_c.c_int, [_c.c_void_p, _c.POINTER(_c.c_int64),
+                                      _c.POINTER(_c.c_int64), _c.POINTER(_c.c_double),
+                                      _c.POINTER(_c.c_double), _c.POINTER(_c.c_double),
+                                      _c.POINTER(_c.c_int64), _c.POINTER(_c.c_int),
+                                      _c.POINTER(_c.c_int64)]),
+    "sp3mm_server_free": (_c.c_int, [_c.c_void_p]),
 }
 
 # Error codes, flavours, variants, value types (include/sp3mm_b200.h).

@@ -209,3 +209,35 @@ def log_uniform_sides(rng, count: int, nmin: float = 1e3, nmax: float = 2e5):
         side = max(2, int(round(n ** (1.0 / dim))))
         out.append((dim, side))
     return out
+
+
+def config3_specs(seed: int = 3, count: int = 256):
+    """Grid shapes of the batched workload: a fair coin for 2D / 3D and a
+    side drawn log-uniformly so that n runs from 1e3 to 2e5."""
+    rng = np.random.default_rng(seed)
+    return [(s,) * d for d, s in log_uniform_sides(rng, count)]
+
+
+def config4_specs(seed: int = 4, count: int = 200, large_fraction: float = 0.1):
+    """Grid shapes of the served workload: 90% drawn as config3_specs, 10%
+    7-point problems with side 64..128."""
+    rng = np.random.default_rng(seed)
+    out = []
+    for _ in range(count):
+        if rng.random() < large_fraction:
+            out.append((int(rng.integers(64, 129)),) * 3)
+        else:
+            d, s = log_uniform_sides(rng, 1)[0]
+            out.append((s,) * d)
+    return out
+
+
+def poisson_arrivals(rate: float, count: int, seed: int = 5) -> np.ndarray:
+    """Arrival times (seconds from 0) of a Poisson process of `rate`/s."""
+    rng = np.random.default_rng(seed)
+    return np.cumsum(rng.exponential(1.0 / rate, count))
+
+
+def stencil_operator(dims) -> CSR:
+    """The 5-point (2D) or 7-point (3D) Poisson operator on a box grid."""
+    return poisson3d(*dims) if len(dims) == 3 else poisson2d(*dims)

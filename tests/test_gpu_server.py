@@ -1,0 +1,146 @@
+"""Request server (continuous batching of hierarchy setups): every result is
+the same alone and in the mix (bit for bit, and equal to the oracle chain),
+admission honours slots and memory, late requests join in-flight steps,
+and a failing request does not take the others down."""
+import numpy as np
+import pytest
+
+import oracle as O
+from oracle import hierarchy as H
+import sp3mm4amg_b200 as S
+from sp3mm4amg_b200 import problems as pb
+from sp3mm4amg_b200 import serving
+
+pytestmark = pytest.mark.gpu
+
+SPECS = [(12, 12, 12), (40, 33), (9, 7, 5), (64, 64), (20, 20, 20), (30, 31)]
+
+
+def _same(got, want):
+    cmp = O.compare(got, want, rtol=0.0)
+    assert cmp["ok"], cmp
+    assert cmp["bitwise_equal"] == want.nnz
+
+
+def _levels(h):
+    out = []
+    for l in range(len(h)):
+        A, P, R = h.level(l)
+        out.append(tuple(m.download() if m is not None else None for m in (A, P, R)))
+    return out
+
+
+def _serve_all(ctx, specs, modes, max_active=64, mem_fraction=0.5, min_coarse=30):
+    srv = S.Server(ctx, max_active, mem_fraction)
+    ids = [srv.submit(pb.stencil_operator(d), d, min_coarse=min_coarse, coarse_val_type=m)
+           for d, m in zip(specs, modes)]
+    while srv.step():
+        pass
+    for rid in ids:
+        assert srv.poll(rid)[0] == S.Server.DONE
+    hs = [srv.take(rid) for rid in ids]
+    st = srv.stats()
+    srv.free()
+    return hs, st
+
+
+def test_server_mix_equals_alone_and_oracle(orc):
+    modes = [S.F64, S.F32, S.F64, S.F32, S.F64, S.F64]
+    with S.Context() as ctx:
+        mix, st = _serve_all(ctx, SPECS, modes)
+        assert st["completed"] == len(SPECS) and st["peak_active"] == len(SPECS)
+        for d, m, h in zip(SPECS, modes, mix):
+            alone, _ = _serve_all(ctx, [d], [m])
+            got, ref = _levels(h), _levels(alone[0])
+            assert len(got) == len(ref)
+            for a, b in zip(got, ref):
+                for x, y in zip(a, b):
+                    if y is None:
+                        assert x is None
+                    else:
+                        _same(x, y)
+            want = H.chain(orc, pb.stencil_operator(d), d, min_coarse=30, max_levels=20,
+                           coarse_f32=(m == S.F32))
+            for (x, _, _), (w, _, _) in zip(got, want):
+                _same(x, w)
+            alone[0].free()
+            h.free()
+
+
+def test_server_late_arrivals_join_in_flight(orc):
+    """Requests submitted between steps are admitted while earlier ones are
+    mid-hierarchy; their results are unaffected."""
+    with S.Context() as ctx:
+        srv = S.Server(ctx)
+        first = [srv.submit(pb.stencil_operator(d), d, min_coarse=30) for d in SPECS[:2]]
+        srv.step()
+        assert all(srv.poll(r)[0] == S.Server.ACTIVE for r in first)
+        late = [srv.submit(pb.stencil_operator(d), d, min_coarse=30) for d in SPECS[2:4]]
+        srv.step()
+        states = [srv.poll(r)[0] for r in first + late]
+        assert all(s in (S.Server.ACTIVE, S.Server.DONE) for s in states)
+        while srv.step():
+            pass
+        for rid, d in zip(first + late, SPECS[:4]):
+            h = srv.take(rid)
+            want = H.chain(orc, pb.stencil_operator(d), d, min_coarse=30, max_levels=20)
+            for l, (w, _, _) in enumerate(want):
+                _same(h.level(l)[0].download(), w)
+            h.free()
+        assert srv.stats()["completed"] == 4
+        srv.free()
+
+
+def test_server_slots_and_memory_admission():
+    with S.Context() as ctx:
+        _, st = _serve_all(ctx, SPECS, [S.F64] * len(SPECS), max_active=2)
+        assert st["peak_active"] <= 2 and st["completed"] == len(SPECS)
+        # A budget that holds one small request at a time.
+        srv = S.Server(ctx, 64, 1e-6)
+        rid = srv.submit(pb.stencil_operator((8, 8)), (8, 8), min_coarse=4)
+        big = srv.submit(pb.stencil_operator((60, 60, 60)), (60, 60, 60))
+        while srv.step():
+            pass
+        st = srv.stats()
+        srv.free()
+        assert st["completed"] <= 1
+    # the 60^3 request never fits this budget: refused, not blocking
+    with S.Context() as ctx:
+        srv = S.Server(ctx, 64, 1e-6)
+        big = srv.submit(pb.stencil_operator((60, 60, 60)), (60, 60, 60))
+        srv.step()
+        assert srv.poll(big)[0] == S.Server.FAILED
+        srv.free()
+
+
+def test_server_failure_is_isolated(orc):
+    a = pb.poisson2d(10, 10).to_scipy().tolil()
+    a[7, 7] = 0.0
+    a = a.tocsr()
+    a.eliminate_zeros()
+    bad = pb.CSR.from_scipy(a)
+    with S.Context() as ctx:
+        srv = S.Server(ctx)
+        good = [srv.submit(pb.stencil_operator(d), d, min_coarse=30) for d in SPECS[:3]]
+        wrong = srv.submit(bad, (10, 10), min_coarse=4)
+        while srv.step():
+            pass
+        assert srv.poll(wrong)[0] == S.Server.FAILED
+        for rid, d in zip(good, SPECS[:3]):
+            assert srv.poll(rid)[0] == S.Server.DONE
+            h = srv.take(rid)
+            want = H.chain(orc, pb.stencil_operator(d), d, min_coarse=30, max_levels=20)
+            _same(h.level(len(h) - 1)[0].download(), want[-1][0])
+            h.free()
+        srv.free()
+
+
+def test_serving_driver_reports_latency():
+    specs = pb.config4_specs(seed=9, count=12, large_fraction=0.0)
+    arrivals = pb.poisson_arrivals(200.0, len(specs), seed=9)
+    with S.Context() as ctx:
+        st, _ = serving.serve_batched(ctx, specs, arrivals)
+        assert st["completed"] == len(specs) and st["failed"] == 0
+        assert 0 < st["p50_s"] <= st["p99_s"] and st["products"] > 0
+        plain = serving.serve_plain(ctx, specs, arrivals)
+        assert plain["products"] == st["products"]

@@ -224,3 +224,17 @@ def test_device_hierarchies_batched_errors():
         hs = ctx.hierarchies([good], [(6, 6)], min_coarse=2)
         assert len(hs[0]) >= 2
         hs[0].free()
+
+
+def test_workload_generators():
+    specs = pb.config3_specs(seed=3, count=256)
+    assert len(specs) == 256
+    ns = [int(np.prod(s)) for s in specs]
+    assert min(ns) >= 500 and max(ns) <= 2.2e5
+    assert 0.3 < np.mean([len(s) == 3 for s in specs]) < 0.7
+    s4 = pb.config4_specs(seed=4, count=400)
+    big = [s for s in s4 if len(s) == 3 and s[0] >= 64]
+    assert 0.04 < len(big) / len(s4) < 0.2
+    t = pb.poisson_arrivals(50.0, 2000, seed=1)
+    assert np.all(np.diff(t) > 0)
+    assert abs(np.mean(np.diff(t)) - 1 / 50.0) < 0.003
