@@ -510,12 +510,16 @@ int batch_plan(sp3mm_batch* b) {
     DevBuf ub_ci, ub_v, row_off, cursor;
     if (b->flavour == SP3MM_UB && rows > 0) {
         // One numeric pass: every row books its exact length from one
-        // cursor, bounded by the output bound and by half the free memory.
-        size_t fr = 0, tot = 0;
-        CK(ctx, cudaMemGetInfo(&fr, &tot));
+        // cursor, in space bounded by the output bound, by eight times the
+        // operands' nonzeros and by half the free memory (a batch that
+        // overflows it is planned symbolically instead).
+        const size_t fr = free_device_bytes(ctx);
         const size_t eb = sizeof(int) + vbytes(b->to);
-        const unsigned long long budget =
-            std::max<unsigned long long>(1ULL << 20, fr / 2 / eb);
+        long long in_nnz = 0;
+        for (const BItem& I : b->items)
+            in_nnz += I.X.nnz + I.Y.nnz + (I.kind == kBatchDirect ? I.Z.nnz : 0);
+        const unsigned long long budget = std::max<unsigned long long>(
+            1ULL << 20, std::min<unsigned long long>(8ULL * in_nnz, fr / 2 / eb));
         const unsigned long long cap = std::min<unsigned long long>(sb.total, budget);
         TRY(ub_ci.alloc(ctx, sizeof(int) * std::max<unsigned long long>(cap, 1)));
         TRY(ub_v.alloc(ctx, vbytes(b->to) * std::max<unsigned long long>(cap, 1)));

@@ -48,6 +48,24 @@ int check_dcsr(sp3mm_ctx* ctx, const sp3mm_dcsr* m, const char* what) {
     return SP3MM_OK;
 }
 
+size_t free_device_bytes(sp3mm_ctx* ctx) {
+    size_t fr = 0, tot = 0;
+    if (cudaMemGetInfo(&fr, &tot) != cudaSuccess) {
+        cudaGetLastError();
+        return 0;
+    }
+    cudaMemPool_t pool;
+    uint64_t reserved = 0, used = 0;
+    if (cudaDeviceGetDefaultMemPool(&pool, ctx->device) == cudaSuccess &&
+        cudaMemPoolGetAttribute(pool, cudaMemPoolAttrReservedMemCurrent, &reserved) ==
+            cudaSuccess &&
+        cudaMemPoolGetAttribute(pool, cudaMemPoolAttrUsedMemCurrent, &used) == cudaSuccess &&
+        reserved > used)
+        fr += static_cast<size_t>(reserved - used);
+    cudaGetLastError();
+    return fr;
+}
+
 int read_err(sp3mm_ctx* ctx, unsigned* out) {
     CK(ctx, cudaMemcpyAsync(out, ctx->d_err, sizeof(unsigned), cudaMemcpyDeviceToHost,
                             ctx->stream));
@@ -131,6 +149,10 @@ struct RowRunner {
     PairRowArgs pa;
     // Longest row of the right operands (first / last; -1: unknown).
     int a_max = -1, b_max = -1;
+
+    long long operand_nnz() const {
+        return direct ? da.R.nnz + da.A.nnz + da.P.nnz : pa.A.nnz + pa.B.nnz;
+    }
 
     int launch(RowParams p, int G, DevBuf& gtab) {
         const size_t per_group = row_table_bytes(direct, mode, G, p.S1, p.S2);
@@ -318,7 +340,15 @@ int product_rows(sp3mm_ctx* ctx, RowRunner& rr, int M, int N, int flavour, int o
         rr.mode = kNumExact;
         TRY(rr.run(nb, p, G, 0, s1_max, s2_max, dc));
     } else {
-        const unsigned long long cap = bins.total;
+        // Rows book their exact length from one cursor, so the space need
+        // only exceed nnz(C): the bound, capped at half the free memory; a
+        // product that still overflows it is redone symbolically.
+        const unsigned long long budget = std::max<unsigned long long>(
+            1ULL << 20,
+            std::min<unsigned long long>(
+                8ULL * static_cast<unsigned long long>(rr.operand_nnz()),
+                free_device_bytes(ctx) / 2 / (sizeof(int) + vbytes(out_vt))));
+        const unsigned long long cap = std::min<unsigned long long>(bins.total, budget);
         DevBuf ub_ci, ub_v, row_off;
         TRY(ub_ci.alloc(ctx, sizeof(int) * cap));
         TRY(ub_v.alloc(ctx, vbytes(out_vt) * cap));
@@ -331,6 +361,19 @@ int product_rows(sp3mm_ctx* ctx, RowRunner& rr, int M, int N, int flavour, int o
         p.ub_v = ub_v.p;
         rr.mode = kNumBook;
         TRY(rr.run(bins, p, G, d2, s1_max, s2_max, dc));
+        if (cap < bins.total) {
+            unsigned e = 0;
+            TRY(read_err(ctx, &e));
+            if ((e & kErrBook) && e != kErrBook) return check_device_err(ctx);
+            if (e == kErrBook) {
+                CK(ctx, cudaMemsetAsync(ctx->d_err, 0, sizeof(unsigned), st));
+                ub_ci.release();
+                ub_v.release();
+                CK(ctx, cudaMemsetAsync(dc, 0, sizeof(Counters), st));
+                return product_rows(ctx, rr, M, N, SP3MM_SYMBNUM, out_vt, need, dc, G, d1, d2,
+                                     s1_bound, s2_bound, p_max_row, C);
+            }
+        }
         TRY(scan_counts(ctx, M, row_cnt.as<int>(), rp, &nnz, &cmax));
         TRY(check_device_err(ctx));
         if (nnz < 0 || nnz >= INT32_MAX)

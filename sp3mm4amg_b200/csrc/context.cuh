@@ -131,6 +131,9 @@ struct Bins {
     DevBuf level, lists;
 };
 
+// Device memory available to new allocations: free HBM plus the idle part
+// of the device's memory pool.
+size_t free_device_bytes(sp3mm_ctx* ctx);
 int read_err(sp3mm_ctx* ctx, unsigned* out);
 // Read and clear the sticky device error word; map it to a return code.
 int check_device_err(sp3mm_ctx* ctx);

@@ -69,23 +69,7 @@ size_t request_estimate(int64_t M, int64_t nnz) {
     return 2 * level0;
 }
 
-size_t free_hbm(sp3mm_ctx* ctx) {
-    size_t fr = 0, tot = 0;
-    if (cudaMemGetInfo(&fr, &tot) != cudaSuccess) {
-        cudaGetLastError();
-        return 0;
-    }
-    cudaMemPool_t pool;
-    uint64_t reserved = 0, used = 0;
-    if (cudaDeviceGetDefaultMemPool(&pool, ctx->device) == cudaSuccess &&
-        cudaMemPoolGetAttribute(pool, cudaMemPoolAttrReservedMemCurrent, &reserved) ==
-            cudaSuccess &&
-        cudaMemPoolGetAttribute(pool, cudaMemPoolAttrUsedMemCurrent, &used) == cudaSuccess &&
-        reserved > used)
-        fr += static_cast<size_t>(reserved - used);
-    cudaGetLastError();
-    return fr;
-}
+size_t free_hbm(sp3mm_ctx* ctx) { return free_device_bytes(ctx); }
 
 }  // namespace
 
