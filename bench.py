@@ -61,6 +61,11 @@ def parse_args():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--cpu-seconds", type=float, default=12.0,
                     help="target CPU time of the cpu_baseline sample")
+    ap.add_argument("--no-batched", action="store_true", help="skip the batched workload")
+    ap.add_argument("--no-served", action="store_true", help="skip the served workload")
+    ap.add_argument("--batch-count", type=int, default=256)
+    ap.add_argument("--serve-count", type=int, default=200)
+    ap.add_argument("--serve-rate", type=float, default=100.0, help="requests per second")
     return ap.parse_args()
 
 
@@ -203,6 +208,154 @@ def run_reference_arm(args, prob, nnz_c):
 
 
 # ---------------------------------------------------------------------------
+# Batched and served workloads.
+
+def _events_time(torch, stream, fn):
+    """Seconds of fn() between events on the context stream (host waits
+    inside fn are part of it)."""
+    a = torch.cuda.Event(enable_timing=True)
+    b = torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    a.record(stream)
+    fn()
+    b.record(stream)
+    b.synchronize()
+    return a.elapsed_time(b) * 1e-3
+
+
+def run_batched(S, torch, ctx, stream, count, seed=3, min_coarse=1000):
+    """Many uneven products: the R*A*P products of `count` device-built
+    smoothed-aggregation hierarchies (2D 5-point / 3D 7-point, n log-uniform
+    in [1e3, 2e5], each repeated until n < 1000), computed one product per
+    call versus as one batch (plan + execute) and as graph replays."""
+    specs = pb.config3_specs(seed, count)
+    ops = [pb.stencil_operator(d) for d in specs]
+    dA = [ctx.upload(o) for o in ops]
+    # Warm-up at full size: the memory pool grows to the workload's needs.
+    for h in ctx.hierarchies(dA, specs, min_coarse=min_coarse, max_levels=20):
+        h.free()
+    hs = []
+    t_hb = _events_time(torch, stream, lambda: hs.extend(
+        ctx.hierarchies(dA, specs, min_coarse=min_coarse, max_levels=20)))
+
+    def singles():
+        for a, d in zip(dA, specs):
+            ctx.hierarchy(a, d, min_coarse=min_coarse, max_levels=20).free()
+    t_hs = _events_time(torch, stream, singles)
+    prods = []
+    for h in hs:
+        for lvl in range(len(h) - 1):
+            A, P, R = h.level(lvl)
+            prods.append((R, A, P))
+    rows = sum(p[0].shape[0] for p in prods)
+
+    def plain():
+        for R, A, P in prods:
+            ctx.rap(R, A, P, S.DIRECT, S.UB).free()
+    plain()   # warm-up
+    t_plain = min(_events_time(torch, stream, plain) for _ in range(2))
+    t_full, reps = [], 10
+    launches0 = ctx.launches()
+    for i in range(3):
+        box = {}
+        t = _events_time(torch, stream, lambda: box.update(b=ctx.batch(prods)) or box["b"].run())
+        b = box["b"]
+        if i > 0:
+            t_full.append(t)
+        if i < 2:
+            b.free()
+    full_launches = (ctx.launches() - launches0) // 3
+    tune = b.autotune(3)
+    t_rep = _events_time(torch, stream, lambda: [b.execute() for _ in range(reps)]) / reps
+    info = b.info()
+    b.free()
+    for h in hs:
+        h.free()
+    for a in dA:
+        a.free()
+    n = len(prods)
+    tf = min(t_full)
+    return {
+        "workload": f"{count} hierarchies (2D 5-pt / 3D 7-pt, n log-uniform 1e3..2e5, "
+                    f"seed {seed}), every R*A*P level product until n < {min_coarse}",
+        "products": n, "rows_C": rows, "nnz_C": info["nnz"],
+        "plain_products_per_s": n / t_plain,
+        "batch_products_per_s": n / tf, "speedup": t_plain / tf,
+        "replay_products_per_s": n / t_rep, "replay_speedup": t_plain / t_rep,
+        "plain_s": t_plain, "batch_s": tf, "replay_s": t_rep,
+        "batch_launches": full_launches, "tiers": info["tiers"],
+        "autotune": tune.strip().splitlines()[:3],
+        "hierarchy_build_batched_s": t_hb, "hierarchy_build_single_s": t_hs,
+        "hierarchy_build_speedup": t_hs / t_hb,
+        "timing": "CUDA events on the context stream around each whole pass",
+    }
+
+
+def _level_errors(h32, h64):
+    """Per level: max relative error of FP32-stored values against FP64
+    (over entries with |ref| > 0) and max error normalised by max |ref|."""
+    out = []
+    for lvl in range(len(h64)):
+        a = h32.level(lvl)[0].download()
+        b = h64.level(lvl)[0].download()
+        if not np.array_equal(a.indices, b.indices) or not np.array_equal(a.indptr, b.indptr):
+            raise RuntimeError("FP32 and FP64 hierarchies differ in pattern")
+        ref = np.abs(b.data)
+        nz = ref > 0
+        rel = float(np.max(np.abs(a.data[nz] - b.data[nz]) / ref[nz])) if nz.any() else 0.0
+        norm = float(np.max(np.abs(a.data - b.data)) / ref.max()) if ref.size else 0.0
+        out.append((rel, norm))
+    return out
+
+
+def run_served(S, ctx, count, rate, seed=4, err_sample=24):
+    """A Poisson stream of hierarchy-setup requests (90% of config-3 sizes,
+    10% 3D 64^3..128^3) served by continuous batching versus one request at
+    a time, at `rate` requests/s and saturated (all arriving at once)."""
+    from sp3mm4amg_b200 import serving
+    specs = pb.config4_specs(seed, count)
+    ops = [pb.stencil_operator(d) for d in specs]
+    arrivals = pb.poisson_arrivals(rate, count, seed + 1)
+    # Warm-up at full size (the memory pool grows to the workload's needs).
+    serving.serve_batched(ctx, specs, np.zeros(count), operators=ops)
+    res = {"workload": f"{count} requests (seed {seed}): 90% 2D/3D n log-uniform 1e3..2e5, "
+                       f"10% 3D side 64..128; hierarchy to n < 1000",
+           "rate_per_s": rate}
+    for name, cvt in (("fp64", S.F64), ("fp32_coarse", S.F32)):
+        st, _ = serving.serve_batched(ctx, specs, arrivals, coarse_val_type=cvt, operators=ops)
+        sat, _ = serving.serve_batched(ctx, specs, np.zeros(count), coarse_val_type=cvt,
+                                       operators=ops)
+        res[name] = {"p50_s": st["p50_s"], "p99_s": st["p99_s"],
+                     "products_per_s": st["products_per_s"], "products": st["products"],
+                     "peak_active": st["peak_active"], "failed": st["failed"],
+                     "saturated_products_per_s": sat["products_per_s"],
+                     "saturated_p99_s": sat["p99_s"]}
+    plain = serving.serve_plain(ctx, specs, arrivals, operators=ops)
+    plain_sat = serving.serve_plain(ctx, specs, np.zeros(count), operators=ops)
+    res["plain_fp64"] = {"p50_s": plain["p50_s"], "p99_s": plain["p99_s"],
+                         "products_per_s": plain["products_per_s"],
+                         "saturated_products_per_s": plain_sat["products_per_s"]}
+    res["saturated_speedup_fp64"] = (res["fp64"]["saturated_products_per_s"] /
+                                     plain_sat["products_per_s"])
+    # FP32 coarse storage: per-level error against the FP64 hierarchies
+    # (which equal the oracle chain bit for bit) on a request sample.
+    k = min(err_sample, count)
+    _, h64 = serving.serve_batched(ctx, specs[:k], np.zeros(k), S.F64, keep=True,
+                                   operators=ops[:k])
+    _, h32 = serving.serve_batched(ctx, specs[:k], np.zeros(k), S.F32, keep=True,
+                                   operators=ops[:k])
+    per_level = {}
+    for a, b in zip(h32, h64):
+        for lvl, (rel, norm) in enumerate(_level_errors(a, b)):
+            r0, n0 = per_level.get(lvl, (0.0, 0.0))
+            per_level[lvl] = (max(r0, rel), max(n0, norm))
+        a.free()
+        b.free()
+    res["fp32_level_max_rel_err"] = {str(lvl): v[0] for lvl, v in sorted(per_level.items())}
+    res["fp32_level_max_err_over_max"] = {str(lvl): v[1] for lvl, v in sorted(per_level.items())}
+    res["fp32_error_sample"] = f"first {k} requests, every level"
+    return res
+
 
 def main():
     args = parse_args()
@@ -360,6 +513,10 @@ def main():
         "gpu_launches": launches,
         "clocks": clk,
     }
+    if rank == 0 and not args.no_batched:
+        line["batched"] = run_batched(S, torch, ctx, stream, args.batch_count)
+    if rank == 0 and not args.no_served:
+        line["served"] = run_served(S, ctx, args.serve_count, args.serve_rate)
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         threads = os.cpu_count() or 1
         kind, run, desc = cpu_reference_runner(prob, threads)

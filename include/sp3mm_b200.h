@@ -336,8 +336,10 @@ SP3MM_API int sp3mm_batch_run(sp3mm_batch *b);
  * fastest; one line per candidate is written to report (may be NULL). */
 SP3MM_API int sp3mm_batch_autotune(sp3mm_batch *b, int reps, char *report, size_t len);
 SP3MM_API int sp3mm_batch_result(const sp3mm_batch *b, int i, sp3mm_dcsr *C);
+/* Rows and nonzeros of the batch, numeric tiers (of which in global
+ * memory), and rows the last plan redid with proven table sizes. */
 SP3MM_API int sp3mm_batch_info(const sp3mm_batch *b, int64_t *rows, int64_t *nnz, int *tiers,
-                               int *global_tiers);
+                               int *global_tiers, int64_t *retried);
 SP3MM_API int sp3mm_batch_free(sp3mm_batch *b);
 
 /* ---- Smoothed-aggregation setup around the product --------------------

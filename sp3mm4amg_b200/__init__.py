@@ -432,13 +432,13 @@ class Batch:
         return DeviceCSR(self.ctx, d, owned=False)
 
     def info(self) -> dict:
-        rows, nnz = ctypes.c_int64(), ctypes.c_int64()
+        rows, nnz, retried = ctypes.c_int64(), ctypes.c_int64(), ctypes.c_int64()
         tiers, gt = ctypes.c_int(), ctypes.c_int()
         self.ctx._check(self.ctx.lib.sp3mm_batch_info(self.h, ctypes.byref(rows),
                                                       ctypes.byref(nnz), ctypes.byref(tiers),
-                                                      ctypes.byref(gt)))
+                                                      ctypes.byref(gt), ctypes.byref(retried)))
         return {"rows": rows.value, "nnz": nnz.value, "tiers": tiers.value,
-                "global_tiers": gt.value}
+                "global_tiers": gt.value, "retried": retried.value}
 
     def free(self) -> None:
         if self.h:

@@ -83,7 +83,7 @@ DEVICE_API = {
     "sp3mm_batch_result": (_c.c_int, [_c.c_void_p, _c.c_int, _c.c_void_p]),
     "sp3mm_batch_info": (_c.c_int, [_c.c_void_p, _c.POINTER(_c.c_int64),
                                     _c.POINTER(_c.c_int64), _c.POINTER(_c.c_int),
-                                    _c.POINTER(_c.c_int)]),
+                                    _c.POINTER(_c.c_int), _c.POINTER(_c.c_int64)]),
     "sp3mm_batch_free": (_c.c_int, [_c.c_void_p]),
     "sp3mm_server_create": (_c.c_int, [_c.c_void_p, _c.c_int, _c.c_double,
                                        _c.POINTER(_c.c_void_p)]),

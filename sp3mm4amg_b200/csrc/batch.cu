@@ -135,6 +135,7 @@ struct BatchTier {
     int lo = 0, hi = 0;      // levels [lo, hi]
     int first = 0, count = 0;   // rows: lists[first, first + count)
     int scap = 0;
+    int slack = 0;           // numeric: tables 2^slack times the exact size
     bool gt = false;
     int block = 0, grid = 0;
     size_t smem = 0;
@@ -154,6 +155,7 @@ struct sp3mm_batch {
     bool trimmed = false;
     std::vector<int> splits;
     bool auto_split = true;
+    std::vector<int> level_slack = std::vector<int>(kLevels, -1);   // per top level; -1: slack
     int warps_cap = 8;
     // Device state.
     DevBuf d_items, d_bases, d_row_item, d_need, d_cnt1, d_cnt2, d_crp;
@@ -164,6 +166,7 @@ struct sp3mm_batch {
     std::vector<long long> rp_off;
     std::vector<sp3mm_dcsr> results;
     long long nnz = 0;
+    long long retried = 0;   // rows of the last plan redone with proven tables
     bool planned = false;
     // Numeric graph (tiers as parallel branches).
     cudaGraph_t graph = nullptr;
@@ -232,7 +235,12 @@ int make_tiers(sp3mm_batch* b, const Bins& bins, int mode, int extra, int tv, in
         }
         t.first = bins.offsets[t.lo];
         t.count = bins.offsets[t.hi] + bins.counts[t.hi] - t.first;
-        const int top = std::min(t.hi + extra, 30 - 5);
+        int ex = extra;
+        if (mode == kNumExact) {
+            ex = b->level_slack[t.hi] >= 0 ? b->level_slack[t.hi] : b->slack;
+            t.slack = ex;
+        }
+        const int top = std::min(t.hi + ex, 30 - 5);
         t.scap = 32 << top;
         const size_t bytes = batch_row_region_bytes(num, t.scap);
         if (bytes > ctx->smem_optin) {
@@ -244,6 +252,7 @@ int make_tiers(sp3mm_batch* b, const Bins& bins, int mode, int extra, int tv, in
             gt.hi = t.hi;
             gt.count = bins.offsets[t.hi] + bins.counts[t.hi] - gt.first;
             gt.scap = t.scap;
+            gt.slack = t.slack;
             L = M;
             continue;
         }
@@ -305,6 +314,7 @@ int run_tiers(sp3mm_batch* b, int mode, const std::vector<BatchTier>& tiers, con
         p.rows = lists + t.first;
         p.nrows = t.count;
         p.scap = t.scap;
+        if (mode == kNumExact) p.slack = t.slack;
         p.reverse = t.hi > t.lo ? 1 : 0;
         size_t smem = t.smem;
         if (t.gt) {
@@ -415,6 +425,7 @@ int row_pass(sp3mm_batch* b, int mode, const Bins& sb, BatchRowParams p, int* ri
         CK(ctx, cudaStreamSynchronize(st));
         if (h[0] == 0) break;
         if (round == 3) return batch_fail(b, SP3MM_EDEVICE, "row retries did not converge");
+        b->retried += h[0];
         CK(ctx, cudaMemsetAsync(rinfo, 0, 2 * sizeof(int), st));
         BatchTier t;
         t.gt = true;
@@ -464,6 +475,7 @@ int batch_plan(sp3mm_batch* b) {
     const size_t R1 = static_cast<size_t>(rows) + 1;
     b->planned = false;
     b->values_ready = false;
+    b->retried = 0;
     if (b->exec) cudaGraphExecDestroy(b->exec);
     if (b->graph) cudaGraphDestroy(b->graph);
     b->exec = nullptr;
@@ -513,14 +525,15 @@ int batch_plan(sp3mm_batch* b) {
         // cursor, in space bounded by the output bound, by eight times the
         // operands' nonzeros and by half the free memory (a batch that
         // overflows it is planned symbolically instead).
-        const size_t fr = free_device_bytes(ctx);
         const size_t eb = sizeof(int) + vbytes(b->to);
         long long in_nnz = 0;
         for (const BItem& I : b->items)
             in_nnz += I.X.nnz + I.Y.nnz + (I.kind == kBatchDirect ? I.Z.nnz : 0);
-        const unsigned long long budget = std::max<unsigned long long>(
-            1ULL << 20, std::min<unsigned long long>(8ULL * in_nnz, fr / 2 / eb));
-        const unsigned long long cap = std::min<unsigned long long>(sb.total, budget);
+        unsigned long long cap = std::min<unsigned long long>(
+            sb.total, std::max<unsigned long long>(1ULL << 20, 8ULL * in_nnz));
+        if (cap * eb > (size_t(1) << 30))
+            cap = std::min<unsigned long long>(
+                cap, std::max<unsigned long long>(1ULL << 20, free_device_bytes(ctx) / 2 / eb));
         TRY(ub_ci.alloc(ctx, sizeof(int) * std::max<unsigned long long>(cap, 1)));
         TRY(ub_v.alloc(ctx, vbytes(b->to) * std::max<unsigned long long>(cap, 1)));
         TRY(row_off.alloc(ctx, sizeof(long long) * R1));
@@ -776,10 +789,11 @@ int sp3mm_batch_result(const sp3mm_batch* b, int i, sp3mm_dcsr* C) {
 }
 
 int sp3mm_batch_info(const sp3mm_batch* b, int64_t* rows, int64_t* nnz, int* tiers,
-                     int* global_tiers) {
+                     int* global_tiers, int64_t* retried) {
     if (!b) return SP3MM_EINVAL;
     if (rows) *rows = b->rows;
     if (nnz) *nnz = b->nnz;
+    if (retried) *retried = b->retried;
     int t = 0, g = 0;
     for (const auto& x : b->tiers) (x.gt ? g : t)++;
     if (tiers) *tiers = t + g;
@@ -801,29 +815,9 @@ int sp3mm_batch_autotune(sp3mm_batch* b, int reps, char* report, size_t len) {
     if (!b->planned) TRY(batch_plan(b));
     if (b->trimmed) return batch_fail(b, SP3MM_EINVAL, "the batch was trimmed");
     TRY(ensure_numeric(b));
-    struct Cand {
-        bool autos;
-        std::vector<int> splits;
-        int slack;
-        float ms;
-    };
-    std::vector<int> present;
-    for (int L = 0; L < kLevels; ++L)
-        if (b->nbins.counts[L]) present.push_back(L);
-    std::vector<Cand> cands;
-    for (int slack = 0; slack <= 1; ++slack) {
-        cands.push_back({true, {}, slack, 0.f});
-        cands.push_back({false, {}, slack, 0.f});
-        for (size_t k = 1; k < present.size() && k <= 4; ++k)
-            cands.push_back({false, {present[k]}, slack, 0.f});
-    }
     std::string rep;
-    size_t best = 0;
-    for (size_t c = 0; c < cands.size(); ++c) {
-        Cand& k = cands[c];
-        b->auto_split = k.autos;
-        b->splits = k.splits;
-        b->slack = k.slack;
+    // Time `reps` replays of the current numeric graph.
+    auto time_graph = [&](float* out) -> int {
         TRY(build_numeric(b));
         CK(ctx, cudaGraphLaunch(b->exec, st));   // warm-up
         CK(ctx, cudaEventRecord(ctx->ev0, st));
@@ -832,22 +826,65 @@ int sp3mm_batch_autotune(sp3mm_batch* b, int reps, char* report, size_t len) {
         CK(ctx, cudaEventSynchronize(ctx->ev1));
         float ms = 0.f;
         CK(ctx, cudaEventElapsedTime(&ms, ctx->ev0, ctx->ev1));
-        k.ms = ms / reps;
+        *out = ms / reps;
+        return SP3MM_OK;
+    };
+    // 1. Tiering: one tier per level, a single tier, or two tiers split at
+    //    one of the first present levels.
+    struct Cand {
+        bool autos;
+        std::vector<int> splits;
+        float ms;
+    };
+    std::vector<int> present;
+    for (int L = 0; L < kLevels; ++L)
+        if (b->nbins.counts[L]) present.push_back(L);
+    std::vector<Cand> cands;
+    cands.push_back({true, {}, 0.f});
+    cands.push_back({false, {}, 0.f});
+    for (size_t k = 1; k < present.size() && k <= 4; ++k) cands.push_back({false, {present[k]}, 0.f});
+    std::fill(b->level_slack.begin(), b->level_slack.end(), -1);
+    b->slack = 0;
+    size_t best = 0;
+    for (size_t c = 0; c < cands.size(); ++c) {
+        Cand& k = cands[c];
+        b->auto_split = k.autos;
+        b->splits = k.splits;
+        TRY(time_graph(&k.ms));
         char line[160];
-        snprintf(line, sizeof line, "%s split=%d slack=%d tiers=%zu ms=%.4f\n",
+        snprintf(line, sizeof line, "%s split=%d tiers=%zu ms=%.4f\n",
                  k.autos ? "per-level" : (k.splits.empty() ? "one-tier" : "two-tier"),
-                 k.splits.empty() ? -1 : k.splits[0], k.slack, b->tiers.size(), k.ms);
+                 k.splits.empty() ? -1 : k.splits[0], b->tiers.size(), k.ms);
         rep += line;
-        if (k.ms < cands[best].ms || c == 0) best = c;
+        if (k.ms < cands[best].ms) best = c;
     }
-    TRY(check_device_err(ctx));
     b->auto_split = cands[best].autos;
     b->splits = cands[best].splits;
-    b->slack = cands[best].slack;
+    float best_ms = cands[best].ms;
+    // 2. Table slack per tier (larger tables shorten probe chains of heavy
+    //    rows at the cost of shared memory per warp).
     TRY(build_numeric(b));
-    if (report && len) {
-        snprintf(report, len, "%s", rep.c_str());
+    std::vector<int> tops;
+    for (const auto& t : b->tiers) tops.push_back(t.hi);
+    for (int top : tops) {
+        for (int sl = 1; sl <= 2; ++sl) {
+            const int keep = b->level_slack[top];
+            b->level_slack[top] = sl;
+            float ms = 0.f;
+            TRY(time_graph(&ms));
+            char line[160];
+            snprintf(line, sizeof line, "  tier level %d slack=%d ms=%.4f\n", top, sl, ms);
+            rep += line;
+            if (ms < best_ms) best_ms = ms;
+            else b->level_slack[top] = keep;
+        }
     }
+    TRY(check_device_err(ctx));
+    TRY(build_numeric(b));
+    char line[96];
+    snprintf(line, sizeof line, "best ms=%.4f\n", best_ms);
+    rep += line;
+    if (report && len) snprintf(report, len, "%s", rep.c_str());
     return SP3MM_OK;
 }
 

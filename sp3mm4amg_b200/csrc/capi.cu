@@ -49,20 +49,34 @@ int check_dcsr(sp3mm_ctx* ctx, const sp3mm_dcsr* m, const char* what) {
 }
 
 size_t free_device_bytes(sp3mm_ctx* ctx) {
-    size_t fr = 0, tot = 0;
-    if (cudaMemGetInfo(&fr, &tot) != cudaSuccess) {
-        cudaGetLastError();
-        return 0;
-    }
+    // The reading is refreshed every 100 ms; in between, the pool's own
+    // growth is subtracted from it (other processes' use is seen at the
+    // next refresh).
     cudaMemPool_t pool;
     uint64_t reserved = 0, used = 0;
-    if (cudaDeviceGetDefaultMemPool(&pool, ctx->device) == cudaSuccess &&
-        cudaMemPoolGetAttribute(pool, cudaMemPoolAttrReservedMemCurrent, &reserved) ==
-            cudaSuccess &&
-        cudaMemPoolGetAttribute(pool, cudaMemPoolAttrUsedMemCurrent, &used) == cudaSuccess &&
-        reserved > used)
-        fr += static_cast<size_t>(reserved - used);
-    cudaGetLastError();
+    if (cudaDeviceGetDefaultMemPool(&pool, ctx->device) != cudaSuccess ||
+        cudaMemPoolGetAttribute(pool, cudaMemPoolAttrReservedMemCurrent, &reserved) !=
+            cudaSuccess ||
+        cudaMemPoolGetAttribute(pool, cudaMemPoolAttrUsedMemCurrent, &used) != cudaSuccess) {
+        cudaGetLastError();
+        reserved = used = 0;
+    }
+    const double now = std::chrono::duration<double>(
+                           std::chrono::steady_clock::now().time_since_epoch())
+                           .count();
+    if (ctx->free_checked_s < 0 || now - ctx->free_checked_s > 0.1) {
+        size_t fr = 0, tot = 0;
+        if (cudaMemGetInfo(&fr, &tot) != cudaSuccess) {
+            cudaGetLastError();
+            return 0;
+        }
+        ctx->free_at_check = fr;
+        ctx->reserved_at_check = reserved;
+        ctx->free_checked_s = now;
+    }
+    const uint64_t grown = reserved > ctx->reserved_at_check ? reserved - ctx->reserved_at_check : 0;
+    size_t fr = ctx->free_at_check > grown ? ctx->free_at_check - grown : 0;
+    if (reserved > used) fr += static_cast<size_t>(reserved - used);
     return fr;
 }
 
@@ -343,12 +357,14 @@ int product_rows(sp3mm_ctx* ctx, RowRunner& rr, int M, int N, int flavour, int o
         // Rows book their exact length from one cursor, so the space need
         // only exceed nnz(C): the bound, capped at half the free memory; a
         // product that still overflows it is redone symbolically.
-        const unsigned long long budget = std::max<unsigned long long>(
-            1ULL << 20,
-            std::min<unsigned long long>(
-                8ULL * static_cast<unsigned long long>(rr.operand_nnz()),
-                free_device_bytes(ctx) / 2 / (sizeof(int) + vbytes(out_vt))));
-        const unsigned long long cap = std::min<unsigned long long>(bins.total, budget);
+        const size_t eb = sizeof(int) + vbytes(out_vt);
+        unsigned long long cap = std::min<unsigned long long>(
+            bins.total,
+            std::max<unsigned long long>(1ULL << 20,
+                                         8ULL * static_cast<unsigned long long>(rr.operand_nnz())));
+        if (cap * eb > (size_t(1) << 30))
+            cap = std::min<unsigned long long>(
+                cap, std::max<unsigned long long>(1ULL << 20, free_device_bytes(ctx) / 2 / eb));
         DevBuf ub_ci, ub_v, row_off;
         TRY(ub_ci.alloc(ctx, sizeof(int) * cap));
         TRY(ub_v.alloc(ctx, vbytes(out_vt) * cap));

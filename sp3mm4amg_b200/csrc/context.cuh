@@ -32,6 +32,11 @@ struct sp3mm_ctx {
     };
     bool profiling = false;
     std::vector<ProfRec> prof;
+    // Last free-memory reading (cudaMemGetInfo costs milliseconds): the
+    // free bytes, the pool's reserved bytes then, and when it was taken.
+    size_t free_at_check = 0;
+    uint64_t reserved_at_check = 0;
+    double free_checked_s = -1.0;
 };
 
 namespace sp3mm {

@@ -143,15 +143,44 @@ __device__ __forceinline__ bool waccumulate(const Left& L, int n, const int* __r
         }
         int total;
         const int off = wscan_excl(len, total);
+        // Short right rows: each lane copies its own run.  Long rows: every
+        // lane fills window slots, finding the slot's step by a binary
+        // search over the lanes' offsets (the last lane whose offset is at
+        // most the slot's position, which has a non-empty run).
+        const bool spread = __reduce_max_sync(kFull, static_cast<unsigned>(len)) > 16u;
         for (int w0 = 0; w0 < total; w0 += kStage) {
-            // Stage this lane's entries of window [w0, w0 + kStage).
-            const int e_end = min(len, w0 + kStage - off);
-            int e = max(0, w0 - off);
+            if (spread) {
+                const int wl = min(kStage, total - w0);
+#pragma unroll
+                for (int r = 0; r < kStage / 32; ++r) {
+                    const int i = lane + 32 * r;
+                    const int pidx = w0 + i;
+                    int j = 0;
+#pragma unroll
+                    for (int step = 16; step > 0; step >>= 1) {
+                        const int oc = __shfl_sync(kFull, off, j + step);
+                        if (oc <= pidx) j += step;
+                    }
+                    const int rbj = __shfl_sync(kFull, rb, j);
+                    const int ofj = __shfl_sync(kFull, off, j);
+                    double sj = 0.0;
+                    if (NUM) sj = __shfl_sync(kFull, s, j);
+                    if (i < wl) {
+                        const int e = rbj + pidx - ofj;
+                        sk[i] = __ldg(b_ci + e);
+                        if (NUM) sv[i] = __dmul_rn(ldv(b_v, e), sj);
+                    }
+                }
+            } else {
+                // Stage this lane's entries of window [w0, w0 + kStage).
+                const int e_end = min(len, w0 + kStage - off);
+                int e = max(0, w0 - off);
 #pragma unroll 4
-            for (; e < e_end; ++e) {
-                const int pos = off + e - w0;
-                sk[pos] = __ldg(b_ci + rb + e);
-                if (NUM) sv[pos] = __dmul_rn(ldv(b_v, rb + e), s);
+                for (; e < e_end; ++e) {
+                    const int pos = off + e - w0;
+                    sk[pos] = __ldg(b_ci + rb + e);
+                    if (NUM) sv[pos] = __dmul_rn(ldv(b_v, rb + e), s);
+                }
             }
             __syncwarp();
             const int wl = min(kStage, total - w0);
