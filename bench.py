@@ -63,6 +63,7 @@ def parse_args():
                     help="target CPU time of the cpu_baseline sample")
     ap.add_argument("--no-batched", action="store_true", help="skip the batched workload")
     ap.add_argument("--no-served", action="store_true", help="skip the served workload")
+    ap.add_argument("--no-irregular", action="store_true", help="skip the irregular workload")
     ap.add_argument("--batch-count", type=int, default=256)
     ap.add_argument("--serve-count", type=int, default=200)
     ap.add_argument("--serve-rate", type=float, default=100.0, help="requests per second")
@@ -291,6 +292,35 @@ def run_batched(S, torch, ctx, stream, count, seed=3, min_coarse=1000):
     }
 
 
+def run_irregular(S, torch, ctx, stream, npoints=1_000_000, steps=10):
+    """The irregular product: kNN graph Laplacian of `npoints` seeded points
+    (16 neighbours, symmetrised), greedy aggregation, one Jacobi step;
+    direct upper-bound R*A*P timed on the device, inputs resident."""
+    prob = pb.knn_problem(npoints, seed=2)
+    d = [ctx.upload(m) for m in (prob.R, prob.A, prob.P)]
+    nnz_c = 0
+    for _ in range(3):
+        C = ctx.rap(*d, S.DIRECT, S.UB)
+        nnz_c = C.nnz
+        C.free()
+    t = _events_time(torch, stream, lambda: [ctx.rap(*d, S.DIRECT, S.UB).free()
+                                             for _ in range(steps)]) / steps
+    ctx.set_profiling(True)
+    ctx.rap(*d, S.DIRECT, S.UB).free()
+    prof = ctx.profile()
+    ctx.set_profiling(False)
+    for m in d:
+        m.free()
+    total = prob.compulsory_bytes(nnz_c=nnz_c, idx_bytes=4)
+    deg = np.diff(prob.A.indptr) - 1
+    return {"workload": f"knn16 Laplacian, {npoints} points (seed 2), greedy aggregation "
+                        f"(mean {prob.A.M / prob.P.N:.2f} per aggregate), Jacobi-smoothed P",
+            "rows_R": prob.R.M, "nnz_A": prob.A.nnz, "nnz_P": prob.P.nnz, "nnz_C": nnz_c,
+            "degree_min_max": [int(deg.min()), int(deg.max())],
+            "ms_per_product": t * 1e3, "GBps": total / t / 1e9, "bytes_per_product": total,
+            "kernels_ms": {k: v[1] for k, v in prof.items()}}
+
+
 def _level_errors(h32, h64):
     """Per level: max relative error of FP32-stored values against FP64
     (over entries with |ref| > 0) and max error normalised by max |ref|."""
@@ -517,6 +547,8 @@ def main():
         line["batched"] = run_batched(S, torch, ctx, stream, args.batch_count)
     if rank == 0 and not args.no_served:
         line["served"] = run_served(S, ctx, args.serve_count, args.serve_rate)
+    if rank == 0 and not args.no_irregular:
+        line["irregular"] = run_irregular(S, torch, ctx, stream)
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         threads = os.cpu_count() or 1
         kind, run, desc = cpu_reference_runner(prob, threads)

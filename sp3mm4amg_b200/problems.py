@@ -241,3 +241,112 @@ def poisson_arrivals(rate: float, count: int, seed: int = 5) -> np.ndarray:
 def stencil_operator(dims) -> CSR:
     """The 5-point (2D) or 7-point (3D) Poisson operator on a box grid."""
     return poisson3d(*dims) if len(dims) == 3 else poisson2d(*dims)
+
+
+def knn_laplacian(npoints: int, k: int = 16, seed: int = 2):
+    """Symmetric graph Laplacian of `npoints` seeded uniform points in the
+    unit cube joined to their k nearest neighbours (pattern symmetrised):
+    off-diagonal weights -U(0.5, 1.5) (one draw per undirected edge), the
+    diagonal the sum of |off-diagonals| plus 1e-3.  Returns (A, points)."""
+    from scipy.spatial import cKDTree
+    rng = np.random.default_rng(seed)
+    pts = rng.random((npoints, 3))
+    _, nb = cKDTree(pts).query(pts, k=k + 1)
+    rows = np.repeat(np.arange(npoints, dtype=np.int64), k)
+    cols = nb[:, 1:].reshape(-1).astype(np.int64)
+    lo, hi = np.minimum(rows, cols), np.maximum(rows, cols)
+    key = np.unique(lo * npoints + hi)          # undirected edges, sorted
+    ei, ej = key // npoints, key % npoints
+    w = -rng.uniform(0.5, 1.5, key.size)
+    off = sp.coo_matrix((np.concatenate([w, w]), (np.concatenate([ei, ej]),
+                                                  np.concatenate([ej, ei]))),
+                        shape=(npoints, npoints)).tocsr()
+    diag = np.asarray(abs(off).sum(axis=1)).ravel() + 1e-3
+    A = (off + sp.diags(diag)).tocsr()
+    return CSR.from_scipy(A), pts
+
+
+def greedy_aggregation(A: CSR, seed: int = 2, max_size: int = 8,
+                       min_free: int = 5) -> np.ndarray:
+    """Aggregate labels by seeded parallel greedy aggregation: in rounds,
+    every unaggregated vertex with at least `min_free` unaggregated
+    neighbours whose random priority is the smallest among them becomes a
+    root and claims up to max_size-1 of its unaggregated neighbours
+    (strongest |a_ij| first; a neighbour adjacent to several roots goes to
+    the one with the smallest priority), so every aggregate has diameter
+    <= 2.  The vertices left over join the aggregate of their strongest
+    aggregated neighbour (in rounds, as aggregates reach them)."""
+    n = A.M
+    rng = np.random.default_rng(seed)
+    prio = np.empty(n, np.int64)
+    prio[rng.permutation(n)] = np.arange(n)
+    rp, ci = A.indptr.astype(np.int64), A.indices.astype(np.int64)
+    rows = np.repeat(np.arange(n, dtype=np.int64), np.diff(rp))
+    offd = ci != rows
+    er, ec, ew = rows[offd], ci[offd], np.abs(A.data[offd])
+    agg = np.full(n, -1, np.int64)
+    nagg = 0
+    big = np.iinfo(np.int64).max
+    while True:
+        free = agg < 0
+        live = free[er] & free[ec]
+        # smallest priority among each free vertex and its free neighbours
+        m = np.where(free, prio, big)
+        np.minimum.at(m, er[live], prio[ec[live]])
+        fdeg = np.bincount(er[live], minlength=n)
+        cand = free & (fdeg >= min_free)
+        # candidates: the local minimum among candidate neighbours
+        mc = np.where(cand, prio, big)
+        lc = live & cand[er] & cand[ec]
+        np.minimum.at(mc, er[lc], prio[ec[lc]])
+        roots = np.flatnonzero(cand & (mc == prio))
+        if roots.size == 0:
+            break
+        is_root = np.zeros(n, bool)
+        is_root[roots] = True
+        # candidate claims: free non-root neighbour u of a root r
+        c = live & is_root[er] & ~is_root[ec]
+        cr, cu, cw = er[c], ec[c], ew[c]
+        # each u keeps the root of smallest priority
+        best = np.full(n, big)
+        np.minimum.at(best, cu, prio[cr])
+        keep = prio[cr] == best[cu]
+        cr, cu, cw = cr[keep], cu[keep], cw[keep]
+        # each root keeps its max_size-1 strongest claims
+        order = np.lexsort((-cw, prio[cr]))
+        cr, cu = cr[order], cu[order]
+        first = np.ones(cr.size, bool)
+        first[1:] = cr[1:] != cr[:-1]
+        start = np.maximum.accumulate(np.where(first, np.arange(cr.size), 0))
+        take = (np.arange(cr.size) - start) < max_size - 1
+        ids = nagg + np.arange(roots.size)
+        label = np.full(n, -1, np.int64)
+        label[roots] = ids
+        agg[roots] = ids
+        agg[cu[take]] = label[cr[take]]
+        nagg += roots.size
+    while True:
+        # leftovers join the aggregate of their strongest aggregated neighbour
+        left = agg < 0
+        sel = left[er] & ~left[ec]
+        if not sel.any():
+            break
+        r, cc, w = er[sel], ec[sel], ew[sel]
+        order = np.lexsort((-w, r))
+        r, cc = r[order], cc[order]
+        first = np.ones(r.size, bool)
+        first[1:] = r[1:] != r[:-1]
+        agg[r[first]] = agg[cc[first]]
+    still = np.flatnonzero(agg < 0)          # no aggregated neighbour at all
+    agg[still] = nagg + np.arange(still.size)
+    return agg
+
+
+def knn_problem(npoints: int = 1_000_000, k: int = 16, seed: int = 2,
+                omega: float = 2.0 / 3.0) -> Problem:
+    """The irregular workload: kNN Laplacian, greedy aggregation, one
+    damped-Jacobi smoothing step, R = P^T."""
+    A, _ = knn_laplacian(npoints, k, seed)
+    P0 = aggregates_from_labels(greedy_aggregation(A, seed))
+    P = jacobi_smooth(A, P0, omega)
+    return Problem(f"knn{k}_{npoints}_seed{seed}", P.transpose(), A, P)
