@@ -387,6 +387,21 @@ def run_served(S, ctx, count, rate, seed=4, err_sample=24):
     return res
 
 
+def max_over_ranks(value: float, dist=None, device: str = "cpu") -> float:
+    """The slowest rank's time: every rank contributes, all receive the max."""
+    if dist is None:
+        return value
+    import torch
+    t = torch.tensor([value], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def job_value(units_per_rank: float, world: int, elapsed_s: float) -> float:
+    """Whole-job throughput: the units all ranks processed over the max time."""
+    return world * units_per_rank / elapsed_s
+
+
 def main():
     args = parse_args()
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -451,12 +466,9 @@ def main():
     launches = ctx.launches() - launches0
     clk = clocks.stop()
     elapsed_ms = ev0.elapsed_time(ev1)
-    if dist is not None:
-        t = torch.tensor([elapsed_ms], device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        elapsed_ms = float(t.item())
+    elapsed_ms = max_over_ranks(elapsed_ms, dist, "cuda")
     ms_per_step = elapsed_ms / args.steps
-    value = world * args.steps * total_bytes / (elapsed_ms * 1e-3) / 1e9
+    value = job_value(args.steps * total_bytes, world, elapsed_ms * 1e-3) / 1e9
 
     # Per-kernel device times (separate pass with per-launch events).
     ctx.set_profiling(True)

@@ -60,20 +60,30 @@ __device__ __forceinline__ WTab make_wtab(int* keys, double* vals, int* ord, int
 // Find `key` or claim an empty slot.  Only group leaders call it, so the
 // keys of concurrent callers are distinct.  The table never fills (the row
 // stops at the load limit), so the probe ends; it is bounded by the size.
+// Probing visits aligned buckets of four slots, read with one 16-byte load
+// (tables hold a power of two >= 32 slots at a 16-byte aligned base), which
+// cuts the divergent probe iterations of a warp's leaders about fourfold.
+// Where a key lands does not matter: insertion order is kept in T.ord.
 __device__ __forceinline__ int winsert(const WTab& T, int key, bool& is_new) {
-    unsigned s = hash_slot(key, T.shift);
-    for (unsigned probe = 0; probe <= T.smask; ++probe) {
-        const int k = T.keys[s];
-        if (k == key) return static_cast<int>(s);
-        if (k == kEmpty) {
-            const int old = atomicCAS(T.keys + s, kEmpty, key);
-            if (old == kEmpty) {
-                is_new = true;
-                return static_cast<int>(s);
+    unsigned s = hash_slot(key, T.shift) & ~3u;
+    for (unsigned probe = 0; probe <= T.smask; probe += 4) {
+        const int4 q = *reinterpret_cast<const int4*>(T.keys + s);
+        const int k[4] = {q.x, q.y, q.z, q.w};
+#pragma unroll
+        for (int j = 0; j < 4; ++j)
+            if (k[j] == key) return static_cast<int>(s) + j;
+#pragma unroll
+        for (int j = 0; j < 4; ++j) {
+            if (k[j] == kEmpty) {
+                const int old = atomicCAS(T.keys + s + j, kEmpty, key);
+                if (old == kEmpty) {
+                    is_new = true;
+                    return static_cast<int>(s) + j;
+                }
+                if (old == key) return static_cast<int>(s) + j;
             }
-            if (old == key) return static_cast<int>(s);
         }
-        s = (s + 1) & T.smask;
+        s = (s + 4) & T.smask;
     }
     return -1;
 }
