@@ -64,6 +64,8 @@ def parse_args():
     ap.add_argument("--no-batched", action="store_true", help="skip the batched workload")
     ap.add_argument("--no-served", action="store_true", help="skip the served workload")
     ap.add_argument("--no-irregular", action="store_true", help="skip the irregular workload")
+    ap.add_argument("--no-library", action="store_true",
+                    help="skip the cuSPARSE context measurement")
     ap.add_argument("--batch-count", type=int, default=256)
     ap.add_argument("--serve-count", type=int, default=200)
     ap.add_argument("--serve-rate", type=float, default=100.0, help="requests per second")
@@ -321,6 +323,37 @@ def run_irregular(S, torch, ctx, stream, npoints=1_000_000, steps=10):
             "kernels_ms": {k: v[1] for k, v in prof.items()}}
 
 
+def run_library(torch, prob, steps=5):
+    """Context only, not the product: the same product as (R*A)*P through
+    torch's sparse CSR matrix product on the device (cuSPARSE SpGEMM), FP64,
+    inputs resident."""
+    try:
+        dev = torch.device("cuda")
+
+        def t(m):
+            return torch.sparse_csr_tensor(
+                torch.as_tensor(m.indptr, dtype=torch.int64, device=dev),
+                torch.as_tensor(m.indices, dtype=torch.int64, device=dev),
+                torch.as_tensor(m.data, dtype=torch.float64, device=dev), size=m.shape)
+        R, A, P = t(prob.R), t(prob.A), t(prob.P)
+        C = (R @ A) @ P
+        torch.cuda.synchronize()
+        a = torch.cuda.Event(enable_timing=True)
+        b = torch.cuda.Event(enable_timing=True)
+        a.record()
+        for _ in range(steps):
+            C = (R @ A) @ P
+        b.record()
+        b.synchronize()
+        nnz = int(C._nnz())
+        del R, A, P, C
+        torch.cuda.empty_cache()
+        return {"library": "cuSPARSE SpGEMM via torch sparse CSR, (R*A)*P, FP64, int64 indices",
+                "ms_per_product": a.elapsed_time(b) / steps, "nnz_C": nnz}
+    except Exception as e:  # noqa: BLE001 - report, do not fail the bench
+        return {"library": "cuSPARSE SpGEMM via torch sparse CSR", "unavailable": repr(e)[:200]}
+
+
 def _level_errors(h32, h64):
     """Per level: max relative error of FP32-stored values against FP64
     (over entries with |ref| > 0) and max error normalised by max |ref|."""
@@ -555,6 +588,8 @@ def main():
         "gpu_launches": launches,
         "clocks": clk,
     }
+    if rank == 0 and not args.no_library:
+        line["library_context"] = run_library(torch, prob)
     if rank == 0 and not args.no_batched:
         line["batched"] = run_batched(S, torch, ctx, stream, args.batch_count)
     if rank == 0 and not args.no_served:
