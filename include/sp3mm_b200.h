@@ -385,13 +385,16 @@ SP3MM_API int sp3mm_hierarchy_build_batch(sp3mm_ctx *ctx, int n, const sp3mm_dcs
 
 /* ---- Request server: continuous batching of hierarchy setups ------------
  * Each request is a host CSR operator A0 (0-based int64 row_ptr/col, FP64
- * values; borrowed until the request is admitted) on a box grid.  Every
- * sp3mm_server_step admits queued requests first come first served while
- * fewer than max_active are in flight and the request's device-memory
+ * values; borrowed until the request is done or has failed) on a box grid.
+ * Every sp3mm_server_step admits queued requests first come first served
+ * while fewer than max_active are in flight and the request's device-memory
  * estimate fits both the budget (mem_fraction of the HBM free at creation,
- * less what admitted requests reserve) and the HBM free now; then advances
- * every admitted hierarchy by one level with batched launches shared by all
- * of them (results equal the single build's); then retires complete ones.
+ * less what admitted requests reserve) and the HBM free now, and hands them
+ * to the server's loader thread, which uploads them on its own stream while
+ * the step computes; then advances every uploaded hierarchy by one level
+ * with batched launches shared by all of them (results equal the single
+ * build's); then retires complete ones.  A request is reported active from
+ * admission on.
  * Times are seconds on the server's clock (sp3mm_server_now); a request's
  * latency runs from its arrival (given, or its submission) to the end of
  * the step that completed it.  Status: 0 queued, 1 active, 2 done,

@@ -480,7 +480,10 @@ class Server:
     def step(self) -> int:
         pending = ctypes.c_int()
         self.ctx._check(self.ctx.lib.sp3mm_server_step(self.h, ctypes.byref(pending)))
-        for rid in [r for r in self._inputs if self.poll(r)[0] != self.QUEUED]:
+        # The loader thread reads a request's host arrays until its upload is
+        # done; drop them once the request has finished.
+        for rid in [r for r in self._inputs
+                    if self.poll(r)[0] in (self.DONE, self.FAILED, self.TAKEN)]:
             del self._inputs[rid]
         return pending.value
 

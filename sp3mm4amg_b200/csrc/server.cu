@@ -7,12 +7,16 @@
 //   1. admits queued requests, first come first served, while a slot is
 //      free and the request's device-memory estimate fits both the server's
 //      budget (what admitted requests have reserved) and the HBM free right
-//      now (cudaMemGetInfo plus the idle part of the memory pool);
-//   2. advances every admitted hierarchy by one level in one level step
+//      now (cudaMemGetInfo plus the idle part of the memory pool), and hands
+//      them to the loader thread, which uploads them on its own context and
+//      stream while this step's kernels run (copies overlap compute);
+//   2. lets the requests the loader has finished join, waiting for the
+//      loader only when nothing else could run;
+//   3. advances every joined hierarchy by one level in one level step
 //      (hierarchy_step: batched launches shared by all requests, whatever
 //      their level or size, so requests admitted while others are in flight
 //      share the device with them);
-//   3. retires the hierarchies that are complete.
+//   4. retires the hierarchies that are complete.
 //
 // Results do not depend on what else is in a step: each product's rows are
 // computed by the same arithmetic whatever the batch.
@@ -20,8 +24,11 @@
 
 #include <algorithm>
 #include <chrono>
+#include <condition_variable>
 #include <deque>
 #include <memory>
+#include <mutex>
+#include <thread>
 #include <unordered_map>
 #include <vector>
 
@@ -52,6 +59,7 @@ struct Request {
     double t_arrival = 0, t_admit = -1, t_done = -1;
     size_t est = 0;
     size_t held = 0;   // bytes of the budget reserved while admitted
+    bool loading = false;   // with the loader thread (reported as active)
     int status = kQueued;
     int error = SP3MM_OK;
     sp3mm_hierarchy* h = nullptr;
@@ -83,6 +91,15 @@ struct sp3mm_server {
     std::deque<int64_t> queue;
     std::vector<int64_t> active;
     std::unordered_map<int64_t, Request> reqs;
+    // Loader thread: admitted requests are uploaded on its own context.
+    sp3mm_ctx* loader_ctx = nullptr;
+    std::thread loader;
+    std::mutex mu;
+    std::condition_variable wake, done;
+    std::deque<Request*> to_load;    // guarded by mu
+    std::vector<Request*> loaded;    // guarded by mu
+    int in_loader = 0;               // guarded by mu
+    bool stop = false;               // guarded by mu
     // Statistics.
     std::vector<double> latency;
     long long products = 0, steps = 0, admitted = 0, deferred = 0;
@@ -90,20 +107,31 @@ struct sp3mm_server {
     double busy = 0;
 
     ~sp3mm_server() {
+        {
+            std::lock_guard<std::mutex> lk(mu);
+            stop = true;
+        }
+        wake.notify_all();
+        if (loader.joinable()) loader.join();
         for (auto& kv : reqs)
             if (kv.second.h && kv.second.status != kTaken) sp3mm_hierarchy_free(ctx, kv.second.h);
+        if (loader_ctx) sp3mm_ctx_destroy(loader_ctx);
     }
 };
 
 namespace {
 
+// Upload a request's operator on the loader context (the call returns once
+// the copy and its validation are complete) and wrap it in a hierarchy.
+// The operator is freed on the server's context, after the work that uses it.
 int admit(sp3mm_server* s, Request& r) {
     sp3mm_ctx* ctx = s->ctx;
     auto A0 = std::shared_ptr<sp3mm_dcsr>(new sp3mm_dcsr{}, [ctx](sp3mm_dcsr* m) {
         sp3mm_dcsr_free(ctx, m);
         delete m;
     });
-    TRY(sp3mm_dcsr_upload_arrays(ctx, r.M, r.M, r.nnz, r.rp, r.ci, r.v, SP3MM_F64, A0.get()));
+    TRY(sp3mm_dcsr_upload_arrays(s->loader_ctx, r.M, r.M, r.nnz, r.rp, r.ci, r.v, SP3MM_F64,
+                                 A0.get()));
     auto* h = new sp3mm_hierarchy();
     h->ndim = r.ndim;
     h->block = r.block;
@@ -120,6 +148,27 @@ int admit(sp3mm_server* s, Request& r) {
     h->keep.push_back(A0);
     r.h = h;
     return SP3MM_OK;
+}
+
+void loader_main(sp3mm_server* s) {
+    cudaSetDevice(s->ctx->device);
+    for (;;) {
+        Request* r = nullptr;
+        {
+            std::unique_lock<std::mutex> lk(s->mu);
+            s->wake.wait(lk, [&] { return s->stop || !s->to_load.empty(); });
+            if (s->stop) return;
+            r = s->to_load.front();
+            s->to_load.pop_front();
+        }
+        r->error = admit(s, *r);
+        {
+            std::lock_guard<std::mutex> lk(s->mu);
+            s->loaded.push_back(r);
+            --s->in_loader;
+        }
+        s->done.notify_all();
+    }
 }
 
 void finish(sp3mm_server* s, Request& r, int status, double t) {
@@ -147,6 +196,12 @@ int sp3mm_server_create(sp3mm_ctx* ctx, int max_active, double mem_fraction,
     s->mem_fraction = mem_fraction;
     s->budget = static_cast<size_t>(mem_fraction * static_cast<double>(free_hbm(ctx)));
     s->t0 = std::chrono::steady_clock::now();
+    const int rc = sp3mm_ctx_create(ctx->device, &s->loader_ctx);
+    if (rc != SP3MM_OK) {
+        delete s;
+        return set_error(ctx, rc, "server: loader context creation failed");
+    }
+    s->loader = std::thread(loader_main, s);
     *out = s;
     return SP3MM_OK;
 }
@@ -193,8 +248,15 @@ int sp3mm_server_step(sp3mm_server* s, int* pending) {
     if (!s) return SP3MM_EINVAL;
     sp3mm_ctx* ctx = s->ctx;
     const double t_begin = now_s(s->t0);
-    // 1. Admission, first come first served.
-    while (!s->queue.empty() && static_cast<int>(s->active.size()) < s->max_active) {
+    int in_loader = 0;
+    {
+        std::lock_guard<std::mutex> lk(s->mu);
+        in_loader = s->in_loader + static_cast<int>(s->loaded.size());
+    }
+    // 1. Admission, first come first served; uploads go to the loader.
+    std::vector<Request*> handed;
+    while (!s->queue.empty() &&
+           static_cast<int>(s->active.size()) + in_loader < s->max_active) {
         Request& r = s->reqs[s->queue.front()];
         if (r.est > s->budget) {   // can never fit: refuse instead of blocking
             r.error = SP3MM_ENOMEM;
@@ -207,25 +269,47 @@ int sp3mm_server_step(sp3mm_server* s, int* pending) {
             break;
         }
         s->queue.pop_front();
-        const int rc = admit(s, r);
-        if (rc != SP3MM_OK) {
-            r.error = rc;
-            r.status = kFailed;
-            r.t_done = now_s(s->t0);
-            continue;
-        }
         r.status = kActive;
+        r.loading = true;
         r.t_admit = now_s(s->t0);
-        r.rp = nullptr;
-        r.ci = nullptr;
-        r.v = nullptr;
         s->reserved += r.est;
         r.held = r.est;
-        s->active.push_back(r.id);
+        handed.push_back(&r);
+        ++in_loader;
         ++s->admitted;
     }
+    if (!handed.empty()) {
+        {
+            std::lock_guard<std::mutex> lk(s->mu);
+            for (Request* r : handed) s->to_load.push_back(r);
+            s->in_loader += static_cast<int>(handed.size());
+        }
+        s->wake.notify_all();
+    }
+    // 2. Requests the loader has finished join; wait only when nothing
+    //    else could run.
+    {
+        std::unique_lock<std::mutex> lk(s->mu);
+        if (s->active.empty() && s->loaded.empty() && s->in_loader > 0)
+            s->done.wait(lk, [&] { return !s->loaded.empty(); });
+        for (Request* r : s->loaded) {
+            r->loading = false;
+            r->rp = nullptr;
+            r->ci = nullptr;
+            r->v = nullptr;
+            if (r->error != SP3MM_OK) {
+                if (r->h) sp3mm_hierarchy_free(ctx, r->h);
+                r->h = nullptr;
+                finish(s, *r, kFailed, now_s(s->t0));
+            } else {
+                s->active.push_back(r->id);
+            }
+        }
+        s->loaded.clear();
+        in_loader = s->in_loader;
+    }
     s->peak_active = std::max(s->peak_active, static_cast<int>(s->active.size()));
-    // 2. One level for every admitted hierarchy.
+    // 3. One level for every joined hierarchy.
     std::vector<sp3mm_hierarchy*> hs;
     for (int64_t id : s->active) hs.push_back(s->reqs[id].h);
     if (!hs.empty()) {
@@ -245,7 +329,7 @@ int sp3mm_server_step(sp3mm_server* s, int* pending) {
         }
         ++s->steps;
     }
-    // 3. Retire complete hierarchies.
+    // 4. Retire complete hierarchies.
     const double t = now_s(s->t0);
     std::vector<int64_t> still;
     for (int64_t id : s->active) {
@@ -256,7 +340,8 @@ int sp3mm_server_step(sp3mm_server* s, int* pending) {
     }
     s->active.swap(still);
     s->busy += t - t_begin;
-    if (pending) *pending = static_cast<int>(s->queue.size() + s->active.size());
+    if (pending)
+        *pending = static_cast<int>(s->queue.size() + s->active.size()) + in_loader;
     return SP3MM_OK;
 }
 
