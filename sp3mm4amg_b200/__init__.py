@@ -81,14 +81,15 @@ def spmm(A: CSR, B: CSR, name: str = "spmmRowByRow_SymbNum_", off_f: int = 0,
 
 
 def sp3mm(R: CSR, A: CSR, P: CSR, name: str = "sp3mmRowByRowPair_", spmm: str | None = None,
-          off_f: int = 0, cfg: CONFIG | None = None) -> CSR:
+          off_f: int = 0, cfg: CONFIG | None = None, pinned: bool = False) -> CSR:
     """C = R*A*P through the reference-named triple-product entry point.
 
     ``spmm`` names this library's SpMM entry point handed to the driver
-    (``None`` passes NULL, the driver's default).
+    (``None`` passes NULL, the driver's default); ``pinned`` passes the
+    inputs in page-locked host memory.
     """
     lib = capi.load()
-    r, a, p = HostSpMat(R, off_f), HostSpMat(A, off_f), HostSpMat(P, off_f)
+    r, a, p = (HostSpMat(m, off_f, pinned=pinned) for m in (R, A, P))
     c = _config(cfg)
     fp = None
     if spmm is not None:

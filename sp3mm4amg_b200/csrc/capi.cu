@@ -8,6 +8,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <atomic>
 #include <chrono>
 #include <cstdarg>
 #include <cstdio>
@@ -15,6 +16,7 @@
 #include <cstring>
 #include <mutex>
 #include <string>
+#include <thread>
 #include <vector>
 
 #include "context.cuh"
@@ -495,7 +497,45 @@ int rap_impl(sp3mm_ctx* ctx, const sp3mm_dcsr& R, const sp3mm_dcsr& A, const sp3
 }
 
 // Upload from 64-bit host arrays with index offset `off`.
-int upload_u64(sp3mm_ctx* ctx, long long M, long long N, long long nnz, const uint64_t* irp,
+// Pinned staging of at least `bytes` (at most kHostStageMax) on the context.
+constexpr size_t kHostStageMax = size_t(256) << 20;
+
+int host_stage(sp3mm_ctx* ctx, size_t bytes, void** out) {
+    bytes = std::min(std::max<size_t>(bytes, size_t(1) << 20), kHostStageMax);
+    if (ctx->host_stage_bytes < bytes) {
+        if (ctx->host_stage) cudaFreeHost(ctx->host_stage);
+        ctx->host_stage = nullptr;
+        ctx->host_stage_bytes = 0;
+        CK(ctx, cudaHostAlloc(&ctx->host_stage, bytes, cudaHostAllocDefault));
+        ctx->host_stage_bytes = bytes;
+    }
+    *out = ctx->host_stage;
+    return SP3MM_OK;
+}
+
+// f(lo, hi) over [0, n) on up to 16 host threads (one for small n).
+template <typename F>
+void host_parallel(long long n, F&& f) {
+    const long long per = 1 << 20;
+    int t = static_cast<int>(std::min<long long>((n + per - 1) / per, 16));
+    const unsigned hw = std::thread::hardware_concurrency();
+    if (hw) t = std::min<int>(t, static_cast<int>(hw));
+    if (t <= 1) {
+        f(0LL, n);
+        return;
+    }
+    std::vector<std::thread> th;
+    const long long chunk = (n + t - 1) / t;
+    for (int k = 0; k < t; ++k) {
+        const long long lo = k * chunk, hi = std::min(n, lo + chunk);
+        if (lo < hi) th.emplace_back([&f, lo, hi] { f(lo, hi); });
+    }
+    for (auto& x : th) x.join();
+}
+
+// Pinned host sources: copy the 64-bit arrays as they are into a device
+// stage and narrow / validate them there.
+int upload_u64_direct(sp3mm_ctx* ctx, long long M, long long N, long long nnz, const uint64_t* irp,
                const uint64_t* ja, const double* as, int off, int vt, sp3mm_dcsr* out) {
     if (M < 0 || N < 0 || nnz < 0) return set_error(ctx, SP3MM_EINVAL, "negative sizes");
     if (M >= INT32_MAX || N >= INT32_MAX || nnz >= INT32_MAX)
@@ -539,27 +579,177 @@ int upload_u64(sp3mm_ctx* ctx, long long M, long long N, long long nnz, const ui
     return finish_matrix(out, rp, ci, v);
 }
 
+bool host_pinned(const void* p) {
+    if (!p) return true;
+    cudaPointerAttributes a;
+    if (cudaPointerGetAttributes(&a, p) != cudaSuccess) {
+        cudaGetLastError();
+        return false;
+    }
+    return a.type == cudaMemoryTypeHost;
+}
+
+// Pageable host sources: host threads narrow the indices to int32 -- validating the row pointers completely
+// (start 0, end nnz, monotone) and the column range -- into pinned staging,
+// two halves used in turn so that filling one overlaps the copy of the
+// other; the device then checks the columns' order and records the longest
+// row.
+int upload_u64_staged(sp3mm_ctx* ctx, long long M, long long N, long long nnz,
+                      const uint64_t* irp,
+               const uint64_t* ja, const double* as, int off, int vt, sp3mm_dcsr* out) {
+    if (M < 0 || N < 0 || nnz < 0) return set_error(ctx, SP3MM_EINVAL, "negative sizes");
+    if (M >= INT32_MAX || N >= INT32_MAX || nnz >= INT32_MAX)
+        return set_error(ctx, SP3MM_ELIMIT,
+                         "matrix %lldx%lld with %lld nonzeros exceeds the 32-bit device limits",
+                         M, N, nnz);
+    if (!irp || (nnz > 0 && (!ja || !as)))
+        return set_error(ctx, SP3MM_EINVAL, "NULL CSR arrays");
+    const cudaStream_t st = ctx->stream;
+    DevBuf rp, ci, v, maxrow;
+    TRY(rp.alloc(ctx, sizeof(int) * (M + 1)));
+    TRY(ci.alloc(ctx, sizeof(int) * nnz));
+    TRY(v.alloc(ctx, vbytes(vt) * nnz));
+    TRY(maxrow.alloc(ctx, sizeof(int)));
+    CK(ctx, cudaMemsetAsync(maxrow.p, 0, sizeof(int), st));
+    const size_t biggest =
+        std::max<size_t>(sizeof(int) * (M + 1), std::max<size_t>(sizeof(double), 4) * nnz);
+    void* stage = nullptr;
+    TRY(host_stage(ctx, 2 * std::min(biggest, kHostStageMax / 2), &stage));
+    const size_t half = ctx->host_stage_bytes / 2 / 256 * 256;
+    std::atomic<bool> bad(false);
+    int h = 0;
+    // Fill and copy one array in chunks through the staging halves: half h
+    // is filled while the other half's copy is in flight; the stream is
+    // synchronised (so that copy, and the other half, are done) before the
+    // copy of half h is issued, so a half is never refilled while copied.
+    auto push = [&](void* dst, size_t esz, long long n, auto&& fill) -> int {
+        const long long per = static_cast<long long>(half / esz);
+        for (long long b = 0; b < n; b += per) {
+            const long long k = std::min(per, n - b);
+            unsigned char* buf = static_cast<unsigned char*>(stage) + h * half;
+            host_parallel(k, [&](long long lo, long long hi) { fill(b, lo, hi, buf); });
+            CK(ctx, cudaStreamSynchronize(st));
+            CK(ctx, cudaMemcpyAsync(static_cast<unsigned char*>(dst) + b * esz, buf, esz * k,
+                                    cudaMemcpyHostToDevice, st));
+            h ^= 1;
+        }
+        return SP3MM_OK;
+    };
+    TRY(push(rp.p, sizeof(int), M + 1, [&](long long b, long long lo, long long hi, void* buf) {
+        int* o = static_cast<int*>(buf);
+        bool ok = true;
+        for (long long i = lo; i < hi; ++i) {
+            const long long g = b + i;
+            const long long x = static_cast<long long>(irp[g]) - off;
+            ok &= x >= 0 && x <= nnz;
+            if (g == 0) ok &= x == 0;
+            if (g == M) ok &= x == nnz;
+            if (g > 0) ok &= static_cast<long long>(irp[g - 1]) - off <= x;
+            o[i] = static_cast<int>(x);
+        }
+        if (!ok) bad = true;
+    }));
+    if (nnz > 0 && !bad) {
+        TRY(push(ci.p, sizeof(int), nnz, [&](long long b, long long lo, long long hi, void* buf) {
+            int* o = static_cast<int*>(buf);
+            bool ok = true;
+            for (long long i = lo; i < hi; ++i) {
+                const long long c = static_cast<long long>(ja[b + i]) - off;
+                ok &= c >= 0 && c < N;
+                o[i] = static_cast<int>(c);
+            }
+            if (!ok) bad = true;
+        }));
+        if (vt == SP3MM_F64) {
+            TRY(push(v.p, sizeof(double), nnz,
+                     [&](long long b, long long lo, long long hi, void* buf) {
+                         std::memcpy(static_cast<double*>(buf) + lo, as + b + lo,
+                                     sizeof(double) * (hi - lo));
+                     }));
+        } else {
+            TRY(push(v.p, sizeof(float), nnz,
+                     [&](long long b, long long lo, long long hi, void* buf) {
+                         float* o = static_cast<float*>(buf);
+                         for (long long i = lo; i < hi; ++i) o[i] = static_cast<float>(as[b + i]);
+                     }));
+        }
+    }
+    if (bad) {
+        CK(ctx, cudaStreamSynchronize(st));
+        return set_error(ctx, SP3MM_EINVAL,
+                         "malformed CSR input (row pointers or column range)");
+    }
+    launch_validate_i32(static_cast<int>(M), static_cast<int>(N), rp.as<int>(), ci.as<int>(),
+                        maxrow.as<int>(), ctx->d_err, st);
+    CK(ctx, cudaGetLastError());
+    int mr = 0;
+    CK(ctx, cudaMemcpyAsync(&mr, maxrow.p, sizeof(int), cudaMemcpyDeviceToHost, st));
+    TRY(check_device_err(ctx));
+    out->M = static_cast<int>(M);
+    out->N = static_cast<int>(N);
+    out->nnz = nnz;
+    out->val_type = vt;
+    out->max_row = mr;
+    return finish_matrix(out, rp, ci, v);
+}
+
+// Host 64-bit CSR (indices shifted by off) -> device CSR, by the faster route
+// for the sources' memory (validated either way).
+int upload_u64(sp3mm_ctx* ctx, long long M, long long N, long long nnz, const uint64_t* irp,
+               const uint64_t* ja, const double* as, int off, int vt, sp3mm_dcsr* out) {
+    if (host_pinned(irp) && host_pinned(ja) && host_pinned(as))
+        return upload_u64_direct(ctx, M, N, nnz, irp, ja, as, off, vt, out);
+    return upload_u64_staged(ctx, M, N, nnz, irp, ja, as, off, vt, out);
+}
+
 // Copy a device CSR into malloc'd host arrays, indices shifted by `off`.
+// Device CSR -> host 64-bit arrays (indices shifted by off, values FP64).
+// The compact device arrays go through pinned staging (full-speed copies);
+// widening and the copy into the caller's (possibly never-touched, pageable)
+// arrays run on host threads.
 int download_u64(sp3mm_ctx* ctx, const sp3mm_dcsr& m, int off, uint64_t* irp, uint64_t* ja,
                  double* as) {
     const cudaStream_t st = ctx->stream;
-    DevBuf stage;
-    TRY(stage.alloc(ctx, sizeof(uint64_t) * std::max<long long>(m.M + 1, m.nnz)));
-    launch_widen(m.M + 1, m.row_ptr, off, stage.as<unsigned long long>(), st);
-    CK(ctx, cudaMemcpyAsync(irp, stage.p, sizeof(uint64_t) * (m.M + 1), cudaMemcpyDeviceToHost, st));
-    if (m.nnz > 0) {
-        CK(ctx, cudaStreamSynchronize(st));
-        launch_widen(m.nnz, m.col, off, stage.as<unsigned long long>(), st);
-        CK(ctx, cudaMemcpyAsync(ja, stage.p, sizeof(uint64_t) * m.nnz, cudaMemcpyDeviceToHost, st));
-        if (m.val_type == SP3MM_F64) {
-            CK(ctx, cudaMemcpyAsync(as, m.val, sizeof(double) * m.nnz, cudaMemcpyDeviceToHost, st));
-        } else {
+    void* stage = nullptr;
+    const size_t want = std::max<size_t>(sizeof(int) * (static_cast<size_t>(m.M) + 1),
+                                         sizeof(double) * static_cast<size_t>(m.nnz));
+    TRY(host_stage(ctx, want, &stage));
+    const size_t cap = ctx->host_stage_bytes;
+    // One array in chunks that fit the staging: copy, then widen on the host.
+    auto pass = [&](const void* src, size_t esz, long long n, auto&& widen) -> int {
+        const long long per = static_cast<long long>(cap / esz);
+        for (long long b = 0; b < n; b += per) {
+            const long long k = std::min(per, n - b);
+            CK(ctx, cudaMemcpyAsync(stage, static_cast<const unsigned char*>(src) + b * esz,
+                                    esz * k, cudaMemcpyDeviceToHost, st));
             CK(ctx, cudaStreamSynchronize(st));
-            launch_convert_values(m.nnz, m.val, m.val_type, stage.p, SP3MM_F64, st);
-            CK(ctx, cudaMemcpyAsync(as, stage.p, sizeof(double) * m.nnz, cudaMemcpyDeviceToHost, st));
+            host_parallel(k, [&](long long lo, long long hi) { widen(b, lo, hi); });
+        }
+        return SP3MM_OK;
+    };
+    const int* srp = static_cast<const int*>(stage);
+    TRY(pass(m.row_ptr, sizeof(int), static_cast<long long>(m.M) + 1,
+             [&](long long b, long long lo, long long hi) {
+                 for (long long i = lo; i < hi; ++i)
+                     irp[b + i] = static_cast<uint64_t>(srp[i]) + static_cast<uint64_t>(off);
+             }));
+    if (m.nnz > 0) {
+        TRY(pass(m.col, sizeof(int), m.nnz, [&](long long b, long long lo, long long hi) {
+            for (long long i = lo; i < hi; ++i)
+                ja[b + i] = static_cast<uint64_t>(srp[i]) + static_cast<uint64_t>(off);
+        }));
+        if (m.val_type == SP3MM_F64) {
+            const double* sv = static_cast<const double*>(stage);
+            TRY(pass(m.val, sizeof(double), m.nnz, [&](long long b, long long lo, long long hi) {
+                std::memcpy(as + b + lo, sv + lo, sizeof(double) * (hi - lo));
+            }));
+        } else {
+            const float* sf = static_cast<const float*>(stage);
+            TRY(pass(m.val, sizeof(float), m.nnz, [&](long long b, long long lo, long long hi) {
+                for (long long i = lo; i < hi; ++i) as[b + i] = static_cast<double>(sf[i]);
+            }));
         }
     }
-    CK(ctx, cudaStreamSynchronize(st));
     return SP3MM_OK;
 }
 
@@ -829,6 +1019,7 @@ int sp3mm_ctx_destroy(sp3mm_ctx* ctx) {
     if (ctx->ev0) cudaEventDestroy(ctx->ev0);
     if (ctx->ev1) cudaEventDestroy(ctx->ev1);
     if (ctx->own_stream) cudaStreamDestroy(ctx->own_stream);
+    if (ctx->host_stage) cudaFreeHost(ctx->host_stage);
     if (tl_ctx == ctx) tl_ctx = nullptr;
     delete ctx;
     return SP3MM_OK;

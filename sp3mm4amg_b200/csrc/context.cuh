@@ -37,6 +37,10 @@ struct sp3mm_ctx {
     size_t free_at_check = 0;
     uint64_t reserved_at_check = 0;
     double free_checked_s = -1.0;
+    // Pinned host staging for downloads (grown on demand, freed with the
+    // context).
+    void* host_stage = nullptr;
+    size_t host_stage_bytes = 0;
 };
 
 namespace sp3mm {

@@ -238,6 +238,9 @@ def test_malformed_inputs_return_null():
             S.spmm(bad, good, "spmmRowByRow_")
         with pytest.raises(S.Sp3mmError):
             S.sp3mm(good, bad, good, "sp3mmRowByRowMerged_")
+        # Page-locked inputs take the other upload route; same checks.
+        with pytest.raises(S.Sp3mmError):
+            S.sp3mm(good, bad, good, "sp3mmRowByRowMerged_", pinned=True)
     # Dimension mismatch.
     with pytest.raises(S.Sp3mmError):
         S.spmm(good, pb.random_sparse(7, 3, 0.5, seed=5), "spmmRowByRow_")
@@ -274,3 +277,16 @@ def test_reference_fixture_on_gpu_if_present(reference_fixture, orc):
                      ("sp3mmRowByRowPair_", "spmmRowByRow_SymbNum_")):
         C = S.sp3mm(R, AC, P, name, spmm=sp)
         assert O.compare(C, ACN, rtol=RTOL)["ok"]
+
+
+@pytest.mark.parametrize("off", [0, 1])
+def test_pinned_and_pageable_inputs_agree(golden, off):
+    """Inputs in page-locked host memory are copied as they are and narrowed
+    on the device; pageable inputs are narrowed by host threads into pinned
+    staging.  Both routes give the reference's result bit for bit."""
+    g = golden["poisson2d_64_agg2"]
+    for name, want in (("sp3mmRowByRowMerged_", g["direct"]), ("sp3mmRowByRowPair_", g["pair"])):
+        a = S.sp3mm(g["R"], g["A"], g["P"], name, off_f=off, pinned=True)
+        b = S.sp3mm(g["R"], g["A"], g["P"], name, off_f=off, pinned=False)
+        assert_same(a, want, what=f"{name} pinned")
+        assert_same(b, want, what=f"{name} pageable")
