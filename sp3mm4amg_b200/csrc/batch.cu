@@ -40,10 +40,12 @@ namespace {
 // need[g] = distinct-key bound of the first table of global row g (the
 // product count of its row of X*Y, at most Y.N); row_item[g] = its product.
 // *total += the output-size bound of every row (SpMM: need; direct:
-// min(R*A products times Z's longest row, Z.N)).
+// min(R*A products times Z's longest row, Z.N)).  need_opt[g] = the
+// optimistic first-table size: need >> d1, or need itself when the row's
+// products reach Y's column count (such rows are dense).
 __global__ void k_batch_bounds(const BItem* __restrict__ items, const long long* __restrict__ bases,
-                               int n, long long rows, int* need, int* row_item,
-                               unsigned long long* total) {
+                               int n, long long rows, int d1, int* need, int* need_opt,
+                               int* row_item, unsigned long long* total) {
     unsigned long long ub = 0;
     for (long long g = blockIdx.x * (long long)blockDim.x + threadIdx.x; g < rows;
          g += (long long)gridDim.x * blockDim.x) {
@@ -63,7 +65,10 @@ __global__ void k_batch_bounds(const BItem* __restrict__ items, const long long*
             const int k = __ldg(xci + t);
             u += __ldg(yrp + k + 1) - __ldg(yrp + k);
         }
-        need[g] = static_cast<int>(u < I->Y.N ? u : I->Y.N);
+        const int nd = static_cast<int>(u < I->Y.N ? u : I->Y.N);
+        need[g] = nd;
+        // (a positive bound stays positive: binning skips rows of need 0)
+        need_opt[g] = nd == 0 ? 0 : (u >= I->Y.N ? nd : max(1, nd >> d1));
         row_item[g] = lo;
         if (I->kind == kBatchDirect) {
             const long long zm = I->zmax >= 0 ? I->zmax : I->Z.N;
@@ -157,8 +162,11 @@ struct sp3mm_batch {
     bool auto_split = true;
     std::vector<int> level_slack = std::vector<int>(kLevels, -1);   // per top level; -1: slack
     int warps_cap = 8;
+    // Tiers whose per-warp tables exceed this go to global memory, where
+    // more warps per SM run (one or two warps per SM hide no latency).
+    size_t smem_tier_max = 110 * 1024;
     // Device state.
-    DevBuf d_items, d_bases, d_row_item, d_need, d_cnt1, d_cnt2, d_crp;
+    DevBuf d_items, d_bases, d_row_item, d_need, d_need_opt, d_cnt1, d_cnt2, d_crp;
     DevBuf d_ci, d_v, d_rp, d_rp_off, d_counters;
     DevBuf num_gtab;
     Bins nbins;
@@ -243,7 +251,7 @@ int make_tiers(sp3mm_batch* b, const Bins& bins, int mode, int extra, int tv, in
         const int top = std::min(t.hi + ex, 30 - 5);
         t.scap = 32 << top;
         const size_t bytes = batch_row_region_bytes(num, t.scap);
-        if (bytes > ctx->smem_optin) {
+        if (bytes > std::min(ctx->smem_optin, b->smem_tier_max)) {
             // Global-memory tier: extend it (levels are visited ascending).
             if (gt.hi < 0) {
                 gt.lo = t.lo;
@@ -489,6 +497,7 @@ int batch_plan(sp3mm_batch* b) {
                             cudaMemcpyHostToDevice, st));
     TRY(b->d_row_item.alloc(ctx, sizeof(int) * R1));
     TRY(b->d_need.alloc(ctx, sizeof(int) * R1));
+    TRY(b->d_need_opt.alloc(ctx, sizeof(int) * R1));
     TRY(b->d_cnt1.alloc(ctx, sizeof(int) * R1));
     TRY(b->d_cnt2.alloc(ctx, sizeof(int) * R1));
     TRY(b->d_crp.alloc(ctx, sizeof(int) * R1));
@@ -502,19 +511,21 @@ int batch_plan(sp3mm_batch* b) {
     if (rows > 0) {
         prof(ctx, "batch.bounds", [&] {
             k_batch_bounds<<<grid_for_rows(rows), 256, 0, st>>>(
-                b->d_items.as<BItem>(), b->d_bases.as<long long>(), n, rows, b->d_need.as<int>(),
-                b->d_row_item.as<int>(), &dc->total);
+                b->d_items.as<BItem>(), b->d_bases.as<long long>(), n, rows, b->d1,
+                b->d_need.as<int>(), b->d_need_opt.as<int>(), b->d_row_item.as<int>(),
+                &dc->total);
         });
         note_launch();
         CK(ctx, cudaGetLastError());
     }
     Bins sb;
-    TRY(bin_rows(ctx, M, b->d_need.as<int>(), b->d1, 32, dc, nullptr, sb));
+    TRY(bin_rows(ctx, M, b->d_need_opt.as<int>(), 0, 32, dc, nullptr, sb));
 
     BatchRowParams p{};
     p.d1 = b->d1;
     p.d2 = b->d2;
     p.need = b->d_need.as<int>();
+    p.need_opt = b->d_need_opt.as<int>();
     p.cnt1 = b->d_cnt1.as<int>();
     p.cnt2 = b->d_cnt2.as<int>();
     p.err = ctx->d_err;
@@ -660,6 +671,7 @@ void batch_trim(sp3mm_batch* b) {
     b->d_bases.release();
     b->d_row_item.release();
     b->d_need.release();
+    b->d_need_opt.release();
     b->d_cnt1.release();
     b->d_cnt2.release();
     b->d_crp.release();

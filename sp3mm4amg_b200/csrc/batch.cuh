@@ -29,6 +29,7 @@ struct BatchRowParams {
     int slack;              // numeric: tables 2^slack times the exact size
     int reverse;            // walk the list from its end (largest rows first)
     const int* need;        // symbolic: first-table bound per global row
+    const int* need_opt;    // symbolic: optimistic first-table size (null: need >> d1)
     int* cnt1;              // direct R*A distinct count (out: symbolic, in: numeric)
     int* cnt2;              // C row length (out: symbolic, in: numeric)
     const int* c_rp;        // numeric: global row pointers into c_ci / c_v

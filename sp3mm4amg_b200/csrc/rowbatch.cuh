@@ -151,8 +151,9 @@ __global__ void __launch_bounds__(256, 4)
             long long need2 = 0;
             if constexpr (MODE != kNumExact) {
                 const int need1 = __ldg(p.need + g);
+                const int opt1 = p.need_opt ? __ldg(p.need_opt + g) : need1 >> p.d1;
                 S1 = batch_accumulate<NUM>(L1, xlen, Y.rp, Y.ci, static_cast<const TV*>(Y.v),
-                                           keys1, vals1, ord1, batch_slots(need1 >> p.d1),
+                                           keys1, vals1, ord1, batch_slots(opt1),
                                            batch_slots(need1), scap, sk, sv, n1);
                 if (S1 == 0) {
                     batch_retry(p, g, need1);
@@ -214,8 +215,9 @@ __global__ void __launch_bounds__(256, 4)
         } else {
             if constexpr (MODE != kNumExact) {
                 const int need1 = __ldg(p.need + g);
+                const int opt1 = p.need_opt ? __ldg(p.need_opt + g) : need1 >> p.d1;
                 S1 = batch_accumulate<NUM>(L1, xlen, Y.rp, Y.ci, static_cast<const TV*>(Y.v),
-                                           keys1, vals1, ord1, batch_slots(need1 >> p.d1),
+                                           keys1, vals1, ord1, batch_slots(opt1),
                                            batch_slots(need1), scap, sk, sv, n1);
                 if (S1 == 0) {
                     batch_retry(p, g, need1);
