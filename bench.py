@@ -354,24 +354,7 @@ def run_library(torch, prob, steps=5):
         return {"library": "cuSPARSE SpGEMM via torch sparse CSR", "unavailable": repr(e)[:200]}
 
 
-def _level_errors(h32, h64):
-    """Per level: max relative error of FP32-stored values against FP64
-    (over entries with |ref| > 0) and max error normalised by max |ref|."""
-    out = []
-    for lvl in range(len(h64)):
-        a = h32.level(lvl)[0].download()
-        b = h64.level(lvl)[0].download()
-        if not np.array_equal(a.indices, b.indices) or not np.array_equal(a.indptr, b.indptr):
-            raise RuntimeError("FP32 and FP64 hierarchies differ in pattern")
-        ref = np.abs(b.data)
-        nz = ref > 0
-        rel = float(np.max(np.abs(a.data[nz] - b.data[nz]) / ref[nz])) if nz.any() else 0.0
-        norm = float(np.max(np.abs(a.data - b.data)) / ref.max()) if ref.size else 0.0
-        out.append((rel, norm))
-    return out
-
-
-def run_served(S, ctx, count, rate, seed=4, err_sample=24):
+def run_served(S, ctx, count, rate, seed=4):
     """A Poisson stream of hierarchy-setup requests (90% of config-3 sizes,
     10% 3D 64^3..128^3) served by continuous batching versus one request at
     a time, at `rate` requests/s and saturated (all arriving at once)."""
@@ -384,15 +367,30 @@ def run_served(S, ctx, count, rate, seed=4, err_sample=24):
     res = {"workload": f"{count} requests (seed {seed}): 90% 2D/3D n log-uniform 1e3..2e5, "
                        f"10% 3D side 64..128; hierarchy to n < 1000",
            "rate_per_s": rate}
+    kept = {}
     for name, cvt in (("fp64", S.F64), ("fp32_coarse", S.F32)):
         st, _ = serving.serve_batched(ctx, specs, arrivals, coarse_val_type=cvt, operators=ops)
-        sat, _ = serving.serve_batched(ctx, specs, np.zeros(count), coarse_val_type=cvt,
-                                       operators=ops)
+        sat, kept[name] = serving.serve_batched(ctx, specs, np.zeros(count), coarse_val_type=cvt,
+                                                operators=ops, keep=True)
         res[name] = {"p50_s": st["p50_s"], "p99_s": st["p99_s"],
                      "products_per_s": st["products_per_s"], "products": st["products"],
                      "peak_active": st["peak_active"], "failed": st["failed"],
                      "saturated_products_per_s": sat["products_per_s"],
                      "saturated_p99_s": sat["p99_s"]}
+    # FP32 coarse storage: every request's every level against its FP64
+    # hierarchy (which equals the oracle chain bit for bit), on the device.
+    per_level = {}
+    for a, b in zip(kept["fp32_coarse"], kept["fp64"]):
+        for lvl, (rel, norm) in enumerate(serving.level_errors(a, b)):
+            per_level.setdefault(lvl, []).append((rel, norm))
+        a.free()
+        b.free()
+    res["fp32_level_max_rel_err"] = {str(l): max(r for r, _ in v) for l, v in sorted(per_level.items())}
+    res["fp32_level_median_rel_err"] = {str(l): float(np.median([r for r, _ in v]))
+                                        for l, v in sorted(per_level.items())}
+    res["fp32_level_max_err_over_max"] = {str(l): max(n for _, n in v)
+                                          for l, v in sorted(per_level.items())}
+    res["fp32_error_coverage"] = f"all {count} requests, every level (device comparison)"
     plain = serving.serve_plain(ctx, specs, arrivals, operators=ops)
     plain_sat = serving.serve_plain(ctx, specs, np.zeros(count), operators=ops)
     res["plain_fp64"] = {"p50_s": plain["p50_s"], "p99_s": plain["p99_s"],
@@ -400,23 +398,6 @@ def run_served(S, ctx, count, rate, seed=4, err_sample=24):
                          "saturated_products_per_s": plain_sat["products_per_s"]}
     res["saturated_speedup_fp64"] = (res["fp64"]["saturated_products_per_s"] /
                                      plain_sat["products_per_s"])
-    # FP32 coarse storage: per-level error against the FP64 hierarchies
-    # (which equal the oracle chain bit for bit) on a request sample.
-    k = min(err_sample, count)
-    _, h64 = serving.serve_batched(ctx, specs[:k], np.zeros(k), S.F64, keep=True,
-                                   operators=ops[:k])
-    _, h32 = serving.serve_batched(ctx, specs[:k], np.zeros(k), S.F32, keep=True,
-                                   operators=ops[:k])
-    per_level = {}
-    for a, b in zip(h32, h64):
-        for lvl, (rel, norm) in enumerate(_level_errors(a, b)):
-            r0, n0 = per_level.get(lvl, (0.0, 0.0))
-            per_level[lvl] = (max(r0, rel), max(n0, norm))
-        a.free()
-        b.free()
-    res["fp32_level_max_rel_err"] = {str(lvl): v[0] for lvl, v in sorted(per_level.items())}
-    res["fp32_level_max_err_over_max"] = {str(lvl): v[1] for lvl, v in sorted(per_level.items())}
-    res["fp32_error_sample"] = f"first {k} requests, every level"
     return res
 
 

@@ -7,7 +7,7 @@ import time
 
 import numpy as np
 
-from . import F64, Context, Server
+from . import F32, F64, Context, Server
 from .problems import stencil_operator
 
 
@@ -73,3 +73,45 @@ def serve_plain(ctx: Context, specs, arrivals, coarse_val_type: int = F64,
     return {"completed": len(lat), "products": products, "p50_s": _pct(lat, 0.5),
             "p99_s": _pct(lat, 0.99), "makespan_s": makespan,
             "products_per_s": products / makespan if makespan > 0 else 0.0}
+
+
+def _device_view(ptr: int, n: int, typestr: str):
+    """A torch tensor over n elements of device memory at ptr (no copy)."""
+    import torch
+
+    class _Mem:
+        __cuda_array_interface__ = {"shape": (n,), "typestr": typestr, "data": (ptr, False),
+                                    "version": 3}
+    return torch.as_tensor(_Mem(), device="cuda")
+
+
+def level_errors(h32, h64):
+    """Per level of two hierarchies of the same request (FP32 coarse storage
+    and FP64): (max entrywise relative error over nonzero FP64 entries, max
+    error over max |FP64 value|), computed on the device.  Raises if the
+    patterns differ (they must not, in any mode)."""
+    import torch
+    out = []
+    if len(h32) != len(h64):
+        raise RuntimeError("hierarchies differ in depth")
+    for lvl in range(len(h64)):
+        a, b = h32.level(lvl)[0], h64.level(lvl)[0]
+        if a.shape != b.shape or a.nnz != b.nnz:
+            raise RuntimeError("hierarchies differ in shape or nonzeros")
+        n = a.nnz
+        if n == 0:
+            out.append((0.0, 0.0))
+            continue
+        rows = a.shape[0] + 1
+        for pa, pb, m in ((a.d.row_ptr, b.d.row_ptr, rows), (a.d.col, b.d.col, n)):
+            if not torch.equal(_device_view(pa, m, "<i4"), _device_view(pb, m, "<i4")):
+                raise RuntimeError("hierarchies differ in pattern")
+        va = _device_view(a.d.val, n, "<f4" if a.val_type == F32 else "<f8").double()
+        vb = _device_view(b.d.val, n, "<f4" if b.val_type == F32 else "<f8").double()
+        diff = (va - vb).abs()
+        ref = vb.abs()
+        nz = ref > 0
+        rel = float((diff[nz] / ref[nz]).max()) if bool(nz.any()) else 0.0
+        norm = float(diff.max() / ref.max()) if float(ref.max()) > 0 else 0.0
+        out.append((rel, norm))
+    return out

@@ -144,3 +144,20 @@ def test_serving_driver_reports_latency():
         assert 0 < st["p50_s"] <= st["p99_s"] and st["products"] > 0
         plain = serving.serve_plain(ctx, specs, arrivals)
         assert plain["products"] == st["products"]
+
+
+def test_serving_level_errors_on_device():
+    """FP32 coarse storage against FP64, compared on the device: level 0 is
+    FP64 in both modes (no error), coarse levels err at FP32 rounding scale,
+    patterns agree."""
+    specs = [(20, 20, 20), (64, 64)]
+    with S.Context() as ctx:
+        _, h64 = serving.serve_batched(ctx, specs, np.zeros(2), S.F64, keep=True, min_coarse=30)
+        _, h32 = serving.serve_batched(ctx, specs, np.zeros(2), S.F32, keep=True, min_coarse=30)
+        for a, b in zip(h32, h64):
+            errs = serving.level_errors(a, b)
+            assert errs[0] == (0.0, 0.0) and len(errs) >= 2
+            for rel, norm in errs[1:]:
+                assert 0.0 < norm <= 1e-5 and rel < 1e-2
+            a.free()
+            b.free()
