@@ -542,7 +542,7 @@ int batch_plan(sp3mm_batch* b) {
             in_nnz += I.X.nnz + I.Y.nnz + (I.kind == kBatchDirect ? I.Z.nnz : 0);
         unsigned long long cap = std::min<unsigned long long>(
             sb.total, std::max<unsigned long long>(1ULL << 20, 8ULL * in_nnz));
-        if (cap * eb > (size_t(1) << 30))
+        if (cap * eb > (size_t(1) << 30) && pool_idle_bytes(ctx) < cap * eb)
             cap = std::min<unsigned long long>(
                 cap, std::max<unsigned long long>(1ULL << 20, free_device_bytes(ctx) / 2 / eb));
         TRY(ub_ci.alloc(ctx, sizeof(int) * std::max<unsigned long long>(cap, 1)));

@@ -50,6 +50,19 @@ int check_dcsr(sp3mm_ctx* ctx, const sp3mm_dcsr* m, const char* what) {
     return SP3MM_OK;
 }
 
+size_t pool_idle_bytes(sp3mm_ctx* ctx) {
+    cudaMemPool_t pool;
+    uint64_t reserved = 0, used = 0;
+    if (cudaDeviceGetDefaultMemPool(&pool, ctx->device) != cudaSuccess ||
+        cudaMemPoolGetAttribute(pool, cudaMemPoolAttrReservedMemCurrent, &reserved) !=
+            cudaSuccess ||
+        cudaMemPoolGetAttribute(pool, cudaMemPoolAttrUsedMemCurrent, &used) != cudaSuccess) {
+        cudaGetLastError();
+        return 0;
+    }
+    return reserved > used ? static_cast<size_t>(reserved - used) : 0;
+}
+
 size_t free_device_bytes(sp3mm_ctx* ctx) {
     // The reading is refreshed every 100 ms; in between, the pool's own
     // growth is subtracted from it (other processes' use is seen at the
@@ -226,6 +239,18 @@ struct RowRunner {
     int run(const Bins& bins, RowParams base, int G, int d2, long long s1_max, long long s2_max,
             Counters* dcnt) {
         DevBuf retry;
+        TRY(run_levels(bins, base, G, d2, dcnt, retry));
+        int nretry = 0;
+        CK(ctx, cudaMemcpyAsync(&nretry, &dcnt->retry_count, sizeof(int), cudaMemcpyDeviceToHost,
+                                ctx->stream));
+        CK(ctx, cudaStreamSynchronize(ctx->stream));
+        return run_retry(base, nretry, retry, s1_max, s2_max);
+    }
+
+    // The level launches alone, with no host round trip; rows that
+    // overflowed are listed in `retry` and counted in dcnt->retry_count.
+    int run_levels(const Bins& bins, RowParams base, int G, int d2, Counters* dcnt,
+                   DevBuf& retry) {
         TRY(retry.alloc(ctx, sizeof(int) * (static_cast<size_t>(base.nrows) + 1)));
         CK(ctx, cudaMemsetAsync(&dcnt->retry_count, 0, sizeof(int), ctx->stream));
         for (int L = 0; L < kLevels; ++L) {
@@ -240,23 +265,24 @@ struct RowRunner {
             DevBuf gtab;
             TRY(launch(p, G, gtab));
         }
-        int nretry = 0;
-        CK(ctx, cudaMemcpyAsync(&nretry, &dcnt->retry_count, sizeof(int), cudaMemcpyDeviceToHost,
-                                ctx->stream));
-        CK(ctx, cudaStreamSynchronize(ctx->stream));
-        if (nretry > 0) {
-            RowParams p = base;
-            p.rows = retry.as<int>();
-            p.nrows = nretry;
-            p.S1 = slots_for_need(s1_max, 32);
-            p.S2 = direct ? slots_for_need(s2_max, 32) : 0;
-            // The direct kernel sorts the C row in the first table's storage.
-            if (p.S1 < p.S2) p.S1 = p.S2;
-            p.retry_rows = nullptr;
-            p.retry_count = nullptr;
-            DevBuf gtab;
-            TRY(launch(p, 32, gtab));
-        }
+        return SP3MM_OK;
+    }
+
+    // The retry launch for `nretry` listed rows, tables sized from the
+    // bounds.
+    int run_retry(RowParams base, int nretry, DevBuf& retry, long long s1_max, long long s2_max) {
+        if (nretry <= 0) return SP3MM_OK;
+        RowParams p = base;
+        p.rows = retry.as<int>();
+        p.nrows = nretry;
+        p.S1 = slots_for_need(s1_max, 32);
+        p.S2 = direct ? slots_for_need(s2_max, 32) : 0;
+        // The direct kernel sorts the C row in the first table's storage.
+        if (p.S1 < p.S2) p.S1 = p.S2;
+        p.retry_rows = nullptr;
+        p.retry_count = nullptr;
+        DevBuf gtab;
+        TRY(launch(p, 32, gtab));
         return SP3MM_OK;
     }
 };
@@ -287,6 +313,43 @@ int scan_counts(sp3mm_ctx* ctx, int M, const int* row_cnt, DevBuf& rp, long long
     CK(ctx, cudaStreamSynchronize(ctx->stream));
     *total = t[0];
     if (max_row) *max_row = t[1];
+    return SP3MM_OK;
+}
+
+// The words a booked product reads back after its numeric pass.
+struct TailReads {
+    long long total;   // nnz(C)
+    int max_row;       // longest C row
+    int retry;         // rows left for the retry launch
+    unsigned err;      // device error word
+};
+
+// Scan row counts into row_ptr (allocated on first use) and read back, in
+// one round trip through the context's pinned words, the total, the longest
+// row, the retry count (d_retry, may be null) and the error word.
+int scan_read(sp3mm_ctx* ctx, int M, const int* row_cnt, DevBuf& rp, const int* d_retry,
+              TailReads* out) {
+    const cudaStream_t st = ctx->stream;
+    if (!rp.p) TRY(rp.alloc(ctx, sizeof(int) * (static_cast<size_t>(M) + 2)));
+    DevBuf tmp;
+    const size_t tb = scan_temp_bytes(M);
+    TRY(tmp.alloc(ctx, tb));
+    prof(ctx, "scan", [&] { launch_scan(M, row_cnt, rp.as<int>(), tmp.p, tb, st); });
+    CK(ctx, cudaGetLastError());
+    int* mr = rp.as<int>() + M + 1;
+    CK(ctx, cudaMemsetAsync(mr, 0, sizeof(int), st));
+    launch_count_max(M, row_cnt, nullptr, mr, st);
+    unsigned* box = ctx->host_box;
+    box[2] = 0;
+    CK(ctx, cudaMemcpyAsync(box, rp.as<int>() + M, 2 * sizeof(int), cudaMemcpyDeviceToHost, st));
+    if (d_retry)
+        CK(ctx, cudaMemcpyAsync(box + 2, d_retry, sizeof(int), cudaMemcpyDeviceToHost, st));
+    CK(ctx, cudaMemcpyAsync(box + 3, ctx->d_err, sizeof(unsigned), cudaMemcpyDeviceToHost, st));
+    CK(ctx, cudaStreamSynchronize(st));
+    out->total = static_cast<int>(box[0]);
+    out->max_row = static_cast<int>(box[1]);
+    out->retry = static_cast<int>(box[2]);
+    out->err = box[3];
     return SP3MM_OK;
 }
 
@@ -364,10 +427,12 @@ int product_rows(sp3mm_ctx* ctx, RowRunner& rr, int M, int N, int flavour, int o
             bins.total,
             std::max<unsigned long long>(1ULL << 20,
                                          8ULL * static_cast<unsigned long long>(rr.operand_nnz())));
-        if (cap * eb > (size_t(1) << 30))
+        // Space the pool already holds idle is used without asking the
+        // device for its free memory (a slow query).
+        if (cap * eb > (size_t(1) << 30) && pool_idle_bytes(ctx) < cap * eb)
             cap = std::min<unsigned long long>(
                 cap, std::max<unsigned long long>(1ULL << 20, free_device_bytes(ctx) / 2 / eb));
-        DevBuf ub_ci, ub_v, row_off;
+        DevBuf ub_ci, ub_v, row_off, retry;
         TRY(ub_ci.alloc(ctx, sizeof(int) * cap));
         TRY(ub_v.alloc(ctx, vbytes(out_vt) * cap));
         TRY(row_off.alloc(ctx, sizeof(long long) * (static_cast<size_t>(M) + 1)));
@@ -378,12 +443,16 @@ int product_rows(sp3mm_ctx* ctx, RowRunner& rr, int M, int N, int flavour, int o
         p.ub_ci = ub_ci.as<int>();
         p.ub_v = ub_v.p;
         rr.mode = kNumBook;
-        TRY(rr.run(bins, p, G, d2, s1_max, s2_max, dc));
-        if (cap < bins.total) {
-            unsigned e = 0;
-            TRY(read_err(ctx, &e));
-            if ((e & kErrBook) && e != kErrBook) return check_device_err(ctx);
-            if (e == kErrBook) {
+        // The scan, the retry count and the error word come back together;
+        // rows that overflowed their tables are redone and rescanned.
+        TRY(rr.run_levels(bins, p, G, d2, dc, retry));
+        TailReads tr{};
+        TRY(scan_read(ctx, M, row_cnt.as<int>(), rp, &dc->retry_count, &tr));
+        for (int pass = 0; pass < 2; ++pass) {
+            if (tr.err & ~kErrBook) return check_device_err(ctx);
+            if (tr.err == kErrBook) {
+                // The booking space overflowed (possible only below the
+                // bound): redo the product symbolically.
                 CK(ctx, cudaMemsetAsync(ctx->d_err, 0, sizeof(unsigned), st));
                 ub_ci.release();
                 ub_v.release();
@@ -391,9 +460,12 @@ int product_rows(sp3mm_ctx* ctx, RowRunner& rr, int M, int N, int flavour, int o
                 return product_rows(ctx, rr, M, N, SP3MM_SYMBNUM, out_vt, need, dc, G, d1, d2,
                                      s1_bound, s2_bound, p_max_row, C);
             }
+            if (pass == 1 || tr.retry <= 0) break;
+            TRY(rr.run_retry(p, tr.retry, retry, s1_max, s2_max));
+            TRY(scan_read(ctx, M, row_cnt.as<int>(), rp, nullptr, &tr));
         }
-        TRY(scan_counts(ctx, M, row_cnt.as<int>(), rp, &nnz, &cmax));
-        TRY(check_device_err(ctx));
+        nnz = tr.total;
+        cmax = tr.max_row;
         if (nnz < 0 || nnz >= INT32_MAX)
             return set_error(ctx, SP3MM_ELIMIT, "result has too many nonzeros");
         TRY(ci.alloc(ctx, sizeof(int) * static_cast<size_t>(nnz)));
@@ -403,7 +475,10 @@ int product_rows(sp3mm_ctx* ctx, RowRunner& rr, int M, int N, int flavour, int o
                            rp.as<int>(), ci.as<int>(), v.p, out_vt, st);
         });
     }
-    TRY(check_device_err(ctx));
+    // The booked tail read the error word after its last flag-setting
+    // kernel (the compaction sets none); the symbolic-numeric tail checks
+    // its numeric pass here.
+    if (flavour == SP3MM_SYMBNUM) TRY(check_device_err(ctx));
     C->M = M;
     C->N = N;
     C->nnz = nnz;
@@ -769,6 +844,7 @@ int ctx_init(sp3mm_ctx* c, int device) {
     CK(c, cudaMemset(c->d_err, 0, sizeof(unsigned)));
     CK(c, cudaEventCreate(&c->ev0));
     CK(c, cudaEventCreate(&c->ev1));
+    CK(c, cudaHostAlloc(reinterpret_cast<void**>(&c->host_box), 64, cudaHostAllocDefault));
     // Keep freed pool memory cached between products.
     cudaMemPool_t pool;
     CK(c, cudaDeviceGetDefaultMemPool(&pool, device));
@@ -1020,6 +1096,7 @@ int sp3mm_ctx_destroy(sp3mm_ctx* ctx) {
     if (ctx->ev1) cudaEventDestroy(ctx->ev1);
     if (ctx->own_stream) cudaStreamDestroy(ctx->own_stream);
     if (ctx->host_stage) cudaFreeHost(ctx->host_stage);
+    if (ctx->host_box) cudaFreeHost(ctx->host_box);
     if (tl_ctx == ctx) tl_ctx = nullptr;
     delete ctx;
     return SP3MM_OK;

@@ -41,6 +41,9 @@ struct sp3mm_ctx {
     // context).
     void* host_stage = nullptr;
     size_t host_stage_bytes = 0;
+    // Pinned words the product tail reads back in one round trip (row
+    // count total, longest row, retry count, error word).
+    unsigned* host_box = nullptr;
 };
 
 namespace sp3mm {
@@ -143,6 +146,8 @@ struct Bins {
 // Device memory available to new allocations: free HBM plus the idle part
 // of the device's memory pool.
 size_t free_device_bytes(sp3mm_ctx* ctx);
+// Bytes the device's memory pool holds reserved but unused (a cheap query).
+size_t pool_idle_bytes(sp3mm_ctx* ctx);
 int read_err(sp3mm_ctx* ctx, unsigned* out);
 // Read and clear the sticky device error word; map it to a return code.
 int check_device_err(sp3mm_ctx* ctx);
