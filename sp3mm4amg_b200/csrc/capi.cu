@@ -353,6 +353,21 @@ int scan_read(sp3mm_ctx* ctx, int M, const int* row_cnt, DevBuf& rp, const int* 
     return SP3MM_OK;
 }
 
+// Read back the retry count (d_retry, may be null: 0) and the error word in
+// one round trip.
+int read_retry_err(sp3mm_ctx* ctx, const int* d_retry, TailReads* out) {
+    const cudaStream_t st = ctx->stream;
+    unsigned* box = ctx->host_box;
+    box[2] = 0;
+    if (d_retry)
+        CK(ctx, cudaMemcpyAsync(box + 2, d_retry, sizeof(int), cudaMemcpyDeviceToHost, st));
+    CK(ctx, cudaMemcpyAsync(box + 3, ctx->d_err, sizeof(unsigned), cudaMemcpyDeviceToHost, st));
+    CK(ctx, cudaStreamSynchronize(st));
+    out->retry = static_cast<int>(box[2]);
+    out->err = box[3];
+    return SP3MM_OK;
+}
+
 // Longest row of m, computed on the device when not recorded.
 int known_max_row(sp3mm_ctx* ctx, const sp3mm_dcsr& m, int* out) {
     if (m.max_row >= 0) {
@@ -397,9 +412,18 @@ int product_rows(sp3mm_ctx* ctx, RowRunner& rr, int M, int N, int flavour, int o
             p.row_cnt1 = row_cnt1.as<int>();
         }
         rr.mode = kSymb;
-        TRY(rr.run(bins, p, G, d2, s1_max, s2_max, dc));
-        TRY(scan_counts(ctx, M, row_cnt.as<int>(), rp, &nnz, &cmax));
-        TRY(check_device_err(ctx));
+        DevBuf retry;
+        TRY(rr.run_levels(bins, p, G, d2, dc, retry));
+        TailReads tr{};
+        TRY(scan_read(ctx, M, row_cnt.as<int>(), rp, &dc->retry_count, &tr));
+        if (tr.err) return check_device_err(ctx);
+        if (tr.retry > 0) {
+            TRY(rr.run_retry(p, tr.retry, retry, s1_max, s2_max));
+            TRY(scan_read(ctx, M, row_cnt.as<int>(), rp, nullptr, &tr));
+            if (tr.err) return check_device_err(ctx);
+        }
+        nnz = tr.total;
+        cmax = tr.max_row;
         if (nnz < 0 || nnz >= INT32_MAX)
             return set_error(ctx, SP3MM_ELIMIT, "result has too many nonzeros");
         TRY(ci.alloc(ctx, sizeof(int) * static_cast<size_t>(nnz)));
@@ -417,7 +441,13 @@ int product_rows(sp3mm_ctx* ctx, RowRunner& rr, int M, int N, int flavour, int o
         p.c_ci = ci.as<int>();
         p.c_v = v.p;
         rr.mode = kNumExact;
-        TRY(rr.run(nb, p, G, 0, s1_max, s2_max, dc));
+        TRY(rr.run_levels(nb, p, G, 0, dc, retry));
+        TRY(read_retry_err(ctx, &dc->retry_count, &tr));
+        if (tr.retry > 0 && !tr.err) {
+            TRY(rr.run_retry(p, tr.retry, retry, s1_max, s2_max));
+            TRY(read_retry_err(ctx, nullptr, &tr));
+        }
+        if (tr.err) return check_device_err(ctx);
     } else {
         // Rows book their exact length from one cursor, so the space need
         // only exceed nnz(C): the bound, capped at half the free memory; a
@@ -475,10 +505,8 @@ int product_rows(sp3mm_ctx* ctx, RowRunner& rr, int M, int N, int flavour, int o
                            rp.as<int>(), ci.as<int>(), v.p, out_vt, st);
         });
     }
-    // The booked tail read the error word after its last flag-setting
-    // kernel (the compaction sets none); the symbolic-numeric tail checks
-    // its numeric pass here.
-    if (flavour == SP3MM_SYMBNUM) TRY(check_device_err(ctx));
+    // Both tails read the error word after their last flag-setting kernel
+    // (the compaction sets none).
     C->M = M;
     C->N = N;
     C->nnz = nnz;

@@ -88,9 +88,31 @@ __device__ __forceinline__ int winsert(const WTab& T, int key, bool& is_new) {
     return -1;
 }
 
+// Find `key` or claim an empty slot probing one slot at a time (linear
+// probing from the key's hash).  Same contract as winsert; the batch kernels
+// use it (measured faster there than bucketed probing, slower on the
+// single-product kNN rows).
+__device__ __forceinline__ int winsert1(const WTab& T, int key, bool& is_new) {
+    unsigned s = hash_slot(key, T.shift);
+    for (unsigned probe = 0; probe <= T.smask; ++probe) {
+        const int k = T.keys[s];
+        if (k == key) return static_cast<int>(s);
+        if (k == kEmpty) {
+            const int old = atomicCAS(T.keys + s, kEmpty, key);
+            if (old == kEmpty) {
+                is_new = true;
+                return static_cast<int>(s);
+            }
+            if (old == key) return static_cast<int>(s);
+        }
+        s = (s + 1) & T.smask;
+    }
+    return -1;
+}
+
 // One batch: lane i holds staged product i (key sk[i], value sv[i]) when
 // `valid`.  Updates nk, the table's distinct count.
-template <bool NUM>
+template <bool NUM, bool B4 = true>
 __device__ __forceinline__ void wbatch(const WTab& T, const int* sk, const double* sv, int i,
                                        bool valid, int& nk) {
     const int lane = threadIdx.x & 31;
@@ -100,7 +122,7 @@ __device__ __forceinline__ void wbatch(const WTab& T, const int* sk, const doubl
     bool is_new = false;
     int slot = 0;
     if (valid && (peers & lt) == 0) {
-        slot = winsert(T, key, is_new);
+        slot = B4 ? winsert(T, key, is_new) : winsert1(T, key, is_new);
         if (NUM && slot >= 0) {
             double acc = T.vals[slot];
             const int i0 = i - lane;
@@ -134,7 +156,7 @@ __device__ __forceinline__ int wscan_excl(int v, int& total) {
 // order (the warp owns the row; n is warp-uniform).  Returns false when the
 // table passed its load limit; nk = distinct columns inserted (listed in
 // T.ord either way).
-template <bool NUM, typename TB, class Left>
+template <bool NUM, bool B4 = true, typename TB, class Left>
 __device__ __forceinline__ bool waccumulate(const Left& L, int n, const int* __restrict__ b_rp,
                                             const int* __restrict__ b_ci,
                                             const TB* __restrict__ b_v, const WTab& T, int* sk,
@@ -195,7 +217,7 @@ __device__ __forceinline__ bool waccumulate(const Left& L, int n, const int* __r
             __syncwarp();
             const int wl = min(kStage, total - w0);
             for (int i0 = 0; i0 < wl; i0 += 32) {
-                wbatch<NUM>(T, sk, sv, i0 + lane, i0 + lane < wl, nk);
+                wbatch<NUM, B4>(T, sk, sv, i0 + lane, i0 + lane < wl, nk);
                 if (nk > T.limit) {
                     __syncwarp();
                     return false;
