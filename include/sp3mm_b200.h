@@ -157,6 +157,27 @@ SP3MM_API idx_t *spMMSizeUpperboundColParts_0(spmat *A, spmat *B, unsigned short
 SP3MM_API idx_t *spMMSizeUpperboundColParts_1(spmat *A, spmat *B, unsigned short gridCols,
                                     idx_t *bColPartOffsets);
 
+/* MatrixMarket coordinate file -> host CSR spmat, 0-based, the arrays from
+ * malloc/calloc (freeSpmat releases them); NULL plus a message on stderr on
+ * error.  Replaces code/src/lib/parser.c:126-330 (MMtoCSR over MMRead,
+ * MMtoCOO, COOtoCSR): real / integer / pattern (value 1.0) fields;
+ * "symmetric" files expanded with each off-diagonal item mirrored right
+ * after it; every row keeps the file's entry order, so files written row by
+ * row in ascending column order give the ordered CSR the products require
+ * (sp3mm_spmat_sort_rows orders the others).  Errors where the reference's
+ * behaviour is undefined: a count of items different from the size line's,
+ * an index outside the declared shape, complex or array files. */
+SP3MM_API spmat *MMtoCSR(char *matPath);
+/* New, no counterpart in the reference: write a host CSR (index base off_f,
+ * 0 or 1) as a "matrix coordinate real general" MatrixMarket file with
+ * 1-based indices and values printed to round-trip exactly (%.17g).
+ * Returns SP3MM_OK or SP3MM_EINVAL (invalid CSR or unwritable path). */
+SP3MM_API int sp3mm_write_mm(const spmat *m, int off_f, const char *path);
+/* New, no counterpart in the reference: sort every row of a host CSR (index
+ * base off_f) by column index in place, keeping the order of equal columns.
+ * Returns SP3MM_OK or SP3MM_EINVAL. */
+SP3MM_API int sp3mm_spmat_sort_rows(spmat *m, int off_f);
+
 /* Dispatch tables with the reference's names and orders
  * (code/src/include/Sp3MM_CSR_OMP_UB_Generic.h:86-95,
  *  code/src/include/Sp3MM_CSR_OMP_Num_Generic.h:86-95), so that the

@@ -21,6 +21,7 @@ Device API (layer 2, operands resident in HBM)::
 from __future__ import annotations
 
 import ctypes
+import os
 
 import numpy as np
 
@@ -35,7 +36,7 @@ __all__ = [
     "CSR", "Problem", "Context", "DeviceCSR", "Sp3mmError", "spmm", "sp3mm",
     "symb_rowsizes", "ub_rowsizes", "ub_colparts_rowsizes", "elapsed_internal",
     "UB", "SYMBNUM", "PAIR", "DIRECT", "PAIR_RIGHT", "F64", "F32", "RBTREE", "IDXMAP",
-    "BATCH_SPMM", "BATCH_RAP", "Batch", "Hierarchy", "Server",
+    "BATCH_SPMM", "BATCH_RAP", "Batch", "Hierarchy", "Server", "read_mm", "write_mm",
 ]
 
 
@@ -130,6 +131,34 @@ def ub_colparts_rowsizes(A: CSR, B: CSR, grid_cols: int, b_col_offsets: np.ndarr
     f = getattr(lib, f"spMMSizeUpperboundColParts_{off_f}")
     return _sizes(f(a.ptr, b.ptr, grid_cols, offs.ctypes.data_as(ctypes.POINTER(idx_t))),
                   A.M * grid_cols + 1)
+
+
+def read_mm(path: str, sort_rows: bool = False) -> CSR:
+    """Read a MatrixMarket coordinate file with the library's MMtoCSR (the
+    reference's loader, code/src/lib/parser.c): 0-based CSR, symmetric files
+    expanded, rows in the file's entry order unless ``sort_rows``."""
+    lib = capi.load()
+    p = lib.MMtoCSR(os.fsencode(path))
+    if not p:
+        raise Sp3mmError(f"MMtoCSR failed for {path} (see stderr)")
+    try:
+        if sort_rows:
+            rc = lib.sp3mm_spmat_sort_rows(ctypes.cast(p, SPMAT_P), 0)
+            if rc:
+                raise Sp3mmError(f"sp3mm_spmat_sort_rows failed ({rc})")
+        return csr_from_spmat(p, 0)
+    finally:
+        _free_spmat(p)
+
+
+def write_mm(csr: CSR, path: str) -> None:
+    """Write a CSR as a MatrixMarket "coordinate real general" file
+    (sp3mm_write_mm; 1-based indices, values that round-trip exactly)."""
+    lib = capi.load()
+    h = HostSpMat(csr, 0)
+    rc = lib.sp3mm_write_mm(h.ptr, 0, os.fsencode(path))
+    if rc:
+        raise Sp3mmError(f"sp3mm_write_mm failed for {path} ({rc})")
 
 
 def elapsed_internal() -> float:

@@ -104,6 +104,13 @@ DEVICE_API = {
     "sp3mm_server_free": (_c.c_int, [_c.c_void_p]),
 }
 
+# Host-side MatrixMarket entry points with (restype, argtypes).
+HOST_API = {
+    "MMtoCSR": (_c.c_void_p, [_c.c_char_p]),
+    "sp3mm_write_mm": (_c.c_int, [SPMAT_P, _c.c_int, _c.c_char_p]),
+    "sp3mm_spmat_sort_rows": (_c.c_int, [SPMAT_P, _c.c_int]),
+}
+
 # Error codes, flavours, variants, value types (include/sp3mm_b200.h).
 SP3MM_OK, SP3MM_ECUDA, SP3MM_EINVAL, SP3MM_ENOMEM, SP3MM_ELIMIT, SP3MM_EDEVICE = range(6)
 UB, SYMBNUM = 0, 1
@@ -132,6 +139,7 @@ def all_symbols() -> list[str]:
         for n in SPMM_UB_NAMES + SPMM_SYMBNUM_NAMES + SP3MM_NAMES + SIZE_NAMES:
             names.append(f"{n}{off}")
     names += list(DEVICE_API)
+    names += list(HOST_API)
     names += ["Start", "End", "Elapsed", "ElapsedInternal"]
     return names
 
@@ -167,7 +175,7 @@ def load(path: str = LIB_PATH) -> ctypes.CDLL:
         f = getattr(lib, f"spMMSizeUpperboundColParts_{off}")
         f.restype = ctypes.c_void_p
         f.argtypes = [SPMAT_P, SPMAT_P, ctypes.c_ushort, ctypes.POINTER(idx_t)]
-    for name, (res, args) in DEVICE_API.items():
+    for name, (res, args) in list(DEVICE_API.items()) + list(HOST_API.items()):
         f = getattr(lib, name)
         f.restype = res
         f.argtypes = args
