@@ -250,10 +250,13 @@ SP3MM_API uint64_t sp3mm_ctx_launches(sp3mm_ctx *ctx);
 /* Block until the context's stream is idle. */
 SP3MM_API int sp3mm_ctx_sync(sp3mm_ctx *ctx);
 /* Row-kernel tuning (results never depend on it): lanes per output row
- * (4, 8, 16, 32; 0 = from the operands' mean row length); d1: the first
- * hash table of a row is sized for its distinct-key bound >> d1; d2: the
- * direct product's second table is the first >> d2 (d1, d2 < 0: defaults).
- * Rows whose tables overflow are recomputed with proven-size tables. */
+ * (4, 8, 16, 32; 512: a CTA of 16 warps per row of a direct product, with
+ * dense shared-memory accumulators; 0 = default: a warp per row, and the
+ * CTA per row for direct rows with thousands of distinct columns); d1: the
+ * first hash table of a row is sized for its distinct-key bound >> d1; d2:
+ * the direct product's second table is the first >> d2 (d1, d2 < 0:
+ * defaults).  Rows whose tables overflow are recomputed with proven-size
+ * tables. */
 SP3MM_API int sp3mm_ctx_set_tuning(sp3mm_ctx *ctx, int lanes_per_row, int d1, int d2);
 /* Time every kernel launch with CUDA events on the context stream (on != 0);
  * switching clears the records. */

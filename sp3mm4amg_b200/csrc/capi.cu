@@ -164,8 +164,21 @@ double wall_seconds() {
 // mean row length of the right operand is kept for callers that tune by it.
 int pick_group(const sp3mm_ctx* ctx, double mean) {
     (void)mean;
-    if (ctx->tune_G) return ctx->tune_G;
+    if (ctx->tune_G && ctx->tune_G != kDenseLanes) return ctx->tune_G;
     return 32;
+}
+
+// Whether a launch of the direct product runs the CTA-per-row kernel: every
+// row when the tuning asks for it; by default the rows binned to tables of
+// kDenseMinSlots or more (thousands of distinct columns: coarse levels),
+// where a warp per row with such a table leaves few warps per SM.  Never
+// the retry launch, which needs proven-size tables.
+constexpr int kDenseMinSlots = 2048;
+bool use_dense(const sp3mm_ctx* ctx, const RowParams& p) {
+    if (!p.retry_rows) return false;
+    if (dense_row_smem() + 1024 > ctx->smem_optin) return false;
+    if (ctx->tune_G == kDenseLanes) return true;
+    return ctx->tune_G == 0 && p.S1 >= kDenseMinSlots;
 }
 
 // One row-kernel family over a set of rows: shared-memory tables when they
@@ -184,6 +197,18 @@ struct RowRunner {
     }
 
     int launch(RowParams p, int G, DevBuf& gtab) {
+        if (direct && use_dense(ctx, p)) {
+            static const char* const kDense[3] = {"direct.dense.symb", "direct.dense.num",
+                                                  "direct.dense.book"};
+            cudaError_t e = cudaSuccess;
+            prof(ctx, kDense[mode], [&] {
+                e = launch_direct_dense(da, p, mode, ctx->num_sms, ctx->stream);
+            });
+            if (e != cudaSuccess)
+                return set_error(ctx, SP3MM_ECUDA, "dense row kernel launch failed: %s",
+                                 cudaGetErrorString(e));
+            return SP3MM_OK;
+        }
         const size_t per_group = row_table_bytes(direct, mode, G, p.S1, p.S2);
         const int gpw = 32 / G;
         int warps = static_cast<int>(ctx->smem_budget / (per_group * gpw));
@@ -1169,8 +1194,9 @@ int sp3mm_ctx_sync(sp3mm_ctx* ctx) {
 int sp3mm_ctx_set_tuning(sp3mm_ctx* ctx, int lanes_per_row, int d1, int d2) {
     if (!ctx) return SP3MM_EINVAL;
     if (lanes_per_row != 0 && lanes_per_row != 4 && lanes_per_row != 8 && lanes_per_row != 16 &&
-        lanes_per_row != 32)
-        return set_error(ctx, SP3MM_EINVAL, "lanes per row must be 0, 4, 8, 16 or 32");
+        lanes_per_row != 32 && lanes_per_row != kDenseLanes)
+        return set_error(ctx, SP3MM_EINVAL, "lanes per row must be 0, 4, 8, 16, 32 or %d",
+                         kDenseLanes);
     if (d1 > 16 || d2 > 16) return set_error(ctx, SP3MM_EINVAL, "table shifts must be <= 16");
     ctx->tune_G = lanes_per_row;
     ctx->tune_d1 = d1;

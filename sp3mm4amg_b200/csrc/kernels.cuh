@@ -70,6 +70,15 @@ int row_table_limit(int S, int G);
 int row_prefetch_cover(int G);
 cudaError_t launch_direct_rows(const DirectRowArgs& a, const RowParams& p, int mode,
                                const RowGeom& geo, cudaStream_t st);
+// Tuning value of "lanes per row" that runs every direct row on the
+// CTA-per-row kernel.
+constexpr int kDenseLanes = 512;
+// Direct rows with heavy work, one CTA per row (rowdense.cuh); rows that do
+// not fit its shared-memory slice go to the retry list.  dense_row_smem():
+// its dynamic shared memory per CTA.
+cudaError_t launch_direct_dense(const DirectRowArgs& a, const RowParams& p, int mode, int grid,
+                                cudaStream_t st);
+size_t dense_row_smem();
 cudaError_t launch_pair_rows(const PairRowArgs& a, const RowParams& p, int mode,
                              const RowGeom& geo, cudaStream_t st);
 

@@ -1,0 +1,409 @@
+// rowdense.cuh -- direct R*A*P rows with heavy work (coarse AMG levels): one
+// CTA per output row, dense accumulators in shared memory (sm_100a).
+//
+// On the coarse levels of a hierarchy the rows are few and long: an R row
+// reaches hundreds of A rows of hundreds of entries, the R*A row has
+// thousands of columns, and one warp per row with a hash table large enough
+// for it leaves a handful of warps per SM.  Here a CTA of kDWarps warps owns
+// one row, and the warps split the row's COLUMNS, not its products: warp w
+// owns a contiguous column range, finds in every right row the segment that
+// falls in its range (binary search; right rows are ordered), and processes
+// exactly its products in the reference's order (left position ascending,
+// then the right row's entries).  Every column therefore still receives its
+// contributions in the reference's order (code/src/include/
+// SpMMUtilsGeneric.h:39-55), and the accumulator of a column range is a
+// dense slice of shared memory indexed by column -- no hashing.  Equal
+// columns within a batch of 32 staged products are resolved as in the warp
+// kernels (__match_any_sync, the group's lowest lane adds the group's
+// products in lane order).
+//
+// Stage 1 (the R*A row) walks the row's column span in chunks of kDSpan
+// columns.  Each column's first touch is recorded as the flat position of
+// the product that made it (left position, then right-row entry), and after
+// each chunk the touched columns are listed with their position and value.
+// Sorting that list by position gives the order in which the reference's
+// index map appends the columns (code/src/include/sparseMatrix.h:85-104), the
+// order in which the direct product forwards the R*A row into P
+// (code/src/Sp3MM_CSR_OMP_UB_Generic.c:542-545).  Stage 2 forwards the list
+// into P over the span of the P columns it reaches (one chunk), and the C row
+// is written in column order straight from the dense slice (no sort).
+//
+// A row whose R*A row has more than kDList columns, or whose C row spans more
+// than kDSpan columns, is appended to the retry list (processed by the
+// retry launch with tables sized from a proven bound).
+#pragma once
+
+#include "rowwarp.cuh"
+
+namespace sp3mm {
+
+constexpr int kDWarps = 16;    // warps per CTA (one output row per CTA)
+constexpr int kDSpan = 8192;   // columns of the dense accumulator slice
+constexpr int kDList = 4096;   // R*A row entries a CTA holds
+
+// Dynamic shared memory: acc double[kDSpan] | ftq int[kDSpan] (after stage 1:
+// u64 sort keys [kDList]) | lkey int[kDList] | lq int[kDList] |
+// lval double[kDList] | touched u8[kDSpan] | per warp: sk int[kStage],
+// sq int[kStage], sv double[kStage].
+__host__ __device__ constexpr size_t dense_smem_bytes() {
+    return static_cast<size_t>(kDSpan) * 8 + static_cast<size_t>(kDSpan) * 4 +
+           static_cast<size_t>(kDList) * 16 + static_cast<size_t>(kDSpan) +
+           static_cast<size_t>(kDWarps) * kStage * 16;
+}
+
+// First index in [b, e) whose column is >= x (columns ascending).
+__device__ __forceinline__ int lbound(const int* __restrict__ ci, int b, int e, int x) {
+    while (b < e) {
+        const int m = b + ((e - b) >> 1);
+        if (__ldg(ci + m) < x) b = m + 1;
+        else e = m;
+    }
+    return b;
+}
+
+// The stage-1 list in first-touch order: entry t is list index sorted[t]
+// (low 32 bits of the sorted (position, index) key).
+struct LeftSorted {
+    const unsigned long long* sorted;
+    const int* keys;
+    const double* vals;
+    __device__ __forceinline__ int key(int t) const {
+        return keys[static_cast<unsigned>(sorted[t])];
+    }
+    __device__ __forceinline__ double val(int t) const {
+        return vals[static_cast<unsigned>(sorted[t])];
+    }
+};
+
+// One batch of staged products into the dense slice (slot = column - base).
+// FT: record a new column's first-touch position.
+template <bool NUM, bool FT>
+__device__ __forceinline__ void dbatch(double* acc, unsigned char* touched, int* ftq, int base,
+                                       const int* sk, const double* sv, const int* sq, int i,
+                                       bool valid) {
+    const int lane = threadIdx.x & 31;
+    const unsigned lt = lanemask_lt();
+    const int key = valid ? sk[i] : -2 - lane;
+    const unsigned peers = __match_any_sync(kFull, key);
+    if (valid && (peers & lt) == 0) {
+        const int slot = key - base;
+        if (!touched[slot]) {
+            touched[slot] = 1;
+            if (FT) ftq[slot] = sq[i];
+        }
+        if (NUM) {
+            double v = acc[slot];
+            const int i0 = i - lane;
+            unsigned m = peers;
+            do {
+                const int l = __ffs(m) - 1;
+                m &= m - 1;
+                v = __dadd_rn(v, sv[i0 + l]);
+            } while (m);
+            acc[slot] = v;
+        }
+    }
+}
+
+// sum_{t<n} L.val(t) * B(L.key(t), :) restricted to the columns [wlo, whi)
+// (inside the slice starting at `base`), in the reference's order.  FT: the
+// flat position of a product is the sum of the full lengths of the right
+// rows before its left position plus its offset in its own right row.
+template <bool NUM, bool FT, typename TB, class Left>
+__device__ __forceinline__ void daccumulate(const Left& L, int n, const int* __restrict__ b_rp,
+                                            const int* __restrict__ b_ci,
+                                            const TB* __restrict__ b_v, int wlo, int whi,
+                                            int base, double* acc, unsigned char* touched,
+                                            int* ftq, int* sk, int* sq, double* sv) {
+    if (wlo >= whi) return;
+    const int lane = threadIdx.x & 31;
+    int qbase = 0;
+    for (int t0 = 0; t0 < n; t0 += 32) {
+        const int t = t0 + lane;
+        int ab = 0, ae = 0, sb = 0, se = 0;
+        double s = 0.0;
+        if (t < n) {
+            const int k = L.key(t);
+            if (NUM) s = L.val(t);
+            ab = __ldg(b_rp + k);
+            ae = __ldg(b_rp + k + 1);
+            sb = lbound(b_ci, ab, ae, wlo);
+            se = lbound(b_ci, sb, ae, whi);
+        }
+        int fo = 0;
+        if (FT) {
+            int full;
+            fo = wscan_excl(ae - ab, full) + qbase;
+            qbase += full;
+        }
+        const int len = se - sb;
+        int total;
+        const int off = wscan_excl(len, total);
+        if (total == 0) continue;
+        const bool spread = __reduce_max_sync(kFull, static_cast<unsigned>(len)) > 16u;
+        for (int w0 = 0; w0 < total; w0 += kStage) {
+            const int wl = min(kStage, total - w0);
+            if (spread) {
+#pragma unroll
+                for (int r = 0; r < kStage / 32; ++r) {
+                    const int i = lane + 32 * r;
+                    const int pidx = w0 + i;
+                    int j = 0;
+#pragma unroll
+                    for (int step = 16; step > 0; step >>= 1) {
+                        const int oc = __shfl_sync(kFull, off, j + step);
+                        if (oc <= pidx) j += step;
+                    }
+                    const int sbj = __shfl_sync(kFull, sb, j);
+                    const int ofj = __shfl_sync(kFull, off, j);
+                    double sj = 0.0;
+                    if (NUM) sj = __shfl_sync(kFull, s, j);
+                    int qj = 0;
+                    if (FT) qj = __shfl_sync(kFull, fo - ab, j);
+                    if (i < wl) {
+                        const int e = sbj + pidx - ofj;
+                        sk[i] = __ldg(b_ci + e);
+                        if (NUM) sv[i] = __dmul_rn(ldv(b_v, e), sj);
+                        if (FT) sq[i] = qj + e;
+                    }
+                }
+            } else {
+                const int e_end = min(len, w0 + kStage - off);
+                int e = max(0, w0 - off);
+#pragma unroll 4
+                for (; e < e_end; ++e) {
+                    const int pos = off + e - w0;
+                    const int ea = sb + e;
+                    sk[pos] = __ldg(b_ci + ea);
+                    if (NUM) sv[pos] = __dmul_rn(ldv(b_v, ea), s);
+                    if (FT) sq[pos] = fo + (ea - ab);
+                }
+            }
+            __syncwarp();
+            for (int i0 = 0; i0 < wl; i0 += 32)
+                dbatch<NUM, FT>(acc, touched, ftq, base, sk, sv, sq, i0 + lane, i0 + lane < wl);
+            __syncwarp();
+        }
+    }
+}
+
+// Block-wide min / max of (lo, hi) into *slo / *shi (initialised by the
+// caller before the barrier that precedes this call).
+__device__ __forceinline__ void block_span(int lo, int hi, int* slo, int* shi) {
+    lo = __reduce_min_sync(kFull, lo);
+    hi = __reduce_max_sync(kFull, hi);
+    if ((threadIdx.x & 31) == 0) {
+        atomicMin(slo, lo);
+        atomicMax(shi, hi);
+    }
+}
+
+template <int MODE, typename TV, typename TO>
+__global__ void __launch_bounds__(kDWarps * 32, 1) k_direct_dense(DirectRowArgs a, RowParams p) {
+    constexpr bool NUM = MODE != kSymb;
+    extern __shared__ __align__(16) unsigned char smem[];
+    __shared__ int s_n1, s_lo, s_hi, s_cnt[kDWarps];
+    __shared__ long long s_base;
+    double* acc = reinterpret_cast<double*>(smem);
+    int* ftq = reinterpret_cast<int*>(acc + kDSpan);
+    unsigned long long* sorted = reinterpret_cast<unsigned long long*>(ftq);
+    int* lkey = ftq + kDSpan;
+    int* lq = lkey + kDList;
+    double* lval = reinterpret_cast<double*>(lq + kDList);
+    unsigned char* touched = reinterpret_cast<unsigned char*>(lval + kDList);
+    const int lane = threadIdx.x & 31;
+    const int wid = threadIdx.x >> 5;
+    unsigned char* wst = touched + kDSpan + static_cast<size_t>(wid) * kStage * 16;
+    int* sk = reinterpret_cast<int*>(wst);
+    int* sq = sk + kStage;
+    double* sv = reinterpret_cast<double*>(sq + kStage);
+    const unsigned lt = lanemask_lt();
+    for (int s = threadIdx.x; s < kDSpan; s += blockDim.x) {
+        acc[s] = 0.0;
+        touched[s] = 0;
+    }
+    const TV* rv = static_cast<const TV*>(a.R.v);
+    const TV* av = static_cast<const TV*>(a.A.v);
+    const TV* pv = static_cast<const TV*>(a.P.v);
+
+    for (long long it = blockIdx.x; it < p.nrows; it += gridDim.x) {
+        const int row = p.rows[it];
+        const int rb = __ldg(a.R.rp + row);
+        const int rlen = __ldg(a.R.rp + row + 1) - rb;
+        if (threadIdx.x == 0) {
+            s_n1 = 0;
+            s_lo = INT_MAX;
+            s_hi = -1;
+        }
+        __syncthreads();
+        // Stage-1 span: the A rows' first and last columns.
+        int lo = INT_MAX, hi = -1;
+        for (int t = threadIdx.x; t < rlen; t += blockDim.x) {
+            const int k = __ldg(a.R.ci + rb + t);
+            const int ab = __ldg(a.A.rp + k), ae = __ldg(a.A.rp + k + 1);
+            if (ab < ae) {
+                lo = min(lo, __ldg(a.A.ci + ab));
+                hi = max(hi, __ldg(a.A.ci + ae - 1));
+            }
+        }
+        block_span(lo, hi, &s_lo, &s_hi);
+        __syncthreads();
+        const int lo1 = s_lo, hi1 = s_hi;
+        const LeftG<TV> L1{a.R.ci, rv, rb};
+        for (long long c0 = lo1; c0 <= hi1; c0 += kDSpan) {
+            const int cb = static_cast<int>(c0);
+            const int ce = static_cast<int>(min(static_cast<long long>(hi1) + 1, c0 + kDSpan));
+            const int width = (ce - cb + kDWarps - 1) / kDWarps;
+            const int wlo = min(ce, cb + wid * width), whi = min(ce, wlo + width);
+            daccumulate<NUM, true>(L1, rlen, a.A.rp, a.A.ci, av, wlo, whi, cb, acc, touched, ftq,
+                                   sk, sq, sv);
+            __syncthreads();
+            // List this warp's touched columns (value and first touch) and
+            // clear them.
+            for (int s0 = wlo; s0 < whi; s0 += 32) {
+                const int col = s0 + lane;
+                const bool hit = col < whi && touched[col - cb];
+                const unsigned b = __ballot_sync(kFull, hit);
+                int pos0 = 0;
+                if (lane == 0 && b) pos0 = atomicAdd(&s_n1, __popc(b));
+                pos0 = __shfl_sync(kFull, pos0, 0);
+                if (hit) {
+                    const int slot = col - cb;
+                    const int pos = pos0 + __popc(b & lt);
+                    if (pos < kDList) {
+                        lkey[pos] = col;
+                        lq[pos] = ftq[slot];
+                        if (NUM) lval[pos] = acc[slot];
+                    }
+                    touched[slot] = 0;
+                    if (NUM) acc[slot] = 0.0;
+                }
+            }
+            __syncthreads();
+        }
+        const int n1 = s_n1;
+        bool fail = n1 > kDList;
+        // First-touch order: sort (position, index) keys.
+        if (!fail && n1 > 1) {
+            const int P2 = static_cast<int>(next_pow2(static_cast<unsigned>(n1)));
+            for (int i = threadIdx.x; i < P2; i += blockDim.x)
+                sorted[i] = i < n1 ? (static_cast<unsigned long long>(static_cast<unsigned>(lq[i]))
+                                      << 32) | static_cast<unsigned>(i)
+                                   : ~0ULL;
+            __syncthreads();
+            for (int k = 2; k <= P2; k <<= 1) {
+                for (int j = k >> 1; j > 0; j >>= 1) {
+                    for (int i = threadIdx.x; i < P2; i += blockDim.x) {
+                        const int ixj = i ^ j;
+                        if (ixj > i) {
+                            const unsigned long long x = sorted[i], y = sorted[ixj];
+                            if ((x > y) == ((i & k) == 0)) {
+                                sorted[i] = y;
+                                sorted[ixj] = x;
+                            }
+                        }
+                    }
+                    __syncthreads();
+                }
+            }
+        } else if (!fail && n1 == 1 && threadIdx.x == 0) {
+            sorted[0] = 0;
+        }
+        if (threadIdx.x == 0) {
+            s_lo = INT_MAX;
+            s_hi = -1;
+        }
+        __syncthreads();
+        // Stage-2 span: the P rows' first and last columns.
+        lo = INT_MAX;
+        hi = -1;
+        if (!fail) {
+            for (int t = threadIdx.x; t < n1; t += blockDim.x) {
+                const int c = lkey[t];
+                const int pb = __ldg(a.P.rp + c), pe = __ldg(a.P.rp + c + 1);
+                if (pb < pe) {
+                    lo = min(lo, __ldg(a.P.ci + pb));
+                    hi = max(hi, __ldg(a.P.ci + pe - 1));
+                }
+            }
+        }
+        block_span(lo, hi, &s_lo, &s_hi);
+        __syncthreads();
+        const int lo2 = s_lo, hi2 = s_hi;
+        if (hi2 >= lo2 && static_cast<long long>(hi2) - lo2 + 1 > kDSpan) fail = true;
+        const bool run2 = !fail && hi2 >= lo2;
+        int wlo2 = 0, whi2 = 0;
+        if (run2) {
+            const int width = (hi2 + 1 - lo2 + kDWarps - 1) / kDWarps;
+            wlo2 = min(hi2 + 1, lo2 + wid * width);
+            whi2 = min(hi2 + 1, wlo2 + width);
+            const LeftSorted L2{sorted, lkey, lval};
+            daccumulate<NUM, false>(L2, n1, a.P.rp, a.P.ci, pv, wlo2, whi2, lo2, acc, touched,
+                                    nullptr, sk, sq, sv);
+        }
+        __syncthreads();
+        int cnt = 0;
+        if (run2) {
+            for (int s0 = wlo2; s0 < whi2; s0 += 32) {
+                const int col = s0 + lane;
+                cnt += __popc(__ballot_sync(kFull, col < whi2 && touched[col - lo2]));
+            }
+        }
+        if (lane == 0) s_cnt[wid] = cnt;
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            long long base = -1;
+            int n2 = 0;
+            for (int w = 0; w < kDWarps; ++w) n2 += s_cnt[w];
+            if (fail) {
+                if (p.retry_rows) p.retry_rows[atomicAdd(p.retry_count, 1)] = row;
+                else atomicOr(p.err, kErrTable);
+            } else if (MODE == kSymb) {
+                p.row_cnt[row] = n2;
+                if (p.row_cnt1) p.row_cnt1[row] = n1;
+            } else if (MODE == kNumBook) {
+                const unsigned long long off =
+                    n2 > 0 ? atomicAdd(p.cursor, static_cast<unsigned long long>(n2)) : 0ULL;
+                if (off + n2 > p.cap) {
+                    atomicOr(p.err, kErrBook);
+                } else {
+                    p.row_off[row] = static_cast<long long>(off);
+                    p.row_cnt[row] = n2;
+                    base = static_cast<long long>(off);
+                }
+            } else {
+                const long long b = p.c_rp[row];
+                if (p.c_rp[row + 1] - b != n2) atomicOr(p.err, kErrCount);
+                else base = b;
+            }
+            s_base = base;
+        }
+        __syncthreads();
+        if (run2) {
+            // Write this warp's columns in order and clear the slice.
+            long long wpos = s_base;
+            for (int w = 0; w < wid; ++w) wpos += s_cnt[w];
+            int* oc = MODE == kNumBook ? p.ub_ci : p.c_ci;
+            TO* ov = static_cast<TO*>(MODE == kNumBook ? p.ub_v : p.c_v);
+            for (int s0 = wlo2; s0 < whi2; s0 += 32) {
+                const int col = s0 + lane;
+                const bool hit = col < whi2 && touched[col - lo2];
+                const unsigned b = __ballot_sync(kFull, hit);
+                if (hit) {
+                    const int slot = col - lo2;
+                    if (NUM && s_base >= 0) {
+                        const long long o = wpos + __popc(b & lt);
+                        oc[o] = col;
+                        stv(ov, o, acc[slot]);
+                    }
+                    touched[slot] = 0;
+                    if (NUM) acc[slot] = 0.0;
+                }
+                wpos += __popc(b);
+            }
+        }
+        __syncthreads();
+    }
+}
+
+}  // namespace sp3mm

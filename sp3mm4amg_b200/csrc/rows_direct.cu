@@ -1,6 +1,6 @@
 // rows_direct.cu -- instantiations and launcher of the direct R*A*P row
 // kernel (rows.cuh).
-#include "rowwarp.cuh"
+#include "rowdense.cuh"
 
 namespace sp3mm {
 
@@ -48,6 +48,38 @@ static cudaError_t direct_mode(const DirectRowArgs& a, const RowParams& p, int m
     if (mode == kSymb) return direct_typed<G, kSymb, GT>(a, p, geo, st);
     if (mode == kNumExact) return direct_typed<G, kNumExact, GT>(a, p, geo, st);
     return direct_typed<G, kNumBook, GT>(a, p, geo, st);
+}
+
+template <int MODE>
+static cudaError_t dense_typed(const DirectRowArgs& a, const RowParams& p, int grid,
+                               cudaStream_t st) {
+    const int tv = a.R.vtype, to = p.c_vt;
+    RowGeom geo{};
+    geo.G = 32 * kDWarps;
+    geo.grid = grid;
+    geo.block = 32 * kDWarps;
+    geo.smem = dense_smem_bytes();
+    if (MODE == kSymb)
+        return launch_row_kernel(k_direct_dense<kSymb, double, double>, a, p, geo, st);
+    if (tv == SP3MM_F64 && to == SP3MM_F64)
+        return launch_row_kernel(k_direct_dense<MODE, double, double>, a, p, geo, st);
+    if (tv == SP3MM_F64 && to == SP3MM_F32)
+        return launch_row_kernel(k_direct_dense<MODE, double, float>, a, p, geo, st);
+    if (tv == SP3MM_F32 && to == SP3MM_F32)
+        return launch_row_kernel(k_direct_dense<MODE, float, float>, a, p, geo, st);
+    return launch_row_kernel(k_direct_dense<MODE, float, double>, a, p, geo, st);
+}
+
+size_t dense_row_smem() { return dense_smem_bytes(); }
+
+cudaError_t launch_direct_dense(const DirectRowArgs& a, const RowParams& p, int mode, int grid,
+                                cudaStream_t st) {
+    if (p.nrows <= 0) return cudaSuccess;
+    note_launch();
+    if (grid > p.nrows) grid = p.nrows;
+    if (mode == kSymb) return dense_typed<kSymb>(a, p, grid, st);
+    if (mode == kNumExact) return dense_typed<kNumExact>(a, p, grid, st);
+    return dense_typed<kNumBook>(a, p, grid, st);
 }
 
 cudaError_t launch_direct_rows(const DirectRowArgs& a, const RowParams& p, int mode,

@@ -1,0 +1,103 @@
+"""The CTA-per-row direct kernel (rowdense.cuh): column ranges split across a
+CTA's warps, dense shared-memory accumulators, first-touch order rebuilt by
+sorting flat product positions.  Its results must be bit-identical to the
+reference's direct product (the oracle) and to the warp-per-row kernels, in
+every flavour and value type, including rows it cannot hold (an R*A row of
+more than 4096 columns, or a C row spanning more than 8192 columns), which go
+to the retry launch."""
+import numpy as np
+import pytest
+
+import oracle as O
+import sp3mm4amg_b200 as S
+from sp3mm4amg_b200 import problems as pb
+
+pytestmark = pytest.mark.gpu
+
+DENSE = 512
+
+
+def _same(got, want, what):
+    cmp = O.compare(got, want, rtol=1e-12)
+    assert cmp["ok"], (what, cmp)
+    assert cmp["bitwise_equal"] == want.nnz, (what, cmp)
+
+
+def _direct_all_ways(ctx, orc, R, A, P, what, vt=S.F64):
+    want = orc.sp3mm_direct(R, A, P)
+    d = [ctx.upload(m, val_type=vt) for m in (R, A, P)]
+    got = {}
+    for lanes in (0, 32, DENSE):
+        ctx.set_tuning(lanes, -1, -1)
+        for fl in (S.UB, S.SYMBNUM):
+            C = ctx.rap(*d, S.DIRECT, fl)
+            got[(lanes, fl)] = C.download()
+            C.free()
+    ctx.set_tuning(0, -1, -1)
+    for m in d:
+        m.free()
+    if vt == S.F64:
+        for k, c in got.items():
+            _same(c, want, (what, k))
+    base = got[(32, S.UB)]
+    for k, c in got.items():
+        assert np.array_equal(c.indptr, base.indptr), (what, k)
+        assert np.array_equal(c.indices, base.indices), (what, k)
+        assert np.array_equal(np.asarray(c.data).view(np.int64),
+                              np.asarray(base.data).view(np.int64)), (what, k)
+
+
+def test_golden_and_random(golden, orc):
+    with S.Context() as ctx:
+        for name, g in golden.items():
+            _direct_all_ways(ctx, orc, g["R"], g["A"], g["P"], name)
+        for seed in (3, 4):
+            R = pb.random_sparse(40, 300, 0.2, seed=seed, empty_rows=0.1)
+            A = pb.random_sparse(300, 900, 0.05, seed=seed + 1, empty_rows=0.1)
+            P = pb.random_sparse(900, 120, 0.06, seed=seed + 2, empty_rows=0.1)
+            _direct_all_ways(ctx, orc, R, A, P, ("random", seed))
+
+
+def test_coarse_level_of_a_hierarchy(orc):
+    # The second level of a 32^3 hierarchy: 512 rows whose R*A rows have
+    # about 2,000 of 4,096 columns -- the case the kernel is for.
+    dims = (32, 32, 32)
+    A0 = pb.poisson3d(*dims)
+    with S.Context() as ctx:
+        dA0 = ctx.upload(A0)
+        h = ctx.hierarchy(dA0, dims, min_coarse=64)
+        A1, P1, R1 = h.level(1)
+        R, A, P = R1.download(), A1.download(), P1.download()
+        h.free()
+        dA0.free()
+        _direct_all_ways(ctx, orc, R, A, P, "level1")
+        _direct_all_ways(ctx, orc, R, A, P, "level1 f32", vt=S.F32)
+
+
+def test_rows_beyond_the_slice_are_retried(orc):
+    rng = np.random.default_rng(5)
+    # Wide: R*A rows with more than 4096 distinct columns.
+    R = pb.random_sparse(6, 400, 0.9, seed=11)
+    A = pb.random_sparse(400, 20000, 0.02, seed=12)
+    P = pb.random_sparse(20000, 64, 0.05, seed=13)
+    # R*A rows spanning several 8192-column slices but holding fewer than
+    # 4096 columns: the slices are walked one after another.
+    Rm = pb.random_sparse(6, 400, 0.5, seed=16)
+    Am = pb.random_sparse(400, 30000, 0.0005, seed=17)
+    Pm_ = pb.random_sparse(30000, 64, 0.05, seed=18)
+    with S.Context() as ctx:
+        _direct_all_ways(ctx, orc, R, A, P, "wide R*A")
+        _direct_all_ways(ctx, orc, Rm, Am, Pm_, "multi-slice R*A")
+    # Far apart: C rows spanning more than 8192 columns (and R*A spans of
+    # several slices).
+    n = 3000
+    cols = np.stack([rng.integers(0, 50, n), rng.integers(20000, 20050, n)], 1)
+    import scipy.sparse as sp
+    Pm = sp.csr_matrix((rng.uniform(0.5, 1.5, 2 * n), cols.ravel(),
+                        np.arange(0, 2 * n + 1, 2)), shape=(n, 20050))
+    Pm.sort_indices()
+    P2 = pb.CSR(Pm.indptr, Pm.indices, Pm.data, Pm.shape)
+    A2 = pb.random_sparse(n, n, 0.01, seed=14)
+    R2 = pb.random_sparse(20, n, 0.3, seed=15)
+    with S.Context() as ctx:
+        _direct_all_ways(ctx, orc, R2, A2, P2, "wide C span")

@@ -130,10 +130,11 @@ def test_random_rectangular_all_variants(orc, seed):
             assert_same(ctx.rap(dR, dA, dP, S.PAIR_RIGHT, fl).download(), right)
 
 
-@pytest.mark.parametrize("lanes", [4, 8, 16, 32])
+@pytest.mark.parametrize("lanes", [4, 8, 16, 32, 512])
 def test_results_do_not_depend_on_tuning(golden, orc, lanes):
-    # Every lanes-per-row instantiation, and table shifts from generous to
-    # tiny (d1 = 8 forces nearly every row through the overflow/retry path).
+    # Every lanes-per-row instantiation (512: a CTA per direct row), and
+    # table shifts from generous to tiny (d1 = 8 forces nearly every row
+    # through the overflow/retry path).
     g = golden["poisson2d_64_agg2"]
     R, A, P = _random_triple(7)
     want_r = (orc.sp3mm_pair(R, A, P), orc.sp3mm_direct(R, A, P))
