@@ -142,6 +142,7 @@ struct BatchTier {
     int scap = 0;
     int slack = 0;           // numeric: tables 2^slack times the exact size
     bool gt = false;
+    bool dense = false;      // one CTA per row, dense accumulators (heavy direct rows)
     int block = 0, grid = 0;
     size_t smem = 0;
 };
@@ -206,6 +207,10 @@ int batch_fail(sp3mm_batch* b, int code, const char* msg) {
 
 namespace {
 
+// Rows binned to tables of at least this many slots (thousands of distinct
+// columns) run on the CTA-per-row kernel in all-direct batches.
+constexpr int kBatchDenseMinSlots = 2048;
+
 // Tiers over the non-empty levels of `bins`.  A tier's tables hold
 // 32 << (its top level + extra) slots per warp (extra: the numeric slack,
 // or the symbolic shift d1 so that a proven-size retry still fits).  Tiers
@@ -220,6 +225,12 @@ int make_tiers(sp3mm_batch* b, const Bins& bins, int mode, int extra, int tv, in
     gt.gt = true;
     gt.lo = kLevels;
     gt.hi = -1;
+    // Heavy levels of an all-direct batch run one CTA per row (symbolic and
+    // booked passes, which have retry rounds for rows it cannot hold).
+    bool all_direct = !b->items.empty();
+    for (const BItem& I : b->items) all_direct = all_direct && I.kind == kBatchDirect;
+    const bool dense_ok = all_direct && mode != kNumExact &&
+                          batch_dense_smem() + 1024 <= ctx->smem_optin;
     auto tier_of = [&](int L) {
         if (b->auto_split) return L;
         int t = 0;
@@ -250,6 +261,15 @@ int make_tiers(sp3mm_batch* b, const Bins& bins, int mode, int extra, int tv, in
         }
         const int top = std::min(t.hi + ex, 30 - 5);
         t.scap = 32 << top;
+        if (dense_ok && (32 << std::min(t.hi, 25)) >= kBatchDenseMinSlots) {
+            t.dense = true;
+            t.block = 512;
+            t.smem = batch_dense_smem();
+            t.grid = static_cast<int>(std::min<long long>(t.count, ctx->num_sms));
+            out.push_back(t);
+            L = M;
+            continue;
+        }
         const size_t bytes = batch_row_region_bytes(num, t.scap);
         if (bytes > std::min(ctx->smem_optin, b->smem_tier_max)) {
             // Global-memory tier: extend it (levels are visited ascending).
@@ -330,8 +350,12 @@ int run_tiers(sp3mm_batch* b, int mode, const std::vector<BatchTier>& tiers, con
             p.gstride = static_cast<long long>(t.smem);
             smem = 0;
         }
-        CK(ctx, launch_batch_rows(mode, t.gt, b->tv, b->to, t.grid, t.block, smem, s,
-                                  b->d_items.as<BItem>(), b->d_row_item.as<int>(), p));
+        if (t.dense)
+            CK(ctx, launch_batch_dense(mode, b->tv, b->to, t.grid, s, b->d_items.as<BItem>(),
+                                       b->d_row_item.as<int>(), p));
+        else
+            CK(ctx, launch_batch_rows(mode, t.gt, b->tv, b->to, t.grid, t.block, smem, s,
+                                      b->d_items.as<BItem>(), b->d_row_item.as<int>(), p));
         if (k > 0) {
             CK(ctx, cudaEventRecord(b->events[k], s));
             CK(ctx, cudaStreamWaitEvent(st, b->events[k], 0));

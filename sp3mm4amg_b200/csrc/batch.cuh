@@ -58,6 +58,11 @@ cudaError_t launch_batch_rows(int mode, bool gt, int tv, int to, int grid, int b
                               size_t smem, cudaStream_t st, const BItem* items,
                               const int* row_item, const BatchRowParams& p);
 size_t batch_row_region_bytes(bool num, int scap);
+// Heavy direct rows of a batch, one CTA of 512 threads per row (symbolic or
+// booked pass); batch_dense_smem(): its dynamic shared memory per CTA.
+cudaError_t launch_batch_dense(int mode, int tv, int to, int grid, cudaStream_t st,
+                               const BItem* items, const int* row_item, const BatchRowParams& p);
+size_t batch_dense_smem();
 // Release a planned, executed batch's planning state and graph; its
 // results stay valid, execute is no longer possible.
 void batch_trim(::sp3mm_batch* b);

@@ -198,211 +198,266 @@ __device__ __forceinline__ void block_span(int lo, int hi, int* slo, int* shi) {
     }
 }
 
+// Shared state of a dense CTA (the dynamic region carved up, plus the
+// block's scalars).
+struct DenseSmem {
+    double* acc;
+    int* ftq;
+    unsigned long long* sorted;
+    int* lkey;
+    int* lq;
+    double* lval;
+    unsigned char* touched;
+    int* sk;
+    int* sq;
+    double* sv;
+    int* s_n1;
+    int* s_lo;
+    int* s_hi;
+    int* s_cnt;
+    long long* s_base;
+};
+
+__device__ __forceinline__ DenseSmem dense_smem(unsigned char* smem, int* s_n1, int* s_lo,
+                                                int* s_hi, int* s_cnt, long long* s_base) {
+    DenseSmem d;
+    d.acc = reinterpret_cast<double*>(smem);
+    d.ftq = reinterpret_cast<int*>(d.acc + kDSpan);
+    d.sorted = reinterpret_cast<unsigned long long*>(d.ftq);
+    d.lkey = d.ftq + kDSpan;
+    d.lq = d.lkey + kDList;
+    d.lval = reinterpret_cast<double*>(d.lq + kDList);
+    d.touched = reinterpret_cast<unsigned char*>(d.lval + kDList);
+    unsigned char* wst = d.touched + kDSpan + static_cast<size_t>(threadIdx.x >> 5) * kStage * 16;
+    d.sk = reinterpret_cast<int*>(wst);
+    d.sq = d.sk + kStage;
+    d.sv = reinterpret_cast<double*>(d.sq + kStage);
+    d.s_n1 = s_n1;
+    d.s_lo = s_lo;
+    d.s_hi = s_hi;
+    d.s_cnt = s_cnt;
+    d.s_base = s_base;
+    return d;
+}
+
+__device__ __forceinline__ void dense_clear(const DenseSmem& d) {
+    for (int s = threadIdx.x; s < kDSpan; s += blockDim.x) {
+        d.acc[s] = 0.0;
+        d.touched[s] = 0;
+    }
+}
+
+// One output row of C = R*A*P (row `row` of R) by the whole CTA.  `finish`
+// runs on thread 0 once the counts are known: finish(n1, n2, fail) returns
+// the output offset of the row, or -1 when nothing is to be written (the
+// symbolic pass, a failed row, a flagged error).  Leaves the dense slice
+// clear.
+template <int MODE, typename TV, typename TO, class Finish>
+__device__ __forceinline__ void dense_row(const DenseSmem& d, const CsrView& R, const CsrView& A,
+                                          const CsrView& P, int row, int* oc, TO* ov,
+                                          Finish&& finish) {
+    constexpr bool NUM = MODE != kSymb;
+    const int lane = threadIdx.x & 31;
+    const int wid = threadIdx.x >> 5;
+    const unsigned lt = lanemask_lt();
+    const TV* rv = static_cast<const TV*>(R.v);
+    const TV* av = static_cast<const TV*>(A.v);
+    const TV* pv = static_cast<const TV*>(P.v);
+    const int rb = __ldg(R.rp + row);
+    const int rlen = __ldg(R.rp + row + 1) - rb;
+    if (threadIdx.x == 0) {
+        *d.s_n1 = 0;
+        *d.s_lo = INT_MAX;
+        *d.s_hi = -1;
+    }
+    __syncthreads();
+    // Stage-1 span: the A rows' first and last columns.
+    int lo = INT_MAX, hi = -1;
+    for (int t = threadIdx.x; t < rlen; t += blockDim.x) {
+        const int k = __ldg(R.ci + rb + t);
+        const int ab = __ldg(A.rp + k), ae = __ldg(A.rp + k + 1);
+        if (ab < ae) {
+            lo = min(lo, __ldg(A.ci + ab));
+            hi = max(hi, __ldg(A.ci + ae - 1));
+        }
+    }
+    block_span(lo, hi, d.s_lo, d.s_hi);
+    __syncthreads();
+    const int lo1 = *d.s_lo, hi1 = *d.s_hi;
+    const LeftG<TV> L1{R.ci, rv, rb};
+    for (long long c0 = lo1; c0 <= hi1; c0 += kDSpan) {
+        const int cb = static_cast<int>(c0);
+        const int ce = static_cast<int>(min(static_cast<long long>(hi1) + 1, c0 + kDSpan));
+        const int width = (ce - cb + kDWarps - 1) / kDWarps;
+        const int wlo = min(ce, cb + wid * width), whi = min(ce, wlo + width);
+        daccumulate<NUM, true>(L1, rlen, A.rp, A.ci, av, wlo, whi, cb, d.acc, d.touched, d.ftq,
+                               d.sk, d.sq, d.sv);
+        __syncthreads();
+        // List this warp's touched columns (value and first touch) and
+        // clear them.
+        for (int s0 = wlo; s0 < whi; s0 += 32) {
+            const int col = s0 + lane;
+            const bool hit = col < whi && d.touched[col - cb];
+            const unsigned b = __ballot_sync(kFull, hit);
+            int pos0 = 0;
+            if (lane == 0 && b) pos0 = atomicAdd(d.s_n1, __popc(b));
+            pos0 = __shfl_sync(kFull, pos0, 0);
+            if (hit) {
+                const int slot = col - cb;
+                const int pos = pos0 + __popc(b & lt);
+                if (pos < kDList) {
+                    d.lkey[pos] = col;
+                    d.lq[pos] = d.ftq[slot];
+                    if (NUM) d.lval[pos] = d.acc[slot];
+                }
+                d.touched[slot] = 0;
+                if (NUM) d.acc[slot] = 0.0;
+            }
+        }
+        __syncthreads();
+    }
+    const int n1 = *d.s_n1;
+    bool fail = n1 > kDList;
+    // First-touch order: sort (position, index) keys.
+    if (!fail && n1 > 1) {
+        const int P2 = static_cast<int>(next_pow2(static_cast<unsigned>(n1)));
+        for (int i = threadIdx.x; i < P2; i += blockDim.x)
+            d.sorted[i] = i < n1 ? (static_cast<unsigned long long>(static_cast<unsigned>(d.lq[i]))
+                                    << 32) | static_cast<unsigned>(i)
+                                 : ~0ULL;
+        __syncthreads();
+        for (int k = 2; k <= P2; k <<= 1) {
+            for (int j = k >> 1; j > 0; j >>= 1) {
+                for (int i = threadIdx.x; i < P2; i += blockDim.x) {
+                    const int ixj = i ^ j;
+                    if (ixj > i) {
+                        const unsigned long long x = d.sorted[i], y = d.sorted[ixj];
+                        if ((x > y) == ((i & k) == 0)) {
+                            d.sorted[i] = y;
+                            d.sorted[ixj] = x;
+                        }
+                    }
+                }
+                __syncthreads();
+            }
+        }
+    } else if (!fail && n1 == 1 && threadIdx.x == 0) {
+        d.sorted[0] = 0;
+    }
+    if (threadIdx.x == 0) {
+        *d.s_lo = INT_MAX;
+        *d.s_hi = -1;
+    }
+    __syncthreads();
+    // Stage-2 span: the P rows' first and last columns.
+    lo = INT_MAX;
+    hi = -1;
+    if (!fail) {
+        for (int t = threadIdx.x; t < n1; t += blockDim.x) {
+            const int c = d.lkey[t];
+            const int pb = __ldg(P.rp + c), pe = __ldg(P.rp + c + 1);
+            if (pb < pe) {
+                lo = min(lo, __ldg(P.ci + pb));
+                hi = max(hi, __ldg(P.ci + pe - 1));
+            }
+        }
+    }
+    block_span(lo, hi, d.s_lo, d.s_hi);
+    __syncthreads();
+    const int lo2 = *d.s_lo, hi2 = *d.s_hi;
+    if (hi2 >= lo2 && static_cast<long long>(hi2) - lo2 + 1 > kDSpan) fail = true;
+    const bool run2 = !fail && hi2 >= lo2;
+    int wlo2 = 0, whi2 = 0;
+    if (run2) {
+        const int width = (hi2 + 1 - lo2 + kDWarps - 1) / kDWarps;
+        wlo2 = min(hi2 + 1, lo2 + wid * width);
+        whi2 = min(hi2 + 1, wlo2 + width);
+        const LeftSorted L2{d.sorted, d.lkey, d.lval};
+        daccumulate<NUM, false>(L2, n1, P.rp, P.ci, pv, wlo2, whi2, lo2, d.acc, d.touched,
+                                nullptr, d.sk, d.sq, d.sv);
+    }
+    __syncthreads();
+    int cnt = 0;
+    if (run2) {
+        for (int s0 = wlo2; s0 < whi2; s0 += 32) {
+            const int col = s0 + lane;
+            cnt += __popc(__ballot_sync(kFull, col < whi2 && d.touched[col - lo2]));
+        }
+    }
+    if (lane == 0) d.s_cnt[wid] = cnt;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        int n2 = 0;
+        for (int w = 0; w < kDWarps; ++w) n2 += d.s_cnt[w];
+        *d.s_base = finish(n1, n2, fail);
+    }
+    __syncthreads();
+    if (run2) {
+        // Write this warp's columns in order and clear the slice.
+        const long long base = *d.s_base;
+        long long wpos = base;
+        for (int w = 0; w < wid; ++w) wpos += d.s_cnt[w];
+        for (int s0 = wlo2; s0 < whi2; s0 += 32) {
+            const int col = s0 + lane;
+            const bool hit = col < whi2 && d.touched[col - lo2];
+            const unsigned b = __ballot_sync(kFull, hit);
+            if (hit) {
+                const int slot = col - lo2;
+                if (NUM && base >= 0) {
+                    const long long o = wpos + __popc(b & lt);
+                    oc[o] = col;
+                    stv(ov, o, d.acc[slot]);
+                }
+                d.touched[slot] = 0;
+                if (NUM) d.acc[slot] = 0.0;
+            }
+            wpos += __popc(b);
+        }
+    }
+    __syncthreads();
+}
+
 template <int MODE, typename TV, typename TO>
 __global__ void __launch_bounds__(kDWarps * 32, 1) k_direct_dense(DirectRowArgs a, RowParams p) {
-    constexpr bool NUM = MODE != kSymb;
     extern __shared__ __align__(16) unsigned char smem[];
     __shared__ int s_n1, s_lo, s_hi, s_cnt[kDWarps];
     __shared__ long long s_base;
-    double* acc = reinterpret_cast<double*>(smem);
-    int* ftq = reinterpret_cast<int*>(acc + kDSpan);
-    unsigned long long* sorted = reinterpret_cast<unsigned long long*>(ftq);
-    int* lkey = ftq + kDSpan;
-    int* lq = lkey + kDList;
-    double* lval = reinterpret_cast<double*>(lq + kDList);
-    unsigned char* touched = reinterpret_cast<unsigned char*>(lval + kDList);
-    const int lane = threadIdx.x & 31;
-    const int wid = threadIdx.x >> 5;
-    unsigned char* wst = touched + kDSpan + static_cast<size_t>(wid) * kStage * 16;
-    int* sk = reinterpret_cast<int*>(wst);
-    int* sq = sk + kStage;
-    double* sv = reinterpret_cast<double*>(sq + kStage);
-    const unsigned lt = lanemask_lt();
-    for (int s = threadIdx.x; s < kDSpan; s += blockDim.x) {
-        acc[s] = 0.0;
-        touched[s] = 0;
-    }
-    const TV* rv = static_cast<const TV*>(a.R.v);
-    const TV* av = static_cast<const TV*>(a.A.v);
-    const TV* pv = static_cast<const TV*>(a.P.v);
-
+    const DenseSmem d = dense_smem(smem, &s_n1, &s_lo, &s_hi, s_cnt, &s_base);
+    dense_clear(d);
+    int* oc = MODE == kNumBook ? p.ub_ci : p.c_ci;
+    TO* ov = static_cast<TO*>(MODE == kNumBook ? p.ub_v : p.c_v);
     for (long long it = blockIdx.x; it < p.nrows; it += gridDim.x) {
         const int row = p.rows[it];
-        const int rb = __ldg(a.R.rp + row);
-        const int rlen = __ldg(a.R.rp + row + 1) - rb;
-        if (threadIdx.x == 0) {
-            s_n1 = 0;
-            s_lo = INT_MAX;
-            s_hi = -1;
-        }
-        __syncthreads();
-        // Stage-1 span: the A rows' first and last columns.
-        int lo = INT_MAX, hi = -1;
-        for (int t = threadIdx.x; t < rlen; t += blockDim.x) {
-            const int k = __ldg(a.R.ci + rb + t);
-            const int ab = __ldg(a.A.rp + k), ae = __ldg(a.A.rp + k + 1);
-            if (ab < ae) {
-                lo = min(lo, __ldg(a.A.ci + ab));
-                hi = max(hi, __ldg(a.A.ci + ae - 1));
-            }
-        }
-        block_span(lo, hi, &s_lo, &s_hi);
-        __syncthreads();
-        const int lo1 = s_lo, hi1 = s_hi;
-        const LeftG<TV> L1{a.R.ci, rv, rb};
-        for (long long c0 = lo1; c0 <= hi1; c0 += kDSpan) {
-            const int cb = static_cast<int>(c0);
-            const int ce = static_cast<int>(min(static_cast<long long>(hi1) + 1, c0 + kDSpan));
-            const int width = (ce - cb + kDWarps - 1) / kDWarps;
-            const int wlo = min(ce, cb + wid * width), whi = min(ce, wlo + width);
-            daccumulate<NUM, true>(L1, rlen, a.A.rp, a.A.ci, av, wlo, whi, cb, acc, touched, ftq,
-                                   sk, sq, sv);
-            __syncthreads();
-            // List this warp's touched columns (value and first touch) and
-            // clear them.
-            for (int s0 = wlo; s0 < whi; s0 += 32) {
-                const int col = s0 + lane;
-                const bool hit = col < whi && touched[col - cb];
-                const unsigned b = __ballot_sync(kFull, hit);
-                int pos0 = 0;
-                if (lane == 0 && b) pos0 = atomicAdd(&s_n1, __popc(b));
-                pos0 = __shfl_sync(kFull, pos0, 0);
-                if (hit) {
-                    const int slot = col - cb;
-                    const int pos = pos0 + __popc(b & lt);
-                    if (pos < kDList) {
-                        lkey[pos] = col;
-                        lq[pos] = ftq[slot];
-                        if (NUM) lval[pos] = acc[slot];
-                    }
-                    touched[slot] = 0;
-                    if (NUM) acc[slot] = 0.0;
-                }
-            }
-            __syncthreads();
-        }
-        const int n1 = s_n1;
-        bool fail = n1 > kDList;
-        // First-touch order: sort (position, index) keys.
-        if (!fail && n1 > 1) {
-            const int P2 = static_cast<int>(next_pow2(static_cast<unsigned>(n1)));
-            for (int i = threadIdx.x; i < P2; i += blockDim.x)
-                sorted[i] = i < n1 ? (static_cast<unsigned long long>(static_cast<unsigned>(lq[i]))
-                                      << 32) | static_cast<unsigned>(i)
-                                   : ~0ULL;
-            __syncthreads();
-            for (int k = 2; k <= P2; k <<= 1) {
-                for (int j = k >> 1; j > 0; j >>= 1) {
-                    for (int i = threadIdx.x; i < P2; i += blockDim.x) {
-                        const int ixj = i ^ j;
-                        if (ixj > i) {
-                            const unsigned long long x = sorted[i], y = sorted[ixj];
-                            if ((x > y) == ((i & k) == 0)) {
-                                sorted[i] = y;
-                                sorted[ixj] = x;
-                            }
-                        }
-                    }
-                    __syncthreads();
-                }
-            }
-        } else if (!fail && n1 == 1 && threadIdx.x == 0) {
-            sorted[0] = 0;
-        }
-        if (threadIdx.x == 0) {
-            s_lo = INT_MAX;
-            s_hi = -1;
-        }
-        __syncthreads();
-        // Stage-2 span: the P rows' first and last columns.
-        lo = INT_MAX;
-        hi = -1;
-        if (!fail) {
-            for (int t = threadIdx.x; t < n1; t += blockDim.x) {
-                const int c = lkey[t];
-                const int pb = __ldg(a.P.rp + c), pe = __ldg(a.P.rp + c + 1);
-                if (pb < pe) {
-                    lo = min(lo, __ldg(a.P.ci + pb));
-                    hi = max(hi, __ldg(a.P.ci + pe - 1));
-                }
-            }
-        }
-        block_span(lo, hi, &s_lo, &s_hi);
-        __syncthreads();
-        const int lo2 = s_lo, hi2 = s_hi;
-        if (hi2 >= lo2 && static_cast<long long>(hi2) - lo2 + 1 > kDSpan) fail = true;
-        const bool run2 = !fail && hi2 >= lo2;
-        int wlo2 = 0, whi2 = 0;
-        if (run2) {
-            const int width = (hi2 + 1 - lo2 + kDWarps - 1) / kDWarps;
-            wlo2 = min(hi2 + 1, lo2 + wid * width);
-            whi2 = min(hi2 + 1, wlo2 + width);
-            const LeftSorted L2{sorted, lkey, lval};
-            daccumulate<NUM, false>(L2, n1, a.P.rp, a.P.ci, pv, wlo2, whi2, lo2, acc, touched,
-                                    nullptr, sk, sq, sv);
-        }
-        __syncthreads();
-        int cnt = 0;
-        if (run2) {
-            for (int s0 = wlo2; s0 < whi2; s0 += 32) {
-                const int col = s0 + lane;
-                cnt += __popc(__ballot_sync(kFull, col < whi2 && touched[col - lo2]));
-            }
-        }
-        if (lane == 0) s_cnt[wid] = cnt;
-        __syncthreads();
-        if (threadIdx.x == 0) {
-            long long base = -1;
-            int n2 = 0;
-            for (int w = 0; w < kDWarps; ++w) n2 += s_cnt[w];
+        dense_row<MODE, TV, TO>(d, a.R, a.A, a.P, row, oc, ov,
+                                [&](int n1, int n2, bool fail) -> long long {
             if (fail) {
                 if (p.retry_rows) p.retry_rows[atomicAdd(p.retry_count, 1)] = row;
                 else atomicOr(p.err, kErrTable);
-            } else if (MODE == kSymb) {
+                return -1;
+            }
+            if (MODE == kSymb) {
                 p.row_cnt[row] = n2;
                 if (p.row_cnt1) p.row_cnt1[row] = n1;
-            } else if (MODE == kNumBook) {
+                return -1;
+            }
+            if (MODE == kNumBook) {
                 const unsigned long long off =
                     n2 > 0 ? atomicAdd(p.cursor, static_cast<unsigned long long>(n2)) : 0ULL;
                 if (off + n2 > p.cap) {
                     atomicOr(p.err, kErrBook);
-                } else {
-                    p.row_off[row] = static_cast<long long>(off);
-                    p.row_cnt[row] = n2;
-                    base = static_cast<long long>(off);
+                    return -1;
                 }
-            } else {
-                const long long b = p.c_rp[row];
-                if (p.c_rp[row + 1] - b != n2) atomicOr(p.err, kErrCount);
-                else base = b;
+                p.row_off[row] = static_cast<long long>(off);
+                p.row_cnt[row] = n2;
+                return static_cast<long long>(off);
             }
-            s_base = base;
-        }
-        __syncthreads();
-        if (run2) {
-            // Write this warp's columns in order and clear the slice.
-            long long wpos = s_base;
-            for (int w = 0; w < wid; ++w) wpos += s_cnt[w];
-            int* oc = MODE == kNumBook ? p.ub_ci : p.c_ci;
-            TO* ov = static_cast<TO*>(MODE == kNumBook ? p.ub_v : p.c_v);
-            for (int s0 = wlo2; s0 < whi2; s0 += 32) {
-                const int col = s0 + lane;
-                const bool hit = col < whi2 && touched[col - lo2];
-                const unsigned b = __ballot_sync(kFull, hit);
-                if (hit) {
-                    const int slot = col - lo2;
-                    if (NUM && s_base >= 0) {
-                        const long long o = wpos + __popc(b & lt);
-                        oc[o] = col;
-                        stv(ov, o, acc[slot]);
-                    }
-                    touched[slot] = 0;
-                    if (NUM) acc[slot] = 0.0;
-                }
-                wpos += __popc(b);
+            const long long b = p.c_rp[row];
+            if (p.c_rp[row + 1] - b != n2) {
+                atomicOr(p.err, kErrCount);
+                return -1;
             }
-        }
-        __syncthreads();
+            return b;
+        });
     }
 }
 

@@ -208,3 +208,36 @@ def test_batch_rejects_bad_inputs():
             ctx.batch([(dA, dA), (dA32, dA32)])   # mixed value types
         with pytest.raises(S.Sp3mmError):
             ctx.batch([(dA, dA, dB)])             # Y.N != Z.M
+
+
+@pytest.mark.parametrize("flavour", [S.UB, S.SYMBNUM])
+@pytest.mark.parametrize("in_vt", [S.F64, S.F32])
+def test_batch_heavy_direct_rows(orc, flavour, in_vt):
+    # An all-direct batch holding a coarse-level product (the second level of
+    # a 32^3 hierarchy: R*A rows of about 2,000 columns), whose rows run on
+    # the CTA-per-row kernel, next to small products on the warp kernels --
+    # and a product whose R*A rows exceed the CTA's 4096-entry list (retried).
+    dims = (32, 32, 32)
+    A0 = pb.poisson3d(*dims)
+    with S.Context() as ctx:
+        dA0 = ctx.upload(A0)
+        h = ctx.hierarchy(dA0, dims, min_coarse=64)
+        A1, P1, R1 = h.level(1)
+        heavy = (R1.download(), A1.download(), P1.download())
+        h.free()
+        dA0.free()
+    wide = (pb.random_sparse(6, 400, 0.9, seed=11), pb.random_sparse(400, 20000, 0.02, seed=12),
+            pb.random_sparse(20000, 64, 0.05, seed=13))
+    specs = [heavy, wide] + [s for s in _problems()[:3]]
+    if in_vt == S.F32:
+        specs = [tuple(_f32(m) for m in s) for s in specs]
+    wants = [orc.sp3mm_direct(*s) for s in specs]
+    with S.Context() as ctx:
+        got, info = _run(ctx, specs, in_vt=in_vt, out_vt=in_vt, flavour=flavour)
+    for g, w in zip(got, wants):
+        if in_vt == S.F64:
+            _same(g, w)
+        else:
+            assert np.array_equal(g.indptr, w.indptr) and np.array_equal(g.indices, w.indices)
+            assert np.array_equal(np.asarray(g.data, np.float32),
+                                  np.asarray(w.data, np.float64).astype(np.float32))
