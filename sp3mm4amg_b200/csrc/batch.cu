@@ -210,6 +210,9 @@ namespace {
 // Rows binned to tables of at least this many slots (thousands of distinct
 // columns) run on the CTA-per-row kernel in all-direct batches.
 constexpr int kBatchDenseMinSlots = 2048;
+// Exact pass: table levels up to this size hold at most 3584 distinct R*A
+// columns per row, within the CTA's 4096-entry list.
+constexpr int kBatchDenseMaxSlots = 4096;
 
 // Tiers over the non-empty levels of `bins`.  A tier's tables hold
 // 32 << (its top level + extra) slots per warp (extra: the numeric slack,
@@ -225,12 +228,13 @@ int make_tiers(sp3mm_batch* b, const Bins& bins, int mode, int extra, int tv, in
     gt.gt = true;
     gt.lo = kLevels;
     gt.hi = -1;
-    // Heavy levels of an all-direct batch run one CTA per row (symbolic and
-    // booked passes, which have retry rounds for rows it cannot hold).
+    // Heavy levels of an all-direct batch run one CTA per row: in the
+    // symbolic and booked passes, whose retry rounds take the rows it cannot
+    // hold; in the exact numeric pass (no retries), the levels of at most
+    // kBatchDenseMaxSlots, whose exact counts fit its R*A list.
     bool all_direct = !b->items.empty();
     for (const BItem& I : b->items) all_direct = all_direct && I.kind == kBatchDirect;
-    const bool dense_ok = all_direct && mode != kNumExact &&
-                          batch_dense_smem() + 1024 <= ctx->smem_optin;
+    const bool dense_ok = all_direct && batch_dense_smem() + 1024 <= ctx->smem_optin;
     auto tier_of = [&](int L) {
         if (b->auto_split) return L;
         int t = 0;
@@ -261,7 +265,9 @@ int make_tiers(sp3mm_batch* b, const Bins& bins, int mode, int extra, int tv, in
         }
         const int top = std::min(t.hi + ex, 30 - 5);
         t.scap = 32 << top;
-        if (dense_ok && (32 << std::min(t.hi, 25)) >= kBatchDenseMinSlots) {
+        const long long slots = 32LL << std::min(t.hi, 25);
+        if (dense_ok && slots >= kBatchDenseMinSlots &&
+            (mode != kNumExact || slots <= kBatchDenseMaxSlots)) {
             t.dense = true;
             t.block = 512;
             t.smem = batch_dense_smem();

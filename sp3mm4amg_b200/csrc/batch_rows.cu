@@ -31,8 +31,9 @@ KFn pick(int mode, bool gt, int tv, int to) {
 }
 
 // Direct rows of a batch, one CTA per row with dense accumulators (the
-// rows of the batch's heavy levels; rowdense.cuh).  Symbolic and booked
-// passes only: a row it cannot hold joins the retry rounds of the plan.
+// rows of the batch's heavy levels; rowdense.cuh).  In the symbolic and
+// booked passes a row it cannot hold joins the retry rounds of the plan; the
+// exact numeric pass (the captured graph) gets only rows whose R*A list fits.
 template <int MODE, typename TV, typename TO>
 __global__ void __launch_bounds__(kDWarps * 32, 1)
     k_batch_dense(const BItem* __restrict__ items, const int* __restrict__ row_item,
@@ -53,8 +54,18 @@ __global__ void __launch_bounds__(kDWarps * 32, 1)
             continue;
         }
         const int i = static_cast<int>(g - I->row_base);
-        dense_row<MODE, TV, TO>(d, I->X, I->Y, I->Z, i, p.ub_ci, static_cast<TO*>(p.ub_v),
+        const long long eb = MODE == kNumExact ? __ldg(p.c_rp + g) : 0;
+        const long long ee = MODE == kNumExact ? eb + __ldg(p.cnt2 + g) : 0;
+        int* oc = MODE == kNumExact ? p.c_ci : p.ub_ci;
+        TO* ov = static_cast<TO*>(MODE == kNumExact ? p.c_v : p.ub_v);
+        dense_row<MODE, TV, TO>(d, I->X, I->Y, I->Z, i, oc, ov, eb, ee,
                                 [&](int n1, int n2, bool fail) -> long long {
+            if (MODE == kNumExact) {
+                // Routed only where the list fits; a count that differs
+                // from the plan's is an error, as in the warp kernels.
+                if (fail || n2 != ee - eb) atomicOr(p.err, kErrCount);
+                return -1;
+            }
             if (fail) {
                 batch_retry(p, g, __ldg(p.need + g));
                 return -1;
@@ -95,8 +106,9 @@ size_t batch_dense_smem() { return dense_smem_bytes(); }
 
 cudaError_t launch_batch_dense(int mode, int tv, int to, int grid, cudaStream_t st,
                                const BItem* items, const int* row_item, const BatchRowParams& p) {
-    if (mode != kSymb && mode != kNumBook) return cudaErrorInvalidValue;
-    const KFn f = mode == kSymb ? pick_dense_types<kSymb>(tv, to) : pick_dense_types<kNumBook>(tv, to);
+    const KFn f = mode == kSymb      ? pick_dense_types<kSymb>(tv, to)
+                  : mode == kNumBook ? pick_dense_types<kNumBook>(tv, to)
+                                     : pick_dense_types<kNumExact>(tv, to);
     const size_t smem = dense_smem_bytes();
     cudaError_t e = cudaFuncSetAttribute(reinterpret_cast<const void*>(f),
                                          cudaFuncAttributeMaxDynamicSharedMemorySize,

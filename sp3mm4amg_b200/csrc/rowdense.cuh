@@ -250,12 +250,13 @@ __device__ __forceinline__ void dense_clear(const DenseSmem& d) {
 // One output row of C = R*A*P (row `row` of R) by the whole CTA.  `finish`
 // runs on thread 0 once the counts are known: finish(n1, n2, fail) returns
 // the output offset of the row, or -1 when nothing is to be written (the
-// symbolic pass, a failed row, a flagged error).  Leaves the dense slice
-// clear.
+// symbolic pass, a failed row, a flagged error).  The exact numeric pass
+// writes the row to [ebase, eend) as it goes and calls finish at the end
+// to check the count.  Leaves the dense slice clear.
 template <int MODE, typename TV, typename TO, class Finish>
 __device__ __forceinline__ void dense_row(const DenseSmem& d, const CsrView& R, const CsrView& A,
                                           const CsrView& P, int row, int* oc, TO* ov,
-                                          Finish&& finish) {
+                                          long long ebase, long long eend, Finish&& finish) {
     constexpr bool NUM = MODE != kSymb;
     const int lane = threadIdx.x & 31;
     const int wid = threadIdx.x >> 5;
@@ -365,55 +366,68 @@ __device__ __forceinline__ void dense_row(const DenseSmem& d, const CsrView& R, 
     block_span(lo, hi, d.s_lo, d.s_hi);
     __syncthreads();
     const int lo2 = *d.s_lo, hi2 = *d.s_hi;
-    if (hi2 >= lo2 && static_cast<long long>(hi2) - lo2 + 1 > kDSpan) fail = true;
+    // The exact pass knows where the row goes: it walks the span in slices
+    // and writes each slice's columns in order.  The other passes must know
+    // the row's length before booking it: one slice, or the row is retried.
+    constexpr bool EXACT = MODE == kNumExact;
+    if (!EXACT && hi2 >= lo2 && static_cast<long long>(hi2) - lo2 + 1 > kDSpan) fail = true;
     const bool run2 = !fail && hi2 >= lo2;
-    int wlo2 = 0, whi2 = 0;
-    if (run2) {
-        const int width = (hi2 + 1 - lo2 + kDWarps - 1) / kDWarps;
-        wlo2 = min(hi2 + 1, lo2 + wid * width);
-        whi2 = min(hi2 + 1, wlo2 + width);
-        const LeftSorted L2{d.sorted, d.lkey, d.lval};
-        daccumulate<NUM, false>(L2, n1, P.rp, P.ci, pv, wlo2, whi2, lo2, d.acc, d.touched,
-                                nullptr, d.sk, d.sq, d.sv);
-    }
-    __syncthreads();
-    int cnt = 0;
-    if (run2) {
-        for (int s0 = wlo2; s0 < whi2; s0 += 32) {
-            const int col = s0 + lane;
-            cnt += __popc(__ballot_sync(kFull, col < whi2 && d.touched[col - lo2]));
+    const LeftSorted L2{d.sorted, d.lkey, d.lval};
+    long long running = 0;
+    for (long long c0 = lo2; run2 ? c0 <= hi2 : c0 == lo2; c0 += kDSpan) {
+        const int cb = static_cast<int>(c0);
+        const int ce = static_cast<int>(min(static_cast<long long>(hi2) + 1, c0 + kDSpan));
+        int wlo2 = 0, whi2 = 0;
+        if (run2) {
+            const int width = (ce - cb + kDWarps - 1) / kDWarps;
+            wlo2 = min(ce, cb + wid * width);
+            whi2 = min(ce, wlo2 + width);
+            daccumulate<NUM, false>(L2, n1, P.rp, P.ci, pv, wlo2, whi2, cb, d.acc, d.touched,
+                                    nullptr, d.sk, d.sq, d.sv);
         }
-    }
-    if (lane == 0) d.s_cnt[wid] = cnt;
-    __syncthreads();
-    if (threadIdx.x == 0) {
-        int n2 = 0;
-        for (int w = 0; w < kDWarps; ++w) n2 += d.s_cnt[w];
-        *d.s_base = finish(n1, n2, fail);
-    }
-    __syncthreads();
-    if (run2) {
-        // Write this warp's columns in order and clear the slice.
-        const long long base = *d.s_base;
-        long long wpos = base;
-        for (int w = 0; w < wid; ++w) wpos += d.s_cnt[w];
-        for (int s0 = wlo2; s0 < whi2; s0 += 32) {
-            const int col = s0 + lane;
-            const bool hit = col < whi2 && d.touched[col - lo2];
-            const unsigned b = __ballot_sync(kFull, hit);
-            if (hit) {
-                const int slot = col - lo2;
-                if (NUM && base >= 0) {
-                    const long long o = wpos + __popc(b & lt);
-                    oc[o] = col;
-                    stv(ov, o, d.acc[slot]);
-                }
-                d.touched[slot] = 0;
-                if (NUM) d.acc[slot] = 0.0;
+        __syncthreads();
+        int cnt = 0;
+        if (run2) {
+            for (int s0 = wlo2; s0 < whi2; s0 += 32) {
+                const int col = s0 + lane;
+                cnt += __popc(__ballot_sync(kFull, col < whi2 && d.touched[col - cb]));
             }
-            wpos += __popc(b);
         }
+        if (lane == 0) d.s_cnt[wid] = cnt;
+        __syncthreads();
+        int chunk_n = 0;
+        for (int w = 0; w < kDWarps; ++w) chunk_n += d.s_cnt[w];
+        if (!EXACT) {
+            if (threadIdx.x == 0) *d.s_base = finish(n1, chunk_n, fail);
+            __syncthreads();
+        }
+        if (run2) {
+            // Write this warp's columns in order and clear the slice.
+            const long long base = EXACT ? ebase + running : *d.s_base;
+            long long wpos = base;
+            for (int w = 0; w < wid; ++w) wpos += d.s_cnt[w];
+            for (int s0 = wlo2; s0 < whi2; s0 += 32) {
+                const int col = s0 + lane;
+                const bool hit = col < whi2 && d.touched[col - cb];
+                const unsigned b = __ballot_sync(kFull, hit);
+                if (hit) {
+                    const int slot = col - cb;
+                    const long long o = wpos + __popc(b & lt);
+                    if (NUM && base >= 0 && (!EXACT || o < eend)) {
+                        oc[o] = col;
+                        stv(ov, o, d.acc[slot]);
+                    }
+                    d.touched[slot] = 0;
+                    if (NUM) d.acc[slot] = 0.0;
+                }
+                wpos += __popc(b);
+            }
+        }
+        running += chunk_n;
+        __syncthreads();
+        if (!run2) break;
     }
+    if (EXACT && threadIdx.x == 0) finish(n1, static_cast<int>(running), fail);
     __syncthreads();
 }
 
@@ -428,7 +442,9 @@ __global__ void __launch_bounds__(kDWarps * 32, 1) k_direct_dense(DirectRowArgs 
     TO* ov = static_cast<TO*>(MODE == kNumBook ? p.ub_v : p.c_v);
     for (long long it = blockIdx.x; it < p.nrows; it += gridDim.x) {
         const int row = p.rows[it];
-        dense_row<MODE, TV, TO>(d, a.R, a.A, a.P, row, oc, ov,
+        const long long eb = MODE == kNumExact ? p.c_rp[row] : 0;
+        const long long ee = MODE == kNumExact ? p.c_rp[row + 1] : 0;
+        dense_row<MODE, TV, TO>(d, a.R, a.A, a.P, row, oc, ov, eb, ee,
                                 [&](int n1, int n2, bool fail) -> long long {
             if (fail) {
                 if (p.retry_rows) p.retry_rows[atomicAdd(p.retry_count, 1)] = row;
@@ -451,12 +467,8 @@ __global__ void __launch_bounds__(kDWarps * 32, 1) k_direct_dense(DirectRowArgs 
                 p.row_cnt[row] = n2;
                 return static_cast<long long>(off);
             }
-            const long long b = p.c_rp[row];
-            if (p.c_rp[row + 1] - b != n2) {
-                atomicOr(p.err, kErrCount);
-                return -1;
-            }
-            return b;
+            if (ee - eb != n2) atomicOr(p.err, kErrCount);
+            return -1;
         });
     }
 }

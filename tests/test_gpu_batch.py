@@ -241,3 +241,33 @@ def test_batch_heavy_direct_rows(orc, flavour, in_vt):
             assert np.array_equal(g.indptr, w.indptr) and np.array_equal(g.indices, w.indices)
             assert np.array_equal(np.asarray(g.data, np.float32),
                                   np.asarray(w.data, np.float64).astype(np.float32))
+
+
+def test_batch_heavy_rows_replay_new_values(orc):
+    # The exact numeric graph (replays) runs the heavy levels on the
+    # CTA-per-row kernel too; new operand values, same patterns.
+    dims = (32, 32, 32)
+    A0 = pb.poisson3d(*dims)
+    rng = np.random.default_rng(9)
+    with S.Context() as ctx:
+        dA0 = ctx.upload(A0)
+        h = ctx.hierarchy(dA0, dims, min_coarse=64)
+        A1, P1, R1 = h.level(1)
+        heavy = (R1.download(), A1.download(), P1.download())
+        h.free()
+        dA0.free()
+        probs = [heavy] + _problems()[:2]
+        dev = [tuple(ctx.upload(m) for m in s) for s in probs]
+        b = ctx.batch(dev)
+        b.run()
+        for _ in range(2):
+            newA = []
+            for (R, A, P), (dR, dA, dP) in zip(probs, dev):
+                A2 = pb.CSR(A.indptr, A.indices, A.data * rng.uniform(0.5, 2.0, A.nnz), A.shape)
+                dA.set_values(A2.data)
+                newA.append(A2)
+            b.execute()
+            ctx.sync()
+            for i, ((R, _, P), A2) in enumerate(zip(probs, newA)):
+                _same(b.result(i).download(), orc.sp3mm_direct(R, A2, P))
+        b.free()
