@@ -40,15 +40,17 @@ namespace sp3mm {
 constexpr int kDWarps = 16;    // warps per CTA (one output row per CTA)
 constexpr int kDSpan = 8192;   // columns of the dense accumulator slice
 constexpr int kDList = 4096;   // R*A row entries a CTA holds
+constexpr int kDHist = 1024;   // bins of the column histogram that balances the warps
+constexpr int kDSamples = 2048;   // columns sampled per stage for that histogram
 
 // Dynamic shared memory: acc double[kDSpan] | ftq int[kDSpan] (after stage 1:
 // u64 sort keys [kDList]) | lkey int[kDList] | lq int[kDList] |
 // lval double[kDList] | touched u8[kDSpan] | per warp: sk int[kStage],
-// sq int[kStage], sv double[kStage].
+// sq int[kStage], sv double[kStage] | hist int[kDHist] | total int.
 __host__ __device__ constexpr size_t dense_smem_bytes() {
     return static_cast<size_t>(kDSpan) * 8 + static_cast<size_t>(kDSpan) * 4 +
            static_cast<size_t>(kDList) * 16 + static_cast<size_t>(kDSpan) +
-           static_cast<size_t>(kDWarps) * kStage * 16;
+           static_cast<size_t>(kDWarps) * kStage * 16 + static_cast<size_t>(kDHist) * 4 + 16;
 }
 
 // First index in [b, e) whose column is >= x (columns ascending).
@@ -187,6 +189,15 @@ __device__ __forceinline__ void daccumulate(const Left& L, int n, const int* __r
     }
 }
 
+// Block-wide sum of `v` into *stot (zeroed by the caller before the barrier
+// that precedes this call).
+__device__ __forceinline__ void block_total(long long v, long long* stot) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(kFull, v, o);
+    if ((threadIdx.x & 31) == 0) atomicAdd(reinterpret_cast<unsigned long long*>(stot),
+                                           static_cast<unsigned long long>(v));
+}
+
 // Block-wide min / max of (lo, hi) into *slo / *shi (initialised by the
 // caller before the barrier that precedes this call).
 __device__ __forceinline__ void block_span(int lo, int hi, int* slo, int* shi) {
@@ -211,6 +222,8 @@ struct DenseSmem {
     int* sk;
     int* sq;
     double* sv;
+    int* hist;
+    long long* s_tot;
     int* s_n1;
     int* s_lo;
     int* s_hi;
@@ -232,6 +245,8 @@ __device__ __forceinline__ DenseSmem dense_smem(unsigned char* smem, int* s_n1, 
     d.sk = reinterpret_cast<int*>(wst);
     d.sq = d.sk + kStage;
     d.sv = reinterpret_cast<double*>(d.sq + kStage);
+    d.hist = reinterpret_cast<int*>(d.touched + kDSpan + static_cast<size_t>(kDWarps) * kStage * 16);
+    d.s_tot = reinterpret_cast<long long*>(d.hist + kDHist);
     d.s_n1 = s_n1;
     d.s_lo = s_lo;
     d.s_hi = s_hi;
@@ -245,6 +260,69 @@ __device__ __forceinline__ void dense_clear(const DenseSmem& d) {
         d.acc[s] = 0.0;
         d.touched[s] = 0;
     }
+}
+
+// Column ranges of the warps over [cb, ce) holding about equal numbers of
+// products: about kDSamples columns of the right rows (every st-th entry of
+// each from a hashed start, st from the stage's product count `total`) go
+// into a histogram of
+// kDHist bins, and warp w starts at the bin where the cumulative count
+// reaches w/kDWarps of the samples.  Any cover of [cb, ce) by disjoint
+// ranges gives the same results; this one gives the warps equal work.
+template <class Left>
+__device__ __forceinline__ void balanced_range(const DenseSmem& d, const Left& L, int n,
+                                               const int* __restrict__ b_rp,
+                                               const int* __restrict__ b_ci, int cb, int ce,
+                                               long long total, int& wlo, int& whi) {
+    const int lane = threadIdx.x & 31;
+    const int wid = threadIdx.x >> 5;
+    int shift = 0;
+    while ((static_cast<long long>(kDHist) << shift) < static_cast<long long>(ce) - cb) ++shift;
+    for (int b = threadIdx.x; b < kDHist; b += blockDim.x) d.hist[b] = 0;
+    __syncthreads();
+    const long long stl = (total + kDSamples - 1) / kDSamples;
+    const int st = static_cast<int>(stl < 1 ? 1 : (stl > INT_MAX ? INT_MAX : stl));
+    for (int t = threadIdx.x; t < n; t += blockDim.x) {
+        const int k = L.key(t);
+        const int ab = __ldg(b_rp + k), ae = __ldg(b_rp + k + 1);
+        // A hashed start per row: every entry is sampled with probability
+        // 1/st, also in rows shorter than st.
+        const unsigned h = static_cast<unsigned>(t) * 2654435761u;
+        for (long long e = ab + static_cast<int>(h % static_cast<unsigned>(st)); e < ae; e += st) {
+            const int col = __ldg(b_ci + e);
+            if (col >= cb && col < ce) atomicAdd(&d.hist[(col - cb) >> shift], 1);
+        }
+    }
+    __syncthreads();
+    if (wid == 0) {
+        // Inclusive prefix: lane l owns bins [32l, 32l + 32).
+        int local = 0;
+        for (int j = 0; j < 32; ++j) local += d.hist[lane * 32 + ((j + lane) & 31)];
+        int all;
+        int run = wscan_excl(local, all);
+        for (int j = 0; j < 32; ++j) {
+            run += d.hist[lane * 32 + j];
+            d.hist[lane * 32 + j] = run;
+        }
+    }
+    __syncthreads();
+    const int tot = d.hist[kDHist - 1];
+    auto bound = [&](int w) -> int {
+        if (w <= 0) return cb;
+        if (w >= kDWarps) return ce;
+        const int q = static_cast<int>((static_cast<long long>(tot) * w + kDWarps - 1) / kDWarps);
+        int a = 0, b = kDHist;
+        while (a < b) {
+            const int m = (a + b) >> 1;
+            if (d.hist[m] < q) a = m + 1;
+            else b = m;
+        }
+        const long long c = static_cast<long long>(cb) + (static_cast<long long>(a + 1) << shift);
+        return static_cast<int>(c < ce ? c : ce);
+    };
+    wlo = bound(wid);
+    whi = bound(wid + 1);
+    __syncthreads();
 }
 
 // One output row of C = R*A*P (row `row` of R) by the whole CTA.  `finish`
@@ -270,27 +348,32 @@ __device__ __forceinline__ void dense_row(const DenseSmem& d, const CsrView& R, 
         *d.s_n1 = 0;
         *d.s_lo = INT_MAX;
         *d.s_hi = -1;
+        *d.s_tot = 0;
     }
     __syncthreads();
     // Stage-1 span: the A rows' first and last columns.
     int lo = INT_MAX, hi = -1;
+    long long tot = 0;
     for (int t = threadIdx.x; t < rlen; t += blockDim.x) {
         const int k = __ldg(R.ci + rb + t);
         const int ab = __ldg(A.rp + k), ae = __ldg(A.rp + k + 1);
+        tot += ae - ab;
         if (ab < ae) {
             lo = min(lo, __ldg(A.ci + ab));
             hi = max(hi, __ldg(A.ci + ae - 1));
         }
     }
     block_span(lo, hi, d.s_lo, d.s_hi);
+    block_total(tot, d.s_tot);
     __syncthreads();
     const int lo1 = *d.s_lo, hi1 = *d.s_hi;
+    const long long tot1 = *d.s_tot;
     const LeftG<TV> L1{R.ci, rv, rb};
     for (long long c0 = lo1; c0 <= hi1; c0 += kDSpan) {
         const int cb = static_cast<int>(c0);
         const int ce = static_cast<int>(min(static_cast<long long>(hi1) + 1, c0 + kDSpan));
-        const int width = (ce - cb + kDWarps - 1) / kDWarps;
-        const int wlo = min(ce, cb + wid * width), whi = min(ce, wlo + width);
+        int wlo, whi;
+        balanced_range(d, L1, rlen, A.rp, A.ci, cb, ce, tot1, wlo, whi);
         daccumulate<NUM, true>(L1, rlen, A.rp, A.ci, av, wlo, whi, cb, d.acc, d.touched, d.ftq,
                                d.sk, d.sq, d.sv);
         __syncthreads();
@@ -348,15 +431,18 @@ __device__ __forceinline__ void dense_row(const DenseSmem& d, const CsrView& R, 
     if (threadIdx.x == 0) {
         *d.s_lo = INT_MAX;
         *d.s_hi = -1;
+        *d.s_tot = 0;
     }
     __syncthreads();
     // Stage-2 span: the P rows' first and last columns.
     lo = INT_MAX;
     hi = -1;
+    tot = 0;
     if (!fail) {
         for (int t = threadIdx.x; t < n1; t += blockDim.x) {
             const int c = d.lkey[t];
             const int pb = __ldg(P.rp + c), pe = __ldg(P.rp + c + 1);
+            tot += pe - pb;
             if (pb < pe) {
                 lo = min(lo, __ldg(P.ci + pb));
                 hi = max(hi, __ldg(P.ci + pe - 1));
@@ -364,8 +450,10 @@ __device__ __forceinline__ void dense_row(const DenseSmem& d, const CsrView& R, 
         }
     }
     block_span(lo, hi, d.s_lo, d.s_hi);
+    block_total(tot, d.s_tot);
     __syncthreads();
     const int lo2 = *d.s_lo, hi2 = *d.s_hi;
+    const long long tot2 = *d.s_tot;
     // The exact pass knows where the row goes: it walks the span in slices
     // and writes each slice's columns in order.  The other passes must know
     // the row's length before booking it: one slice, or the row is retried.
@@ -379,9 +467,7 @@ __device__ __forceinline__ void dense_row(const DenseSmem& d, const CsrView& R, 
         const int ce = static_cast<int>(min(static_cast<long long>(hi2) + 1, c0 + kDSpan));
         int wlo2 = 0, whi2 = 0;
         if (run2) {
-            const int width = (ce - cb + kDWarps - 1) / kDWarps;
-            wlo2 = min(ce, cb + wid * width);
-            whi2 = min(ce, wlo2 + width);
+            balanced_range(d, L2, n1, P.rp, P.ci, cb, ce, tot2, wlo2, whi2);
             daccumulate<NUM, false>(L2, n1, P.rp, P.ci, pv, wlo2, whi2, cb, d.acc, d.touched,
                                     nullptr, d.sk, d.sq, d.sv);
         }
