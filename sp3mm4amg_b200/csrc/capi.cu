@@ -114,12 +114,12 @@ int check_device_err(sp3mm_ctx* ctx) {
 }
 
 int bin_rows(sp3mm_ctx* ctx, int M, const int* need, int shift, int G, Counters* dcnt,
-             int* row_cnt, Bins& b) {
+             int* row_cnt, Bins& b, const int* est) {
     TRY(b.level.alloc(ctx, static_cast<size_t>(M) + 1));
     TRY(b.lists.alloc(ctx, sizeof(int) * (static_cast<size_t>(M) + 1)));
     prof(ctx, "bin.levels", [&] {
         launch_bin_levels(M, need, shift, G, b.level.as<signed char>(), dcnt->counts,
-                          &dcnt->nmax, row_cnt, ctx->stream);
+                          &dcnt->nmax, row_cnt, ctx->stream, est);
     });
     Counters h{};
     CK(ctx, cudaMemcpyAsync(&h, dcnt, sizeof h, cudaMemcpyDeviceToHost, ctx->stream));
@@ -413,12 +413,13 @@ int known_max_row(sp3mm_ctx* ctx, const sp3mm_dcsr& m, int* out) {
 // per row; s1_max/s2_max bound the tables of the retry launch.
 int product_rows(sp3mm_ctx* ctx, RowRunner& rr, int M, int N, int flavour, int out_vt,
                  DevBuf& need, Counters* dc, int G, int d1, int d2, long long s1_bound,
-                 long long s2_bound, double p_max_row, sp3mm_dcsr* C) {
+                 long long s2_bound, double p_max_row, sp3mm_dcsr* C,
+                 const int* est = nullptr) {
     const cudaStream_t st = ctx->stream;
     DevBuf row_cnt, row_cnt1, rp, ci, v;
     TRY(row_cnt.alloc(ctx, sizeof(int) * (static_cast<size_t>(M) + 1)));
     Bins bins;
-    TRY(bin_rows(ctx, M, need.as<int>(), d1, G, dc, row_cnt.as<int>(), bins));
+    TRY(bin_rows(ctx, M, need.as<int>(), d1, G, dc, row_cnt.as<int>(), bins, est));
     const long long s1_max = std::min<long long>(bins.nmax, s1_bound);
     const long long s2_max = std::min<long long>(
         static_cast<long long>(static_cast<double>(bins.nmax) * p_max_row), s2_bound);
@@ -513,7 +514,7 @@ int product_rows(sp3mm_ctx* ctx, RowRunner& rr, int M, int N, int flavour, int o
                 ub_v.release();
                 CK(ctx, cudaMemsetAsync(dc, 0, sizeof(Counters), st));
                 return product_rows(ctx, rr, M, N, SP3MM_SYMBNUM, out_vt, need, dc, G, d1, d2,
-                                     s1_bound, s2_bound, p_max_row, C);
+                                     s1_bound, s2_bound, p_max_row, C, est);
             }
             if (pass == 1 || tr.retry <= 0) break;
             TRY(rr.run_retry(p, tr.retry, retry, s1_max, s2_max));
@@ -580,18 +581,20 @@ int direct_impl(sp3mm_ctx* ctx, const sp3mm_dcsr& R, const sp3mm_dcsr& A, const 
     const int d2 = ctx->tune_d2 >= 0 ? ctx->tune_d2 : 0;
     int pmax = 0;
     TRY(known_max_row(ctx, P, &pmax));
-    DevBuf cnt_buf, need;
+    DevBuf cnt_buf, need, need_opt;
     TRY(cnt_buf.alloc(ctx, sizeof(Counters)));
     TRY(need.alloc(ctx, sizeof(int) * (static_cast<size_t>(M) + 1)));
+    TRY(need_opt.alloc(ctx, sizeof(int) * (static_cast<size_t>(M) + 1)));
     Counters* dc = cnt_buf.as<Counters>();
     CK(ctx, cudaMemsetAsync(dc, 0, sizeof(Counters), st));
     prof(ctx, "direct.bounds", [&] {
-        launch_direct_bounds(view(R), view(A), pmax, need.as<int>(), &dc->total, st);
+        launch_direct_bounds(view(R), view(A), pmax, need.as<int>(), &dc->total, st,
+                             need_opt.as<int>(), d1);
     });
     RowRunner rr{ctx, true, kSymb, DirectRowArgs{view(R), view(A), view(P)}, {}, A.max_row,
                  P.max_row};
     return product_rows(ctx, rr, M, P.N, flavour, out_vt, need, dc, G, d1, d2, A.N, P.N,
-                        static_cast<double>(pmax), C);
+                        static_cast<double>(pmax), C, need_opt.as<int>());
 }
 
 void free_dcsr_arrays(sp3mm_ctx* ctx, sp3mm_dcsr* m) {

@@ -151,10 +151,10 @@ size_t pool_idle_bytes(sp3mm_ctx* ctx);
 int read_err(sp3mm_ctx* ctx, unsigned* out);
 // Read and clear the sticky device error word; map it to a return code.
 int check_device_err(sp3mm_ctx* ctx);
-// Bin M rows by need[i] >> shift for groups of G lanes; `dcnt` is the
+// Bin M rows by need[i] >> shift (or est[i]) for groups of G lanes; `dcnt` is the
 // device counter block (its `total` was accumulated by the bounds kernel);
 // row_cnt of empty rows is zeroed when given.  Synchronises the stream once.
 int bin_rows(sp3mm_ctx* ctx, int M, const int* need, int shift, int G, Counters* dcnt,
-             int* row_cnt, Bins& b);
+             int* row_cnt, Bins& b, const int* est = nullptr);
 
 }  // namespace sp3mm

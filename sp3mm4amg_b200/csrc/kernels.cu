@@ -68,7 +68,8 @@ __global__ void __launch_bounds__(256) k_pair_bounds(CsrView A, CsrView B, int* 
 // entries).
 template <int G>
 __global__ void __launch_bounds__(256) k_direct_bounds(CsrView R, CsrView A, int p_max_row,
-                                                        int* need, unsigned long long* total) {
+                                                        int* need, int* need_opt, int d1,
+                                                        unsigned long long* total) {
     const Group<G> g;
     const int groups = (gridDim.x * blockDim.x) / G;
     unsigned long long mine = 0;
@@ -83,6 +84,18 @@ __global__ void __launch_bounds__(256) k_direct_bounds(CsrView R, CsrView A, int
         if (g.gl == 0) {
             const long long d = u1 < A.N ? u1 : A.N;
             need[row] = static_cast<int>(d < INT_MAX ? d : INT_MAX);
+            if (need_opt) {
+                // Optimistic first-table size: the bound >> d1, at most
+                // 8 sqrt(products) -- long R*A rows repeat their columns
+                // (stencil coarse levels: ~6 sqrt, kNN rows: <= 8.4 sqrt);
+                // a row that overflows is recomputed with the bound.
+                long long o = d >> d1;
+                const long long r =
+                    static_cast<long long>(ceil(8.0 * sqrt(static_cast<double>(u1))));
+                if (r < o) o = r;
+                if (d > 0 && o < 1) o = 1;
+                need_opt[row] = static_cast<int>(o < INT_MAX ? o : INT_MAX);
+            }
             mine += static_cast<unsigned long long>(u1) * static_cast<unsigned long long>(p_max_row);
         }
     }
@@ -120,9 +133,9 @@ int slots_for_need(long long need, int G) {
 }
 int level_for_need(long long need, int G) { return level_of(need, G); }
 
-__global__ void __launch_bounds__(256) k_bin_levels(int M, const int* need, int shift, int G,
-                                                     signed char* level, int* counts,
-                                                     int* nmax, int* row_cnt_zero) {
+__global__ void __launch_bounds__(256) k_bin_levels(int M, const int* need, const int* est,
+                                                     int shift, int G, signed char* level,
+                                                     int* counts, int* nmax, int* row_cnt_zero) {
     __shared__ int sc[kLevels + 1];
     __shared__ int smax;
     for (int i = threadIdx.x; i <= kLevels; i += blockDim.x) sc[i] = 0;
@@ -132,7 +145,7 @@ __global__ void __launch_bounds__(256) k_bin_levels(int M, const int* need, int 
         const int n = need[i];
         int L = -1;
         if (n > 0) {
-            const int s = n >> shift;
+            const int s = est ? est[i] : n >> shift;
             L = level_of(s > 0 ? s : 1, G);
         }
         level[i] = static_cast<signed char>(L);
@@ -373,10 +386,10 @@ void launch_pair_bounds(const CsrView& A, const CsrView& B, int* need,
 }
 
 void launch_direct_bounds(const CsrView& R, const CsrView& A, int p_max_row, int* need,
-                          unsigned long long* total, cudaStream_t st) {
+                          unsigned long long* total, cudaStream_t st, int* need_opt, int d1) {
     if (R.M == 0) return;
     k_direct_bounds<8><<<grid_for(static_cast<long long>(R.M) * 8, 256), 256, 0, st>>>(
-        R, A, p_max_row, need, total);
+        R, A, p_max_row, need, need_opt, d1, total);
     note_launch();
 }
 
@@ -403,9 +416,10 @@ void launch_need_from_counts(int M, const int* cnt, const int* cnt1, int* need,
 }
 
 void launch_bin_levels(int M, const int* need, int shift, int G, signed char* level,
-                       int* counts, int* nmax, int* row_cnt_zero, cudaStream_t st) {
+                       int* counts, int* nmax, int* row_cnt_zero, cudaStream_t st,
+                       const int* est) {
     if (M == 0) return;
-    k_bin_levels<<<grid_for(M, 256), 256, 0, st>>>(M, need, shift, G, level, counts, nmax,
+    k_bin_levels<<<grid_for(M, 256), 256, 0, st>>>(M, need, est, shift, G, level, counts, nmax,
                                                     row_cnt_zero);
     note_launch();
 }

@@ -87,19 +87,23 @@ cudaError_t launch_pair_rows(const PairRowArgs& a, const RowParams& p, int mode,
 // bound of the output (A*B: flops; R*A*P: R*A flops times P's longest row).
 void launch_pair_bounds(const CsrView& A, const CsrView& B, int* need,
                         unsigned long long* total, cudaStream_t st);
+// need_opt (optional): optimistic first-table size per row, min(need >> d1,
+// 8 sqrt(R*A products)).
 void launch_direct_bounds(const CsrView& R, const CsrView& A, int p_max_row, int* need,
-                          unsigned long long* total, cudaStream_t st);
+                          unsigned long long* total, cudaStream_t st, int* need_opt = nullptr,
+                          int d1 = 0);
 // *out = max(*out, largest cnt[i]) (cnt null: largest row length of rp).
 void launch_count_max(int M, const int* cnt, const int* rp, int* out, cudaStream_t st);
 // need from exact counts: max(cnt[i], cnt1[i]) (cnt1 may be null).
 void launch_need_from_counts(int M, const int* cnt, const int* cnt1, int* need,
                              cudaStream_t st);
 
-// Binning: level of every row from need[i] >> shift for a group of G lanes
-// (counts[kLevels] = empty rows, whose row_cnt is zeroed when given);
-// nmax = largest need.
+// Binning: level of every row from need[i] >> shift -- or est[i] when est is
+// given -- for a group of G lanes (counts[kLevels] = empty rows, whose
+// row_cnt is zeroed when given); nmax = largest need.
 void launch_bin_levels(int M, const int* need, int shift, int G, signed char* level,
-                       int* counts, int* nmax, int* row_cnt_zero, cudaStream_t st);
+                       int* counts, int* nmax, int* row_cnt_zero, cudaStream_t st,
+                       const int* est = nullptr);
 void launch_bin_scatter(int M, const signed char* level, int* cursors, int* lists,
                         cudaStream_t st);
 // Smallest slot count (power of two >= 32) whose load limit for G lanes

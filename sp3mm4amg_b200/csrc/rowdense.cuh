@@ -129,8 +129,19 @@ __device__ __forceinline__ void daccumulate(const Left& L, int n, const int* __r
             if (NUM) s = L.val(t);
             ab = __ldg(b_rp + k);
             ae = __ldg(b_rp + k + 1);
-            sb = lbound(b_ci, ab, ae, wlo);
-            se = lbound(b_ci, sb, ae, whi);
+            // Rows wholly on one side of the range need no search.
+            sb = se = ae;
+            if (ab < ae) {
+                const int first = __ldg(b_ci + ab), last = __ldg(b_ci + ae - 1);
+                if (last < wlo) {
+                    sb = se = ae;
+                } else if (first >= whi) {
+                    sb = se = ab;
+                } else {
+                    sb = first >= wlo ? ab : lbound(b_ci, ab + 1, ae, wlo);
+                    se = last < whi ? ae : lbound(b_ci, sb, ae - 1, whi);
+                }
+            }
         }
         int fo = 0;
         if (FT) {
