@@ -64,6 +64,8 @@ def parse_args():
     ap.add_argument("--no-batched", action="store_true", help="skip the batched workload")
     ap.add_argument("--no-served", action="store_true", help="skip the served workload")
     ap.add_argument("--no-irregular", action="store_true", help="skip the irregular workload")
+    ap.add_argument("--no-hierarchy", action="store_true",
+                    help="skip the hierarchy build of the main grid")
     ap.add_argument("--no-library", action="store_true",
                     help="skip the cuSPARSE context measurement")
     ap.add_argument("--batch-count", type=int, default=256)
@@ -323,6 +325,42 @@ def run_irregular(S, torch, ctx, stream, npoints=1_000_000, steps=10):
             "kernels_ms": {k: v[1] for k, v in prof.items()}}
 
 
+def run_hierarchy(S, torch, ctx, stream, side=128, steps=3):
+    """The AMG caller of the path: a device hierarchy over the 3D 7-point
+    operator on a side^3 grid (2x2x2 aggregation, one Jacobi step, R = P^T,
+    A_{l+1} = R_l A_l P_l direct, until fewer than 1000 rows), its build time,
+    and every level's R*A*P product timed alone with its kernels."""
+    dims = (side, side, side)
+    dA = ctx.upload(pb.stencil_operator(dims))
+    for _ in range(2):
+        ctx.hierarchy(dA, dims, min_coarse=1000).free()
+    t_build = _events_time(torch, stream, lambda: [ctx.hierarchy(dA, dims, min_coarse=1000).free()
+                                                   for _ in range(steps)]) / steps
+    h = ctx.hierarchy(dA, dims, min_coarse=1000)
+    levels = []
+    for l in range(len(h)):
+        A, P, R = h.level(l)
+        if P is None:
+            levels.append({"level": l, "rows": A.d.M, "nnz": A.d.nnz})
+            continue
+        for _ in range(2):
+            ctx.rap(R, A, P, S.DIRECT, S.UB).free()
+        t = _events_time(torch, stream, lambda: [ctx.rap(R, A, P, S.DIRECT, S.UB).free()
+                                                 for _ in range(steps)]) / steps
+        ctx.set_profiling(True)
+        ctx.rap(R, A, P, S.DIRECT, S.UB).free()
+        prof = ctx.profile()
+        ctx.set_profiling(False)
+        levels.append({"level": l, "rows_R": R.d.M, "nnz_A": A.d.nnz, "nnz_P": P.d.nnz,
+                       "ms_per_product": t * 1e3,
+                       "kernels_ms": {k: round(v[1], 4) for k, v in prof.items()}})
+    h.free()
+    dA.free()
+    return {"workload": f"3D 7-point {side}^3, block 2 aggregation, one Jacobi step, direct UB "
+                        "products until n < 1000",
+            "build_ms": t_build * 1e3, "levels": levels}
+
+
 def run_library(torch, prob, steps=5):
     """Context only, not the product: the same product as (R*A)*P through
     torch's sparse CSR matrix product on the device (cuSPARSE SpGEMM), FP64,
@@ -577,6 +615,8 @@ def main():
         line["served"] = run_served(S, ctx, args.serve_count, args.serve_rate)
     if rank == 0 and not args.no_irregular:
         line["irregular"] = run_irregular(S, torch, ctx, stream)
+    if rank == 0 and not args.no_hierarchy:
+        line["hierarchy"] = run_hierarchy(S, torch, ctx, stream, side=args.side)
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         threads = os.cpu_count() or 1
         kind, run, desc = cpu_reference_runner(prob, threads)
