@@ -19,6 +19,8 @@
 #include <thread>
 #include <vector>
 
+#include <sys/mman.h>
+
 #include "context.cuh"
 #include "kernels.cuh"
 #include "sp3mm_b200.h"
@@ -727,7 +729,8 @@ bool host_pinned(const void* p) {
 // row.
 int upload_u64_staged(sp3mm_ctx* ctx, long long M, long long N, long long nnz,
                       const uint64_t* irp,
-               const uint64_t* ja, const double* as, int off, int vt, sp3mm_dcsr* out) {
+               const uint64_t* ja, const double* as, int off, int vt, sp3mm_dcsr* out,
+               bool values_direct = false) {
     if (M < 0 || N < 0 || nnz < 0) return set_error(ctx, SP3MM_EINVAL, "negative sizes");
     if (M >= INT32_MAX || N >= INT32_MAX || nnz >= INT32_MAX)
         return set_error(ctx, SP3MM_ELIMIT,
@@ -766,6 +769,24 @@ int upload_u64_staged(sp3mm_ctx* ctx, long long M, long long N, long long nnz,
         }
         return SP3MM_OK;
     };
+    // Page-locked FP64 values go to the device as they are, queued first so
+    // that the host threads narrow the indices while they are copied; then
+    // the columns (the larger index array) and the row pointers.
+    const bool vdirect = values_direct && vt == SP3MM_F64 && nnz > 0;
+    if (vdirect)
+        CK(ctx, cudaMemcpyAsync(v.p, as, sizeof(double) * nnz, cudaMemcpyHostToDevice, st));
+    if (nnz > 0) {
+        TRY(push(ci.p, sizeof(int), nnz, [&](long long b, long long lo, long long hi, void* buf) {
+            int* o = static_cast<int*>(buf);
+            bool ok = true;
+            for (long long i = lo; i < hi; ++i) {
+                const long long c = static_cast<long long>(ja[b + i]) - off;
+                ok &= c >= 0 && c < N;
+                o[i] = static_cast<int>(c);
+            }
+            if (!ok) bad = true;
+        }));
+    }
     TRY(push(rp.p, sizeof(int), M + 1, [&](long long b, long long lo, long long hi, void* buf) {
         int* o = static_cast<int*>(buf);
         bool ok = true;
@@ -780,17 +801,7 @@ int upload_u64_staged(sp3mm_ctx* ctx, long long M, long long N, long long nnz,
         }
         if (!ok) bad = true;
     }));
-    if (nnz > 0 && !bad) {
-        TRY(push(ci.p, sizeof(int), nnz, [&](long long b, long long lo, long long hi, void* buf) {
-            int* o = static_cast<int*>(buf);
-            bool ok = true;
-            for (long long i = lo; i < hi; ++i) {
-                const long long c = static_cast<long long>(ja[b + i]) - off;
-                ok &= c >= 0 && c < N;
-                o[i] = static_cast<int>(c);
-            }
-            if (!ok) bad = true;
-        }));
+    if (nnz > 0 && !bad && !vdirect) {
         if (vt == SP3MM_F64) {
             TRY(push(v.p, sizeof(double), nnz,
                      [&](long long b, long long lo, long long hi, void* buf) {
@@ -828,8 +839,14 @@ int upload_u64_staged(sp3mm_ctx* ctx, long long M, long long N, long long nnz,
 // for the sources' memory (validated either way).
 int upload_u64(sp3mm_ctx* ctx, long long M, long long N, long long nnz, const uint64_t* irp,
                const uint64_t* ja, const double* as, int off, int vt, sp3mm_dcsr* out) {
-    if (host_pinned(irp) && host_pinned(ja) && host_pinned(as))
-        return upload_u64_direct(ctx, M, N, nnz, irp, ja, as, off, vt, out);
+    // Page-locked sources: FP64 values copied as they are, indices narrowed
+    // to 32 bits by host threads meanwhile (fewer bytes over the bus); FP32
+    // storage narrows the values on the device.  Pageable sources go through
+    // pinned staging entirely.
+    if (host_pinned(irp) && host_pinned(ja) && host_pinned(as)) {
+        if (vt != SP3MM_F64) return upload_u64_direct(ctx, M, N, nnz, irp, ja, as, off, vt, out);
+        return upload_u64_staged(ctx, M, N, nnz, irp, ja, as, off, vt, out, true);
+    }
     return upload_u64_staged(ctx, M, N, nnz, irp, ja, as, off, vt, out);
 }
 
@@ -842,43 +859,61 @@ int download_u64(sp3mm_ctx* ctx, const sp3mm_dcsr& m, int off, uint64_t* irp, ui
                  double* as) {
     const cudaStream_t st = ctx->stream;
     void* stage = nullptr;
-    const size_t want = std::max<size_t>(sizeof(int) * (static_cast<size_t>(m.M) + 1),
-                                         sizeof(double) * static_cast<size_t>(m.nnz));
-    TRY(host_stage(ctx, want, &stage));
-    const size_t cap = ctx->host_stage_bytes;
-    // One array in chunks that fit the staging: copy, then widen on the host.
-    auto pass = [&](const void* src, size_t esz, long long n, auto&& widen) -> int {
-        const long long per = static_cast<long long>(cap / esz);
-        for (long long b = 0; b < n; b += per) {
-            const long long k = std::min(per, n - b);
-            CK(ctx, cudaMemcpyAsync(stage, static_cast<const unsigned char*>(src) + b * esz,
-                                    esz * k, cudaMemcpyDeviceToHost, st));
-            CK(ctx, cudaStreamSynchronize(st));
-            host_parallel(k, [&](long long lo, long long hi) { widen(b, lo, hi); });
-        }
+    const size_t want = 2 * std::max<size_t>(sizeof(int) * (static_cast<size_t>(m.M) + 1),
+                                             sizeof(double) * static_cast<size_t>(m.nnz));
+    TRY(host_stage(ctx, std::min(want, kHostStageMax), &stage));
+    const size_t half = ctx->host_stage_bytes / 2 / 256 * 256;
+    // The three arrays as one sequence of chunks, each copied into one half
+    // of the staging while the host threads widen the previous chunk from
+    // the other half (an event per half marks its copy done).
+    struct Piece {
+        const void* src;
+        size_t esz;
+        long long b, k;
+        int what;   // 0 row pointers, 1 columns, 2 values
+    };
+    std::vector<Piece> pieces;
+    auto add = [&](const void* src, size_t esz, long long n, int what) {
+        const long long per = static_cast<long long>(half / esz);
+        for (long long b = 0; b < n; b += per) pieces.push_back({src, esz, b, std::min(per, n - b), what});
+    };
+    add(m.row_ptr, sizeof(int), static_cast<long long>(m.M) + 1, 0);
+    if (m.nnz > 0) {
+        add(m.col, sizeof(int), m.nnz, 1);
+        add(m.val, vbytes(m.val_type), m.nnz, 2);
+    }
+    auto issue = [&](size_t i) -> int {
+        const Piece& q = pieces[i];
+        void* buf = static_cast<unsigned char*>(stage) + (i & 1) * half;
+        CK(ctx, cudaMemcpyAsync(buf, static_cast<const unsigned char*>(q.src) + q.b * q.esz,
+                                q.esz * q.k, cudaMemcpyDeviceToHost, st));
+        CK(ctx, cudaEventRecord((i & 1) ? ctx->ev1 : ctx->ev0, st));
         return SP3MM_OK;
     };
-    const int* srp = static_cast<const int*>(stage);
-    TRY(pass(m.row_ptr, sizeof(int), static_cast<long long>(m.M) + 1,
-             [&](long long b, long long lo, long long hi) {
-                 for (long long i = lo; i < hi; ++i)
-                     irp[b + i] = static_cast<uint64_t>(srp[i]) + static_cast<uint64_t>(off);
-             }));
-    if (m.nnz > 0) {
-        TRY(pass(m.col, sizeof(int), m.nnz, [&](long long b, long long lo, long long hi) {
-            for (long long i = lo; i < hi; ++i)
-                ja[b + i] = static_cast<uint64_t>(srp[i]) + static_cast<uint64_t>(off);
-        }));
-        if (m.val_type == SP3MM_F64) {
-            const double* sv = static_cast<const double*>(stage);
-            TRY(pass(m.val, sizeof(double), m.nnz, [&](long long b, long long lo, long long hi) {
-                std::memcpy(as + b + lo, sv + lo, sizeof(double) * (hi - lo));
-            }));
+    if (!pieces.empty()) TRY(issue(0));
+    const uint64_t o = static_cast<uint64_t>(off);
+    for (size_t i = 0; i < pieces.size(); ++i) {
+        if (i + 1 < pieces.size()) TRY(issue(i + 1));
+        CK(ctx, cudaEventSynchronize((i & 1) ? ctx->ev1 : ctx->ev0));
+        const Piece& q = pieces[i];
+        const void* buf = static_cast<unsigned char*>(stage) + (i & 1) * half;
+        const long long b = q.b;
+        if (q.what == 0 || q.what == 1) {
+            const int* src = static_cast<const int*>(buf);
+            uint64_t* dst = (q.what == 0 ? irp : ja) + b;
+            host_parallel(q.k, [&](long long lo, long long hi) {
+                for (long long x = lo; x < hi; ++x) dst[x] = static_cast<uint64_t>(src[x]) + o;
+            });
+        } else if (m.val_type == SP3MM_F64) {
+            const double* src = static_cast<const double*>(buf);
+            host_parallel(q.k, [&](long long lo, long long hi) {
+                std::memcpy(as + b + lo, src + lo, sizeof(double) * (hi - lo));
+            });
         } else {
-            const float* sf = static_cast<const float*>(stage);
-            TRY(pass(m.val, sizeof(float), m.nnz, [&](long long b, long long lo, long long hi) {
-                for (long long i = lo; i < hi; ++i) as[b + i] = static_cast<double>(sf[i]);
-            }));
+            const float* src = static_cast<const float*>(buf);
+            host_parallel(q.k, [&](long long lo, long long hi) {
+                for (long long x = lo; x < hi; ++x) as[b + x] = static_cast<double>(src[x]);
+            });
         }
     }
     return SP3MM_OK;
@@ -939,6 +974,19 @@ int upload_spmat(sp3mm_ctx* ctx, const spmat* m, int off, sp3mm_dcsr* out) {
                       reinterpret_cast<const uint64_t*>(m->JA), m->AS, off, SP3MM_F64, out);
 }
 
+void advise_huge(void* p, size_t bytes) {
+#ifdef MADV_HUGEPAGE
+    if (!p || bytes < (size_t(8) << 20)) return;
+    const uintptr_t pg = 4096;
+    const uintptr_t a = (reinterpret_cast<uintptr_t>(p) + pg - 1) & ~(pg - 1);
+    const uintptr_t e = (reinterpret_cast<uintptr_t>(p) + bytes) & ~(pg - 1);
+    if (e > a) madvise(reinterpret_cast<void*>(a), e - a, MADV_HUGEPAGE);
+#else
+    (void)p;
+    (void)bytes;
+#endif
+}
+
 spmat* download_spmat(sp3mm_ctx* ctx, const sp3mm_dcsr& m, int off) {
     spmat* out = static_cast<spmat*>(calloc(1, sizeof(spmat)));
     if (!out) {
@@ -951,6 +999,10 @@ spmat* download_spmat(sp3mm_ctx* ctx, const sp3mm_dcsr& m, int off) {
     out->IRP = static_cast<idx_t*>(calloc(static_cast<size_t>(m.M) + 1, sizeof(idx_t)));
     out->JA = static_cast<idx_t*>(malloc(sizeof(idx_t) * std::max<long long>(m.nnz, 1)));
     out->AS = static_cast<double*>(malloc(sizeof(double) * std::max<long long>(m.nnz, 1)));
+    // Large result arrays are written once by the host threads: ask for
+    // huge pages so that the first touch takes far fewer page faults.
+    advise_huge(out->JA, sizeof(idx_t) * static_cast<size_t>(std::max<long long>(m.nnz, 1)));
+    advise_huge(out->AS, sizeof(double) * static_cast<size_t>(std::max<long long>(m.nnz, 1)));
     if (!out->IRP || !out->JA || !out->AS) {
         fprintf(stderr, "sp3mm_b200: output spmat arrays allocation failed\n");
         free(out->IRP);
