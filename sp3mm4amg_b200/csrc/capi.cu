@@ -10,10 +10,12 @@
 #include <algorithm>
 #include <atomic>
 #include <chrono>
+#include <condition_variable>
 #include <cstdarg>
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
+#include <functional>
 #include <mutex>
 #include <string>
 #include <thread>
@@ -646,19 +648,109 @@ int host_stage(sp3mm_ctx* ctx, size_t bytes, void** out) {
     return SP3MM_OK;
 }
 
+// Persistent host workers for the transfer loops (narrowing, widening,
+// copies into caller arrays): creating threads per call cost more than the
+// work of a call.  One caller at a time uses the pool; a concurrent caller
+// (e.g. the server's loader thread) spawns its own threads instead.  The
+// pool is never destroyed (detached workers end with the process).
+class HostPool {
+public:
+    explicit HostPool(int n) : nthreads_(n) {
+        for (int k = 0; k < n; ++k) std::thread([this] { work(); }).detach();
+    }
+    int size() const { return nthreads_; }
+    std::mutex use;
+    // Run fn over `chunks` pieces [i*chunk, min(n, (i+1)*chunk)); the caller
+    // takes pieces too and returns when all are done.
+    void run(const std::function<void(long long, long long)>& fn, long long n, long long chunk,
+             int chunks) {
+        {
+            std::lock_guard<std::mutex> lk(m_);
+            fn_ = &fn;
+            n_ = n;
+            chunk_ = chunk;
+            chunks_ = chunks;
+            next_.store(0);
+            finished_ = 0;
+            ++gen_;
+        }
+        cv_.notify_all();
+        pull();
+        std::unique_lock<std::mutex> lk(m_);
+        done_.wait(lk, [&] { return finished_ == chunks_; });
+        fn_ = nullptr;
+    }
+
+private:
+    void pull() {
+        int done = 0;
+        for (;;) {
+            const int i = next_.fetch_add(1);
+            if (i >= chunks_) break;
+            const long long lo = i * chunk_;
+            const long long hi = std::min(n_, lo + chunk_);
+            (*fn_)(lo, hi);
+            ++done;
+        }
+        if (done) {
+            std::lock_guard<std::mutex> lk(m_);
+            finished_ += done;
+            if (finished_ == chunks_) done_.notify_all();
+        }
+    }
+    void work() {
+        unsigned seen = 0;
+        for (;;) {
+            {
+                std::unique_lock<std::mutex> lk(m_);
+                cv_.wait(lk, [&] { return gen_ != seen; });
+                seen = gen_;
+                if (!fn_) continue;
+            }
+            pull();
+        }
+    }
+    const int nthreads_;
+    std::mutex m_;
+    std::condition_variable cv_, done_;
+    const std::function<void(long long, long long)>* fn_ = nullptr;
+    long long n_ = 0, chunk_ = 1;
+    int chunks_ = 0, finished_ = 0;
+    std::atomic<int> next_{0};
+    unsigned gen_ = 0;
+};
+
+HostPool& host_pool() {
+    static HostPool* pool = [] {
+        const unsigned hw = std::thread::hardware_concurrency();
+        const int n = static_cast<int>(std::max(1u, std::min(hw ? hw : 1u, 16u)) - 1);
+        return new HostPool(n);
+    }();
+    return *pool;
+}
+
 // f(lo, hi) over [0, n) on up to 16 host threads (one for small n).
 template <typename F>
 void host_parallel(long long n, F&& f) {
-    const long long per = 1 << 20;
-    int t = static_cast<int>(std::min<long long>((n + per - 1) / per, 16));
+    const long long per = 1 << 18;
     const unsigned hw = std::thread::hardware_concurrency();
+    int t = static_cast<int>(std::min<long long>((n + per - 1) / per, 16));
     if (hw) t = std::min<int>(t, static_cast<int>(hw));
     if (t <= 1) {
         f(0LL, n);
         return;
     }
-    std::vector<std::thread> th;
     const long long chunk = (n + t - 1) / t;
+    HostPool& pool = host_pool();
+    std::unique_lock<std::mutex> lk(pool.use, std::try_to_lock);
+    if (lk.owns_lock() && pool.size() > 0) {
+        const std::function<void(long long, long long)> fn = [&f](long long lo, long long hi) {
+            f(lo, hi);
+        };
+        pool.run(fn, n, chunk, static_cast<int>((n + chunk - 1) / chunk));
+        return;
+    }
+    std::vector<std::thread> th;
     for (int k = 0; k < t; ++k) {
         const long long lo = k * chunk, hi = std::min(n, lo + chunk);
         if (lo < hi) th.emplace_back([&f, lo, hi] { f(lo, hi); });
