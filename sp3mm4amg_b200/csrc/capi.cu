@@ -821,8 +821,7 @@ bool host_pinned(const void* p) {
 // row.
 int upload_u64_staged(sp3mm_ctx* ctx, long long M, long long N, long long nnz,
                       const uint64_t* irp,
-               const uint64_t* ja, const double* as, int off, int vt, sp3mm_dcsr* out,
-               bool values_direct = false) {
+               const uint64_t* ja, const double* as, int off, int vt, sp3mm_dcsr* out) {
     if (M < 0 || N < 0 || nnz < 0) return set_error(ctx, SP3MM_EINVAL, "negative sizes");
     if (M >= INT32_MAX || N >= INT32_MAX || nnz >= INT32_MAX)
         return set_error(ctx, SP3MM_ELIMIT,
@@ -861,24 +860,6 @@ int upload_u64_staged(sp3mm_ctx* ctx, long long M, long long N, long long nnz,
         }
         return SP3MM_OK;
     };
-    // Page-locked FP64 values go to the device as they are, queued first so
-    // that the host threads narrow the indices while they are copied; then
-    // the columns (the larger index array) and the row pointers.
-    const bool vdirect = values_direct && vt == SP3MM_F64 && nnz > 0;
-    if (vdirect)
-        CK(ctx, cudaMemcpyAsync(v.p, as, sizeof(double) * nnz, cudaMemcpyHostToDevice, st));
-    if (nnz > 0) {
-        TRY(push(ci.p, sizeof(int), nnz, [&](long long b, long long lo, long long hi, void* buf) {
-            int* o = static_cast<int*>(buf);
-            bool ok = true;
-            for (long long i = lo; i < hi; ++i) {
-                const long long c = static_cast<long long>(ja[b + i]) - off;
-                ok &= c >= 0 && c < N;
-                o[i] = static_cast<int>(c);
-            }
-            if (!ok) bad = true;
-        }));
-    }
     TRY(push(rp.p, sizeof(int), M + 1, [&](long long b, long long lo, long long hi, void* buf) {
         int* o = static_cast<int*>(buf);
         bool ok = true;
@@ -893,7 +874,17 @@ int upload_u64_staged(sp3mm_ctx* ctx, long long M, long long N, long long nnz,
         }
         if (!ok) bad = true;
     }));
-    if (nnz > 0 && !bad && !vdirect) {
+    if (nnz > 0 && !bad) {
+        TRY(push(ci.p, sizeof(int), nnz, [&](long long b, long long lo, long long hi, void* buf) {
+            int* o = static_cast<int*>(buf);
+            bool ok = true;
+            for (long long i = lo; i < hi; ++i) {
+                const long long c = static_cast<long long>(ja[b + i]) - off;
+                ok &= c >= 0 && c < N;
+                o[i] = static_cast<int>(c);
+            }
+            if (!ok) bad = true;
+        }));
         if (vt == SP3MM_F64) {
             TRY(push(v.p, sizeof(double), nnz,
                      [&](long long b, long long lo, long long hi, void* buf) {
@@ -931,14 +922,8 @@ int upload_u64_staged(sp3mm_ctx* ctx, long long M, long long N, long long nnz,
 // for the sources' memory (validated either way).
 int upload_u64(sp3mm_ctx* ctx, long long M, long long N, long long nnz, const uint64_t* irp,
                const uint64_t* ja, const double* as, int off, int vt, sp3mm_dcsr* out) {
-    // Page-locked sources: FP64 values copied as they are, indices narrowed
-    // to 32 bits by host threads meanwhile (fewer bytes over the bus); FP32
-    // storage narrows the values on the device.  Pageable sources go through
-    // pinned staging entirely.
-    if (host_pinned(irp) && host_pinned(ja) && host_pinned(as)) {
-        if (vt != SP3MM_F64) return upload_u64_direct(ctx, M, N, nnz, irp, ja, as, off, vt, out);
-        return upload_u64_staged(ctx, M, N, nnz, irp, ja, as, off, vt, out, true);
-    }
+    if (host_pinned(irp) && host_pinned(ja) && host_pinned(as))
+        return upload_u64_direct(ctx, M, N, nnz, irp, ja, as, off, vt, out);
     return upload_u64_staged(ctx, M, N, nnz, irp, ja, as, off, vt, out);
 }
 
