@@ -778,9 +778,10 @@ int upload_u64_direct(sp3mm_ctx* ctx, long long M, long long N, long long nnz, c
     TRY(stage.alloc(ctx, sizeof(uint64_t) * std::max(M + 1, nnz)));
     CK(ctx, cudaMemsetAsync(maxrow.p, 0, sizeof(int), st));
     CK(ctx, cudaMemcpyAsync(stage.p, irp, sizeof(uint64_t) * (M + 1), cudaMemcpyHostToDevice, st));
+    // Malformed row pointers are flagged and narrowed to 0, so the column
+    // pass below stays in bounds; the error is reported by the final check.
     launch_narrow_rowptr(M, nnz, stage.as<unsigned long long>(), off, rp.as<int>(), ctx->d_err, st);
     CK(ctx, cudaGetLastError());
-    TRY(check_device_err(ctx));
     if (nnz > 0) {
         CK(ctx, cudaMemcpyAsync(stage.p, ja, sizeof(uint64_t) * nnz, cudaMemcpyHostToDevice, st));
         launch_narrow_cols(M, N, rp.as<int>(), stage.as<unsigned long long>(), off, ci.as<int>(),
