@@ -16,6 +16,7 @@
 #include <cstdlib>
 #include <cstring>
 #include <functional>
+#include <map>
 #include <mutex>
 #include <string>
 #include <thread>
@@ -635,14 +636,80 @@ int rap_impl(sp3mm_ctx* ctx, const sp3mm_dcsr& R, const sp3mm_dcsr& A, const sp3
 // Pinned staging of at least `bytes` (at most kHostStageMax) on the context.
 constexpr size_t kHostStageMax = size_t(256) << 20;
 
+// Page-locked staging buffers outlive the contexts that used them: a
+// process-wide cache hands the buffer of a destroyed (or grown) context to
+// the next context that needs one.  cudaHostAlloc costs about 0.4 ms per MB
+// (100 ms for 256 MB on a B200 host), ten times the copy it stages, and a
+// server creates its loader context per instance, a caller thread its
+// context per thread.  A buffer is given back only after its context's
+// stream has been synchronised, so no copy from it is in flight.
+class PinnedCache {
+public:
+    // A cached buffer of at least `bytes`, else a new one; *got = its size.
+    void* take(size_t bytes, size_t* got) {
+        {
+            std::lock_guard<std::mutex> lk(mu_);
+            auto it = free_.lower_bound(bytes);
+            if (it != free_.end()) {
+                void* p = it->second;
+                *got = it->first;
+                held_ -= it->first;
+                free_.erase(it);
+                return p;
+            }
+        }
+        void* p = nullptr;
+        if (cudaHostAlloc(&p, bytes, cudaHostAllocPortable) != cudaSuccess) return nullptr;
+        *got = bytes;
+        return p;
+    }
+    void give(void* p, size_t bytes) {
+        if (!p) return;
+        {
+            std::lock_guard<std::mutex> lk(mu_);
+            if (held_ + bytes <= kMaxHeld) {
+                free_.emplace(bytes, p);
+                held_ += bytes;
+                return;
+            }
+        }
+        cudaFreeHost(p);
+    }
+
+private:
+    static constexpr size_t kMaxHeld = size_t(1) << 30;
+    std::mutex mu_;
+    std::multimap<size_t, void*> free_;
+    size_t held_ = 0;
+};
+
+// Never destroyed: cached buffers are released with the process.
+PinnedCache& pinned_cache() {
+    static PinnedCache* c = new PinnedCache();
+    return *c;
+}
+
+// Sizes are rounded up to powers of two (1 MB .. kHostStageMax), so a
+// context grows its staging a few times at most.
 int host_stage(sp3mm_ctx* ctx, size_t bytes, void** out) {
     bytes = std::min(std::max<size_t>(bytes, size_t(1) << 20), kHostStageMax);
-    if (ctx->host_stage_bytes < bytes) {
-        if (ctx->host_stage) cudaFreeHost(ctx->host_stage);
+    size_t want = size_t(1) << 20;
+    while (want < bytes) want <<= 1;
+    if (ctx->host_stage_bytes < want) {
+        if (ctx->host_stage) {
+            CK(ctx, cudaStreamSynchronize(ctx->stream));
+            pinned_cache().give(ctx->host_stage, ctx->host_stage_bytes);
+        }
         ctx->host_stage = nullptr;
         ctx->host_stage_bytes = 0;
-        CK(ctx, cudaHostAlloc(&ctx->host_stage, bytes, cudaHostAllocDefault));
-        ctx->host_stage_bytes = bytes;
+        size_t got = 0;
+        void* p = pinned_cache().take(want, &got);
+        if (!p) {
+            cudaGetLastError();
+            return set_error(ctx, SP3MM_ENOMEM, "page-locked staging of %zu bytes", want);
+        }
+        ctx->host_stage = p;
+        ctx->host_stage_bytes = got;
     }
     *out = ctx->host_stage;
     return SP3MM_OK;
@@ -1281,7 +1348,7 @@ int sp3mm_ctx_destroy(sp3mm_ctx* ctx) {
     if (ctx->ev0) cudaEventDestroy(ctx->ev0);
     if (ctx->ev1) cudaEventDestroy(ctx->ev1);
     if (ctx->own_stream) cudaStreamDestroy(ctx->own_stream);
-    if (ctx->host_stage) cudaFreeHost(ctx->host_stage);
+    pinned_cache().give(ctx->host_stage, ctx->host_stage_bytes);
     if (ctx->host_box) cudaFreeHost(ctx->host_box);
     if (tl_ctx == ctx) tl_ctx = nullptr;
     delete ctx;

@@ -83,6 +83,30 @@ void prof(sp3mm_ctx* ctx, const char* label, F&& f) {
     ctx->prof.push_back(r);
 }
 
+// Events around a phase of several launches and host steps (profiling
+// only): the span ends at end() or when it goes out of scope, on any path.
+// Its time includes the gaps in which the stream waited for the host.
+struct ProfSpan {
+    sp3mm_ctx* ctx;
+    sp3mm_ctx::ProfRec r{nullptr, nullptr, nullptr};
+    ProfSpan(sp3mm_ctx* c, const char* label) : ctx(c) {
+        if (!ctx->profiling) return;
+        r.label = label;
+        cudaEventCreate(&r.a);
+        cudaEventCreate(&r.b);
+        cudaEventRecord(r.a, ctx->stream);
+    }
+    void end() {
+        if (!r.a) return;
+        cudaEventRecord(r.b, ctx->stream);
+        ctx->prof.push_back(r);
+        r.a = nullptr;
+    }
+    ~ProfSpan() { end(); }
+    ProfSpan(const ProfSpan&) = delete;
+    ProfSpan& operator=(const ProfSpan&) = delete;
+};
+
 // Stream-ordered device allocation from the device's memory pool.
 struct DevBuf {
     sp3mm_ctx* ctx = nullptr;

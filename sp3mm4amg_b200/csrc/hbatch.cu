@@ -236,6 +236,8 @@ int step_group(sp3mm_ctx* ctx, const std::vector<sp3mm_hierarchy*>& hs) {
     if (rows >= INT32_MAX || cols >= INT32_MAX)
         return set_error(ctx, SP3MM_ELIMIT, "hierarchy step: too many rows");
 
+    ProfSpan whole(ctx, "hstep");
+    ProfSpan phase(ctx, "hstep.labels");
     DevBuf dH, dB, dCB, agg, d, iota, ones, cnt, cursor, grp, tmp, rrp_off;
     TRY(dH.alloc(ctx, sizeof(HStep) * k));
     TRY(dB.alloc(ctx, sizeof(long long) * (k + 1)));
@@ -257,6 +259,8 @@ int step_group(sp3mm_ctx* ctx, const std::vector<sp3mm_hierarchy*>& hs) {
     CK(ctx, cudaGetLastError());
 
     // A*P0 for every hierarchy: one SpMM batch.
+    phase.end();
+    ProfSpan phase_ap0(ctx, "hstep.ap0");
     std::vector<int> kinds(k, SP3MM_BATCH_SPMM);
     std::vector<sp3mm_dcsr> X(k), Y(k), Z(k);
     for (int t = 0; t < k; ++t) {
@@ -278,6 +282,8 @@ int step_group(sp3mm_ctx* ctx, const std::vector<sp3mm_hierarchy*>& hs) {
     batch_trim(b1.get());
 
     // P values (in place when FP64) and the restriction arrays.
+    phase_ap0.end();
+    ProfSpan phase_jac(ctx, "hstep.jacobi");
     auto arena = std::make_shared<Arena>(ctx);
     std::vector<sp3mm_dcsr> AP0(k), P(k), R(k);
     long long nnz_p = 0;
@@ -309,6 +315,8 @@ int step_group(sp3mm_ctx* ctx, const std::vector<sp3mm_hierarchy*>& hs) {
     CK(ctx, cudaGetLastError());
 
     // R = P^T of the block-diagonal concatenation.
+    phase_jac.end();
+    ProfSpan phase_tr(ctx, "hstep.transpose");
     TRY(cnt.alloc(ctx, sizeof(int) * (cols + 1)));
     TRY(cursor.alloc(ctx, sizeof(int) * (cols + 1)));
     TRY(grp.alloc(ctx, sizeof(int) * (cols + 1)));
@@ -349,6 +357,8 @@ int step_group(sp3mm_ctx* ctx, const std::vector<sp3mm_hierarchy*>& hs) {
     }
 
     // A_c = R*A*P for every hierarchy: one batch of direct products.
+    phase_tr.end();
+    ProfSpan phase_rap(ctx, "hstep.rap");
     std::vector<int> rk(k, SP3MM_BATCH_RAP);
     for (int t = 0; t < k; ++t) X[t] = R[t];
     raw = nullptr;

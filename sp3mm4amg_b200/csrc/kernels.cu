@@ -88,11 +88,17 @@ __global__ void __launch_bounds__(256) k_direct_bounds(CsrView R, CsrView A, int
                 // Optimistic first-table size: the bound >> d1, at most
                 // 8 sqrt(products) -- long R*A rows repeat their columns
                 // (stencil coarse levels: ~6 sqrt, kNN rows: <= 8.4 sqrt);
-                // a row that overflows is recomputed with the bound.
+                // a row that overflows is recomputed with the bound.  A row
+                // with at least as many products as A has columns is taken
+                // as dense (the coarsest levels: every column, hundreds of
+                // thousands of products) and gets the bound itself, which
+                // bins it to the CTA-per-row kernel instead of a warp that
+                // overflows and retries alone.
                 long long o = d >> d1;
                 const long long r =
                     static_cast<long long>(ceil(8.0 * sqrt(static_cast<double>(u1))));
                 if (r < o) o = r;
+                if (u1 >= A.N) o = d;
                 if (d > 0 && o < 1) o = 1;
                 need_opt[row] = static_cast<int>(o < INT_MAX ? o : INT_MAX);
             }

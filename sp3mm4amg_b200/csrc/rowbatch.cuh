@@ -90,12 +90,12 @@ __device__ __forceinline__ int batch_accumulate(const Left& L, int n, const int*
                                                 double* vals, int* ord, int S, int Sp, int scap,
                                                 int* sk, double* sv, int& nk) {
     WTab T = make_wtab(keys, vals, ord, S);
-    if (waccumulate<NUM, false>(L, n, b_rp, b_ci, b_v, T, sk, sv, nk)) return S;
+    if (waccumulate<NUM, kProbeBySize>(L, n, b_rp, b_ci, b_v, T, sk, sv, nk)) return S;
     wclear(T, nk, NUM);
     __syncwarp();
     if (Sp <= S || Sp > scap) return 0;
     T = make_wtab(keys, vals, ord, Sp);
-    if (waccumulate<NUM, false>(L, n, b_rp, b_ci, b_v, T, sk, sv, nk)) return Sp;
+    if (waccumulate<NUM, kProbeBySize>(L, n, b_rp, b_ci, b_v, T, sk, sv, nk)) return Sp;
     wclear(T, nk, NUM);
     __syncwarp();
     return 0;
@@ -193,12 +193,14 @@ __global__ void __launch_bounds__(256, 4)
                 const WTab T1 = make_wtab(keys1, vals1, ord1, S1);
                 const WTab T2 = make_wtab(keys2, vals2, ord2, S2);
                 bool ok = S1 <= scap && S2 <= scap &&
-                          waccumulate<NUM, false>(L1, xlen, Y.rp, Y.ci, static_cast<const TV*>(Y.v),
-                                           T1, sk, sv, n1);
+                          waccumulate<NUM, kProbeBySize>(L1, xlen, Y.rp, Y.ci,
+                                                         static_cast<const TV*>(Y.v), T1, sk, sv,
+                                                         n1);
                 if (ok) {
                     const LeftT L2{keys1, vals1, ord1};
-                    ok = waccumulate<NUM, false>(L2, n1, Z.rp, Z.ci, static_cast<const TV*>(Z.v), T2,
-                                          sk, sv, n2);
+                    ok = waccumulate<NUM, kProbeBySize>(L2, n1, Z.rp, Z.ci,
+                                                        static_cast<const TV*>(Z.v), T2, sk, sv,
+                                                        n2);
                 }
                 if (S1 <= scap) wclear(T1, n1, NUM);
                 __syncwarp();
@@ -238,7 +240,7 @@ __global__ void __launch_bounds__(256, 4)
                 if (S1 <= scap) S1 = min(S1 << p.slack, scap);
                 const WTab T = make_wtab(keys1, vals1, ord1, S1);
                 const bool ok = S1 <= scap &&
-                                waccumulate<NUM, false>(L1, xlen, Y.rp, Y.ci,
+                                waccumulate<NUM, kProbeBySize>(L1, xlen, Y.rp, Y.ci,
                                                  static_cast<const TV*>(Y.v), T, sk, sv, n1);
                 if (!ok || n1 != e) {
                     if (S1 <= scap) wclear(T, n1, NUM);

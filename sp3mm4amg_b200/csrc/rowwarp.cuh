@@ -90,8 +90,8 @@ __device__ __forceinline__ int winsert(const WTab& T, int key, bool& is_new) {
 
 // Find `key` or claim an empty slot probing one slot at a time (linear
 // probing from the key's hash).  Same contract as winsert; the batch kernels
-// use it (measured faster there than bucketed probing, slower on the
-// single-product kNN rows).
+// use it for small tables (measured faster there than bucketed probing,
+// slower on long rows and the single-product kNN rows).
 __device__ __forceinline__ int winsert1(const WTab& T, int key, bool& is_new) {
     unsigned s = hash_slot(key, T.shift);
     for (unsigned probe = 0; probe <= T.smask; ++probe) {
@@ -110,9 +110,16 @@ __device__ __forceinline__ int winsert1(const WTab& T, int key, bool& is_new) {
     return -1;
 }
 
+// Probing of wbatch: bucketed (winsert), linear (winsert1), or chosen per
+// table -- linear below kBucketMinSlots, where tables are lightly loaded
+// and short, bucketed above, where a warp's 32 leaders otherwise wait on
+// the longest of their linear probe runs.
+enum { kProbeBucket = 0, kProbeLinear = 1, kProbeBySize = 2 };
+constexpr unsigned kBucketMinSlots = 256;
+
 // One batch: lane i holds staged product i (key sk[i], value sv[i]) when
 // `valid`.  Updates nk, the table's distinct count.
-template <bool NUM, bool B4 = true>
+template <bool NUM, int PROBE = kProbeBucket>
 __device__ __forceinline__ void wbatch(const WTab& T, const int* sk, const double* sv, int i,
                                        bool valid, int& nk) {
     const int lane = threadIdx.x & 31;
@@ -122,7 +129,9 @@ __device__ __forceinline__ void wbatch(const WTab& T, const int* sk, const doubl
     bool is_new = false;
     int slot = 0;
     if (valid && (peers & lt) == 0) {
-        slot = B4 ? winsert(T, key, is_new) : winsert1(T, key, is_new);
+        const bool bucket =
+            PROBE == kProbeBucket || (PROBE == kProbeBySize && T.smask + 1 >= kBucketMinSlots);
+        slot = bucket ? winsert(T, key, is_new) : winsert1(T, key, is_new);
         if (NUM && slot >= 0) {
             double acc = T.vals[slot];
             const int i0 = i - lane;
@@ -156,7 +165,7 @@ __device__ __forceinline__ int wscan_excl(int v, int& total) {
 // order (the warp owns the row; n is warp-uniform).  Returns false when the
 // table passed its load limit; nk = distinct columns inserted (listed in
 // T.ord either way).
-template <bool NUM, bool B4 = true, typename TB, class Left>
+template <bool NUM, int PROBE = kProbeBucket, typename TB, class Left>
 __device__ __forceinline__ bool waccumulate(const Left& L, int n, const int* __restrict__ b_rp,
                                             const int* __restrict__ b_ci,
                                             const TB* __restrict__ b_v, const WTab& T, int* sk,
@@ -217,7 +226,7 @@ __device__ __forceinline__ bool waccumulate(const Left& L, int n, const int* __r
             __syncwarp();
             const int wl = min(kStage, total - w0);
             for (int i0 = 0; i0 < wl; i0 += 32) {
-                wbatch<NUM, B4>(T, sk, sv, i0 + lane, i0 + lane < wl, nk);
+                wbatch<NUM, PROBE>(T, sk, sv, i0 + lane, i0 + lane < wl, nk);
                 if (nk > T.limit) {
                     __syncwarp();
                     return false;
