@@ -41,8 +41,10 @@ namespace {
 // product count of its row of X*Y, at most Y.N); row_item[g] = its product.
 // *total += the output-size bound of every row (SpMM: need; direct:
 // min(R*A products times Z's longest row, Z.N)).  need_opt[g] = the
-// optimistic first-table size: need >> d1, or need itself when the row's
-// products reach Y's column count (such rows are dense).
+// optimistic first-table size: need >> d1 capped at 8 sqrt(products) (long
+// rows repeat their columns; the single-product bound kernel uses the same
+// guess), or need itself when the row's products reach Y's column count
+// (such rows are dense).
 __global__ void k_batch_bounds(const BItem* __restrict__ items, const long long* __restrict__ bases,
                                int n, long long rows, int d1, int* need, int* need_opt,
                                int* row_item, unsigned long long* total) {
@@ -68,7 +70,10 @@ __global__ void k_batch_bounds(const BItem* __restrict__ items, const long long*
         const int nd = static_cast<int>(u < I->Y.N ? u : I->Y.N);
         need[g] = nd;
         // (a positive bound stays positive: binning skips rows of need 0)
-        need_opt[g] = nd == 0 ? 0 : (u >= I->Y.N ? nd : max(1, nd >> d1));
+        long long o = nd >> d1;
+        const long long r = static_cast<long long>(ceil(8.0 * sqrt(static_cast<double>(u))));
+        if (r < o) o = r;
+        need_opt[g] = nd == 0 ? 0 : (u >= I->Y.N ? nd : max(1, static_cast<int>(o)));
         row_item[g] = lo;
         if (I->kind == kBatchDirect) {
             const long long zm = I->zmax >= 0 ? I->zmax : I->Z.N;
@@ -563,15 +568,18 @@ int batch_plan(sp3mm_batch* b) {
     DevBuf ub_ci, ub_v, row_off, cursor;
     if (b->flavour == SP3MM_UB && rows > 0) {
         // One numeric pass: every row books its exact length from one
-        // cursor, in space bounded by the output bound, by eight times the
+        // cursor, in space bounded by the output bound, by twice the
         // operands' nonzeros and by half the free memory (a batch that
-        // overflows it is planned symbolically instead).
+        // overflows it is planned symbolically instead).  Galerkin products
+        // and their A*P0 steps write well under their operands' nonzeros;
+        // reserving more made the pool map tens of GB for a batch of large
+        // hierarchies' first levels.
         const size_t eb = sizeof(int) + vbytes(b->to);
         long long in_nnz = 0;
         for (const BItem& I : b->items)
             in_nnz += I.X.nnz + I.Y.nnz + (I.kind == kBatchDirect ? I.Z.nnz : 0);
         unsigned long long cap = std::min<unsigned long long>(
-            sb.total, std::max<unsigned long long>(1ULL << 20, 8ULL * in_nnz));
+            sb.total, std::max<unsigned long long>(1ULL << 20, 2ULL * in_nnz));
         if (cap * eb > (size_t(1) << 30) && pool_idle_bytes(ctx) < cap * eb)
             cap = std::min<unsigned long long>(
                 cap, std::max<unsigned long long>(1ULL << 20, free_device_bytes(ctx) / 2 / eb));
