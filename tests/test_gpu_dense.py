@@ -101,3 +101,28 @@ def test_rows_beyond_the_slice_are_retried(orc):
     R2 = pb.random_sparse(20, n, 0.3, seed=15)
     with S.Context() as ctx:
         _direct_all_ways(ctx, orc, R2, A2, P2, "wide C span")
+
+
+def test_rows_with_more_products_than_columns_run_one_cta_per_row(orc):
+    # The coarsest levels' shape (93^3 level 3: 216 rows, 270k products and
+    # all 1,728 columns each): every R*A row has more products than A has
+    # columns.  Such rows are binned by their bound (here 2,000 columns, a
+    # table of 4,096 slots), not the bound shifted right, so the default
+    # routing sends them to the CTA-per-row kernel.
+    R = pb.random_sparse(20, 2000, 0.3, seed=21)
+    A = pb.random_sparse(2000, 2000, 0.1, seed=22)
+    P = pb.random_sparse(2000, 60, 0.1, seed=23)
+    want = orc.sp3mm_direct(R, A, P)
+    with S.Context() as ctx:
+        d = [ctx.upload(m) for m in (R, A, P)]
+        for fl in (S.UB, S.SYMBNUM):
+            ctx.set_profiling(True)
+            C = ctx.rap(*d, S.DIRECT, fl)
+            got = C.download()
+            prof = ctx.profile()
+            ctx.set_profiling(False)
+            C.free()
+            _same(got, want, ("dense rows", fl))
+            assert any(k.startswith("direct.dense") for k in prof), prof
+        for m in d:
+            m.free()
