@@ -8,10 +8,12 @@
 //      free and the request's device-memory estimate fits both the server's
 //      budget (what admitted requests have reserved) and the HBM free right
 //      now (cudaMemGetInfo plus the idle part of the memory pool), and hands
-//      them to the loader thread, which uploads them on its own context and
-//      stream while this step's kernels run (copies overlap compute);
-//   2. lets the requests the loader has finished join, waiting for the
-//      loader only when nothing else could run;
+//      them to the loader threads, which upload them on their own contexts
+//      and streams while this step's kernels run (copies overlap compute;
+//      two loaders keep two uploads, each narrowing on host threads, in
+//      flight);
+//   2. lets the requests the loaders have finished join, waiting for them
+//      only when nothing else could run;
 //   3. advances every joined hierarchy by one level in one level step
 //      (hierarchy_step: batched launches shared by all requests, whatever
 //      their level or size, so requests admitted while others are in flight
@@ -59,7 +61,7 @@ struct Request {
     double t_arrival = 0, t_admit = -1, t_done = -1;
     size_t est = 0;
     size_t held = 0;   // bytes of the budget reserved while admitted
-    bool loading = false;   // with the loader thread (reported as active)
+    bool loading = false;   // with a loader thread (reported as active)
     int status = kQueued;
     int error = SP3MM_OK;
     sp3mm_hierarchy* h = nullptr;
@@ -91,9 +93,10 @@ struct sp3mm_server {
     std::deque<int64_t> queue;
     std::vector<int64_t> active;
     std::unordered_map<int64_t, Request> reqs;
-    // Loader thread: admitted requests are uploaded on its own context.
-    sp3mm_ctx* loader_ctx = nullptr;
-    std::thread loader;
+    // Loader threads: admitted requests are uploaded on their own contexts.
+    static constexpr int kLoaders = 2;
+    sp3mm_ctx* loader_ctx[kLoaders] = {};
+    std::thread loader[kLoaders];
     std::mutex mu;
     std::condition_variable wake, done;
     std::deque<Request*> to_load;    // guarded by mu
@@ -112,25 +115,27 @@ struct sp3mm_server {
             stop = true;
         }
         wake.notify_all();
-        if (loader.joinable()) loader.join();
+        for (auto& t : loader)
+            if (t.joinable()) t.join();
         for (auto& kv : reqs)
             if (kv.second.h && kv.second.status != kTaken) sp3mm_hierarchy_free(ctx, kv.second.h);
-        if (loader_ctx) sp3mm_ctx_destroy(loader_ctx);
+        for (sp3mm_ctx* c : loader_ctx)
+            if (c) sp3mm_ctx_destroy(c);
     }
 };
 
 namespace {
 
-// Upload a request's operator on the loader context (the call returns once
+// Upload a request's operator on a loader context (the call returns once
 // the copy and its validation are complete) and wrap it in a hierarchy.
 // The operator is freed on the server's context, after the work that uses it.
-int admit(sp3mm_server* s, Request& r) {
+int admit(sp3mm_server* s, sp3mm_ctx* lctx, Request& r) {
     sp3mm_ctx* ctx = s->ctx;
     auto A0 = std::shared_ptr<sp3mm_dcsr>(new sp3mm_dcsr{}, [ctx](sp3mm_dcsr* m) {
         sp3mm_dcsr_free(ctx, m);
         delete m;
     });
-    TRY(sp3mm_dcsr_upload_arrays(s->loader_ctx, r.M, r.M, r.nnz, r.rp, r.ci, r.v, SP3MM_F64,
+    TRY(sp3mm_dcsr_upload_arrays(lctx, r.M, r.M, r.nnz, r.rp, r.ci, r.v, SP3MM_F64,
                                  A0.get()));
     auto* h = new sp3mm_hierarchy();
     h->ndim = r.ndim;
@@ -150,7 +155,7 @@ int admit(sp3mm_server* s, Request& r) {
     return SP3MM_OK;
 }
 
-void loader_main(sp3mm_server* s) {
+void loader_main(sp3mm_server* s, sp3mm_ctx* lctx) {
     cudaSetDevice(s->ctx->device);
     for (;;) {
         Request* r = nullptr;
@@ -161,7 +166,7 @@ void loader_main(sp3mm_server* s) {
             r = s->to_load.front();
             s->to_load.pop_front();
         }
-        r->error = admit(s, *r);
+        r->error = admit(s, lctx, *r);
         {
             std::lock_guard<std::mutex> lk(s->mu);
             s->loaded.push_back(r);
@@ -196,12 +201,15 @@ int sp3mm_server_create(sp3mm_ctx* ctx, int max_active, double mem_fraction,
     s->mem_fraction = mem_fraction;
     s->budget = static_cast<size_t>(mem_fraction * static_cast<double>(free_hbm(ctx)));
     s->t0 = std::chrono::steady_clock::now();
-    const int rc = sp3mm_ctx_create(ctx->device, &s->loader_ctx);
-    if (rc != SP3MM_OK) {
-        delete s;
-        return set_error(ctx, rc, "server: loader context creation failed");
+    for (int k = 0; k < sp3mm_server::kLoaders; ++k) {
+        const int rc = sp3mm_ctx_create(ctx->device, &s->loader_ctx[k]);
+        if (rc != SP3MM_OK) {
+            delete s;
+            return set_error(ctx, rc, "server: loader context creation failed");
+        }
     }
-    s->loader = std::thread(loader_main, s);
+    for (int k = 0; k < sp3mm_server::kLoaders; ++k)
+        s->loader[k] = std::thread(loader_main, s, s->loader_ctx[k]);
     *out = s;
     return SP3MM_OK;
 }
@@ -253,7 +261,7 @@ int sp3mm_server_step(sp3mm_server* s, int* pending) {
         std::lock_guard<std::mutex> lk(s->mu);
         in_loader = s->in_loader + static_cast<int>(s->loaded.size());
     }
-    // 1. Admission, first come first served; uploads go to the loader.
+    // 1. Admission, first come first served; uploads go to the loaders.
     std::vector<Request*> handed;
     while (!s->queue.empty() &&
            static_cast<int>(s->active.size()) + in_loader < s->max_active) {
@@ -286,7 +294,7 @@ int sp3mm_server_step(sp3mm_server* s, int* pending) {
         }
         s->wake.notify_all();
     }
-    // 2. Requests the loader has finished join; wait only when nothing
+    // 2. Requests the loaders have finished join; wait only when nothing
     //    else could run.
     {
         std::unique_lock<std::mutex> lk(s->mu);
