@@ -414,8 +414,8 @@ SP3MM_API int sp3mm_hierarchy_build_batch(sp3mm_ctx *ctx, int n, const sp3mm_dcs
  * while fewer than max_active are in flight and the request's device-memory
  * estimate fits both the budget (mem_fraction of the HBM free at creation,
  * less what admitted requests reserve) and the HBM free now, and hands them
- * to the server's loader thread, which uploads them on its own stream while
- * the step computes; then advances every uploaded hierarchy by one level
+ * to the server's two loader threads, which upload them on their own
+ * contexts and streams while the step computes; then advances every uploaded hierarchy by one level
  * with batched launches shared by all of them (results equal the single
  * build's); then retires complete ones.  A request is reported active from
  * admission on.

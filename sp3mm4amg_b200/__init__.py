@@ -510,7 +510,7 @@ class Server:
     def step(self) -> int:
         pending = ctypes.c_int()
         self.ctx._check(self.ctx.lib.sp3mm_server_step(self.h, ctypes.byref(pending)))
-        # The loader thread reads a request's host arrays until its upload is
+        # The loader threads read a request's host arrays until its upload is
         # done; drop them once the request has finished.
         for rid in [r for r in self._inputs
                     if self.poll(r)[0] in (self.DONE, self.FAILED, self.TAKEN)]:
