@@ -241,7 +241,9 @@ SP3MM_API int sp3mm_ctx_set_stream(sp3mm_ctx *ctx, void *stream);
 SP3MM_API void *sp3mm_ctx_stream(sp3mm_ctx *ctx);
 /* Bytes of device memory the context may hold for workspace (0: no limit). */
 SP3MM_API int sp3mm_ctx_set_workspace_limit(sp3mm_ctx *ctx, size_t bytes);
-/* Release cached workspace. */
+/* Release cached workspace: the device memory pool's idle memory, this
+ * context's page-locked staging and the process-wide cache of staging
+ * buffers that destroyed contexts gave back. */
 SP3MM_API int sp3mm_ctx_trim(sp3mm_ctx *ctx);
 /* Last error message of this context (static storage of the context). */
 SP3MM_API const char *sp3mm_ctx_last_error(sp3mm_ctx *ctx);

@@ -258,6 +258,11 @@ class Context:
         depend on it -- rows whose tables overflow are recomputed."""
         self._check(self.lib.sp3mm_ctx_set_tuning(self.h, lanes_per_row, d1, d2))
 
+    def trim(self) -> None:
+        """Release cached workspace: the device pool's idle memory and the
+        page-locked staging (this context's and the process-wide cache)."""
+        self._check(self.lib.sp3mm_ctx_trim(self.h))
+
     def set_profiling(self, on: bool) -> None:
         """Time every kernel launch with CUDA events on the context stream."""
         self._check(self.lib.sp3mm_ctx_set_profiling(self.h, 1 if on else 0))

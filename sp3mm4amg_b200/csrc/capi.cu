@@ -675,6 +675,16 @@ public:
         }
         cudaFreeHost(p);
     }
+    // Free every cached buffer.
+    void drain() {
+        std::multimap<size_t, void*> all;
+        {
+            std::lock_guard<std::mutex> lk(mu_);
+            all.swap(free_);
+            held_ = 0;
+        }
+        for (auto& kv : all) cudaFreeHost(kv.second);
+    }
 
 private:
     static constexpr size_t kMaxHeld = size_t(1) << 30;
@@ -1375,6 +1385,12 @@ int sp3mm_ctx_trim(sp3mm_ctx* ctx) {
     cudaMemPool_t pool;
     CK(ctx, cudaDeviceGetDefaultMemPool(&pool, ctx->device));
     CK(ctx, cudaMemPoolTrimTo(pool, 0));
+    // Page-locked staging: this context's (allocated again on next use) and
+    // the process-wide cache of buffers other contexts gave back.
+    if (ctx->host_stage) CK(ctx, cudaFreeHost(ctx->host_stage));
+    ctx->host_stage = nullptr;
+    ctx->host_stage_bytes = 0;
+    pinned_cache().drain();
     return SP3MM_OK;
 }
 

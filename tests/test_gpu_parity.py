@@ -291,3 +291,24 @@ def test_pinned_and_pageable_inputs_agree(golden, off):
         b = S.sp3mm(g["R"], g["A"], g["P"], name, off_f=off, pinned=False)
         assert_same(a, want, what=f"{name} pinned")
         assert_same(b, want, what=f"{name} pageable")
+
+
+def test_trim_releases_staging_and_transfers_continue(golden):
+    # Page-locked staging given back by a destroyed context is cached for the
+    # next one; trim frees it (and the context's own) and later transfers
+    # allocate staging again, with the same results.
+    A = golden[sorted(golden)[0]]["A"]
+    with S.Context() as first:
+        d = first.upload(A)
+        d.download()
+        d.free()
+    with S.Context() as ctx:
+        for _ in range(2):
+            ctx.trim()
+            d = ctx.upload(A)
+            got = d.download()
+            d.free()
+            assert np.array_equal(got.indptr, A.indptr)
+            assert np.array_equal(got.indices, A.indices)
+            assert np.array_equal(np.asarray(got.data).view(np.int64),
+                                  np.asarray(A.data, np.float64).view(np.int64))
