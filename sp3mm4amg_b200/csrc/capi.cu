@@ -25,6 +25,7 @@
 #include <sys/mman.h>
 
 #include "context.cuh"
+#include "host_pool.h"
 #include "kernels.cuh"
 #include "sp3mm_b200.h"
 #include "sp3mm_internal.cuh"
@@ -725,78 +726,9 @@ int host_stage(sp3mm_ctx* ctx, size_t bytes, void** out) {
     return SP3MM_OK;
 }
 
-// Persistent host workers for the transfer loops (narrowing, widening,
-// copies into caller arrays): creating threads per call cost more than the
-// work of a call.  One caller at a time uses the pool; a concurrent caller
-// (e.g. the server's loader thread) spawns its own threads instead.  The
-// pool is never destroyed (detached workers end with the process).
-class HostPool {
-public:
-    explicit HostPool(int n) : nthreads_(n) {
-        for (int k = 0; k < n; ++k) std::thread([this] { work(); }).detach();
-    }
-    int size() const { return nthreads_; }
-    std::mutex use;
-    // Run fn over `chunks` pieces [i*chunk, min(n, (i+1)*chunk)); the caller
-    // takes pieces too and returns when all are done.
-    void run(const std::function<void(long long, long long)>& fn, long long n, long long chunk,
-             int chunks) {
-        {
-            std::lock_guard<std::mutex> lk(m_);
-            fn_ = &fn;
-            n_ = n;
-            chunk_ = chunk;
-            chunks_ = chunks;
-            next_.store(0);
-            finished_ = 0;
-            ++gen_;
-        }
-        cv_.notify_all();
-        pull();
-        std::unique_lock<std::mutex> lk(m_);
-        done_.wait(lk, [&] { return finished_ == chunks_; });
-        fn_ = nullptr;
-    }
-
-private:
-    void pull() {
-        int done = 0;
-        for (;;) {
-            const int i = next_.fetch_add(1);
-            if (i >= chunks_) break;
-            const long long lo = i * chunk_;
-            const long long hi = std::min(n_, lo + chunk_);
-            (*fn_)(lo, hi);
-            ++done;
-        }
-        if (done) {
-            std::lock_guard<std::mutex> lk(m_);
-            finished_ += done;
-            if (finished_ == chunks_) done_.notify_all();
-        }
-    }
-    void work() {
-        unsigned seen = 0;
-        for (;;) {
-            {
-                std::unique_lock<std::mutex> lk(m_);
-                cv_.wait(lk, [&] { return gen_ != seen; });
-                seen = gen_;
-                if (!fn_) continue;
-            }
-            pull();
-        }
-    }
-    const int nthreads_;
-    std::mutex m_;
-    std::condition_variable cv_, done_;
-    const std::function<void(long long, long long)>* fn_ = nullptr;
-    long long n_ = 0, chunk_ = 1;
-    int chunks_ = 0, finished_ = 0;
-    std::atomic<int> next_{0};
-    unsigned gen_ = 0;
-};
-
+// Persistent host workers for the transfer loops (host_pool.h).  One
+// caller at a time uses the pool; a concurrent caller (e.g. a server's
+// second loader thread) spawns its own threads instead.
 HostPool& host_pool() {
     static HostPool* pool = [] {
         const unsigned hw = std::thread::hardware_concurrency();
