@@ -24,6 +24,7 @@
 
 #include <sys/mman.h>
 
+#include "buffer_cache.h"
 #include "context.cuh"
 #include "host_pool.h"
 #include "kernels.cuh"
@@ -637,66 +638,27 @@ int rap_impl(sp3mm_ctx* ctx, const sp3mm_dcsr& R, const sp3mm_dcsr& A, const sp3
 // Pinned staging of at least `bytes` (at most kHostStageMax) on the context.
 constexpr size_t kHostStageMax = size_t(256) << 20;
 
-// Page-locked staging buffers outlive the contexts that used them: a
-// process-wide cache hands the buffer of a destroyed (or grown) context to
-// the next context that needs one.  cudaHostAlloc costs about 0.4 ms per MB
-// (100 ms for 256 MB on a B200 host), ten times the copy it stages, and a
-// server creates its loader context per instance, a caller thread its
-// context per thread.  A buffer is given back only after its context's
-// stream has been synchronised, so no copy from it is in flight.
-class PinnedCache {
-public:
-    // A cached buffer of at least `bytes`, else a new one; *got = its size.
-    void* take(size_t bytes, size_t* got) {
-        {
-            std::lock_guard<std::mutex> lk(mu_);
-            auto it = free_.lower_bound(bytes);
-            if (it != free_.end()) {
-                void* p = it->second;
-                *got = it->first;
-                held_ -= it->first;
-                free_.erase(it);
-                return p;
-            }
-        }
+// Page-locked staging buffers outlive the contexts that used them
+// (buffer_cache.h): cudaHostAlloc costs about 0.4 ms per MB (100 ms for
+// 256 MB on a B200 host), ten times the copy it stages, and a server
+// creates its loader contexts per instance, a caller thread its context per
+// thread.  A buffer is given back only after its context's stream has been
+// synchronised, so no copy from it is in flight.
+struct PinnedAlloc {
+    void* operator()(size_t bytes) const {
         void* p = nullptr;
         if (cudaHostAlloc(&p, bytes, cudaHostAllocPortable) != cudaSuccess) return nullptr;
-        *got = bytes;
         return p;
     }
-    void give(void* p, size_t bytes) {
-        if (!p) return;
-        {
-            std::lock_guard<std::mutex> lk(mu_);
-            if (held_ + bytes <= kMaxHeld) {
-                free_.emplace(bytes, p);
-                held_ += bytes;
-                return;
-            }
-        }
-        cudaFreeHost(p);
-    }
-    // Free every cached buffer.
-    void drain() {
-        std::multimap<size_t, void*> all;
-        {
-            std::lock_guard<std::mutex> lk(mu_);
-            all.swap(free_);
-            held_ = 0;
-        }
-        for (auto& kv : all) cudaFreeHost(kv.second);
-    }
-
-private:
-    static constexpr size_t kMaxHeld = size_t(1) << 30;
-    std::mutex mu_;
-    std::multimap<size_t, void*> free_;
-    size_t held_ = 0;
 };
+struct PinnedRelease {
+    void operator()(void* p) const { cudaFreeHost(p); }
+};
+using PinnedCache = BufferCache<PinnedAlloc, PinnedRelease>;
 
 // Never destroyed: cached buffers are released with the process.
 PinnedCache& pinned_cache() {
-    static PinnedCache* c = new PinnedCache();
+    static PinnedCache* c = new PinnedCache(PinnedAlloc{}, PinnedRelease{}, size_t(1) << 30);
     return *c;
 }
 

@@ -1,5 +1,5 @@
 // Stress test of sp3mm::HostPool (sp3mm4amg_b200/csrc/host_pool.h), built
-// and run by tests/test_host_pool.py: many short runs back to back, so that
+// and run by tests/test_host_native.py: many short runs back to back, so that
 // workers wake late for runs that already finished.  Every index of every
 // run must be processed exactly once, and no chunk may still be running
 // when run() returns.
