@@ -59,6 +59,10 @@ def parse_args():
     ap.add_argument("--side", type=int, default=128, help="grid side of the 3D problem")
     ap.add_argument("--e2e-steps", type=int, default=3)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--ref-seconds", type=float, default=2.5,
+                    help="seconds of reference work per step of --impl reference")
+    ap.add_argument("--no-ref-full", action="store_true",
+                    help="--impl reference: skip the one unsampled full product")
     ap.add_argument("--cpu-seconds", type=float, default=12.0,
                     help="target CPU time of the cpu_baseline sample")
     ap.add_argument("--no-batched", action="store_true", help="skip the batched workload")
@@ -147,13 +151,25 @@ def smi_index(local_rank: int) -> int:
 # CPU baseline: the reference's own OpenMP code (oracle/_ref) on a bounded
 # row sample of the same product, extrapolated to the full product.
 
-def cpu_reference_runner(prob, threads):
-    """Returns (kind, fn(rows) -> seconds, description)."""
+def cpu_reference_runner(prob, threads, variant="direct"):
+    """Returns (kind, fn(rows) -> seconds, description) for the reference's
+    own code (oracle/_ref) on the first `rows` rows of R: the direct
+    upper-bound product sp3mmRowByRowMerged_0 -- the variant the main line
+    runs -- or (variant "pair") sp3mmRowByRowPair_0 with spmmRowByRow_0."""
     os.environ["OMP_NUM_THREADS"] = str(threads)
     import oracle
     try:
         ref = oracle.Reference(threads=threads)
         ref.adapt_grid(0)
+        if variant == "direct":
+            def run(rows):
+                Rs = prob.R.rows(0, rows)
+                t0 = time.perf_counter()
+                ref.sp3mm_direct(Rs, prob.A, prob.P, 0)
+                return time.perf_counter() - t0
+            return ("reference", run,
+                    "reference sp3mmRowByRowMerged_0 (direct, upper-bound: the main line's "
+                    "variant)")
 
         def run(rows):
             Rs = prob.R.rows(0, rows)
@@ -161,8 +177,7 @@ def cpu_reference_runner(prob, threads):
             ref.sp3mm_pair("spmmRowByRow_", Rs, prob.A, prob.P, 0)
             return time.perf_counter() - t0
         return ("reference", run,
-                "reference sp3mmRowByRowPair_0 with spmmRowByRow_0 (upper-bound 1D, its "
-                "fastest variant here)")
+                "reference sp3mmRowByRowPair_0 with spmmRowByRow_0 (pair-wise, upper-bound 1D)")
     except (FileNotFoundError, OSError):
         orc = oracle.Oracle()
         orc.set_threads(threads)
@@ -170,9 +185,12 @@ def cpu_reference_runner(prob, threads):
         def run(rows):
             Rs = prob.R.rows(0, rows)
             t0 = time.perf_counter()
-            orc.sp3mm_pair(Rs, prob.A, prob.P)
+            if variant == "direct":
+                orc.sp3mm_direct(Rs, prob.A, prob.P)
+            else:
+                orc.sp3mm_pair(Rs, prob.A, prob.P)
             return time.perf_counter() - t0
-        return "port", run, "oracle restatement (pair), reference library not built"
+        return "port", run, f"oracle restatement ({variant}), reference library not built"
 
 
 def calibrated_sample(run, M, seconds):
@@ -186,28 +204,54 @@ def calibrated_sample(run, M, seconds):
 
 
 def run_reference_arm(args, prob, nnz_c):
+    """The reference's own CPU code on the main line's product (direct,
+    upper-bound) with all host threads: each step a row sample of R, its
+    time scaled to the whole product (the reference's cost is linear in the
+    rows of R: every row resets its dense accumulators); once per run the
+    whole product unsampled (`full_product`, unless --no-ref-full), which
+    checks that scaling; and a sample of the pair-wise upper-bound product
+    (`pair_ub`) beside it."""
     threads = os.cpu_count() or 1
     total_bytes = prob.compulsory_bytes(nnz_c=nnz_c, idx_bytes=4)
-    kind, run, desc = cpu_reference_runner(prob, threads)
+    ref_variant = "direct" if args.variant == "direct" else "pair"
+    kind, run, desc = cpu_reference_runner(prob, threads, ref_variant)
     M = prob.R.M
-    rows = calibrated_sample(run, M, 4.0)
-    vals = []
+    rows = calibrated_sample(run, M, args.ref_seconds)
+    vals, times = [], []
     for i in range(args.warmup + args.steps):
         t = run(rows)
         if i >= args.warmup:
+            times.append(t)
             vals.append(total_bytes / (t * M / rows) / 1e9)
     value = statistics.median(vals)
+    scaled_s = statistics.median(times) * M / rows
     sample = f"rows 0..{rows} of {M} of R per step ({desc}), time scaled by {M}/{rows}"
+    full = None
+    if not args.no_ref_full:
+        t_full = run(M) if rows < M else statistics.median(times)
+        full = {"seconds": t_full, "value": total_bytes / t_full / 1e9, "unit": "GB/s",
+                "scaled_estimate_s": scaled_s, "scaled_over_full": scaled_s / t_full}
+    pkind, prun, pdesc = cpu_reference_runner(prob, threads, "pair")
+    prows = calibrated_sample(prun, M, args.ref_seconds)
+    ptimes = [prun(prows) for _ in range(3)]
+    pair = {"value": total_bytes / (statistics.median(ptimes) * M / prows) / 1e9, "unit": "GB/s",
+            "seconds_per_product": statistics.median(ptimes) * M / prows,
+            "sample": f"rows 0..{prows} of {M} of R, median of 3 ({pdesc})"}
     line = {
         "impl": "reference", "metric": "rap_compulsory_GBps", "value": value, "unit": "GB/s",
         "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
         "ms_per_step": total_bytes / (value * 1e9) * 1e3, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-        "config": {"workload": workload_name(args.side), "variant": "pair", "flavour": "ub"},
+        "config": {"workload": workload_name(args.side), "variant": args.variant,
+                   "flavour": args.flavour, "rows_R": M, "nnz_A": prob.A.nnz,
+                   "nnz_P": prob.P.nnz, "nnz_C": nnz_c, "bytes_per_product": total_bytes,
+                   "byte_basis": "int32 idx + f64 val"},
         "cpu_baseline": {"value": value, "unit": "GB/s", "cores": threads, "kind": kind,
                          "sample": sample},
         "e2e": {"value": value, "unit": "GB/s", "h2d_bytes_per_step": 0,
                 "d2h_bytes_per_step": 0},
+        "full_product": full,
+        "pair_ub": pair,
     }
     print(json.dumps(line), flush=True)
 
@@ -392,7 +436,7 @@ def run_library(torch, prob, steps=5):
         return {"library": "cuSPARSE SpGEMM via torch sparse CSR", "unavailable": repr(e)[:200]}
 
 
-def run_served(S, ctx, count, rate, seed=4):
+def run_served(S, ctx, count, rate, seed=4, reps=3):
     """A Poisson stream of hierarchy-setup requests (90% of config-3 sizes,
     10% 3D 64^3..128^3) served by continuous batching versus one request at
     a time, at `rate` requests/s and saturated (all arriving at once)."""
@@ -400,42 +444,63 @@ def run_served(S, ctx, count, rate, seed=4):
     specs = pb.config4_specs(seed, count)
     ops = [pb.stencil_operator(d) for d in specs]
     arrivals = pb.poisson_arrivals(rate, count, seed + 1)
-    # Warm-up at full size (the memory pool grows to the workload's needs).
-    serving.serve_batched(ctx, specs, np.zeros(count), operators=ops)
+    # Warm-up at full size in both value types (the memory pool grows to the
+    # workload's needs; every kernel instantiation is loaded).
+    for cvt in (S.F64, S.F32):
+        serving.serve_batched(ctx, specs, np.zeros(count), coarse_val_type=cvt, operators=ops)
+    serving.serve_plain(ctx, specs[:8], np.zeros(8), operators=ops[:8])
     res = {"workload": f"{count} requests (seed {seed}): 90% 2D/3D n log-uniform 1e3..2e5, "
                        f"10% 3D side 64..128; hierarchy to n < 1000",
-           "rate_per_s": rate}
+           "rate_per_s": rate, "repeats": reps}
+    runs = {"fp64": [], "fp32_coarse": [], "plain_fp64": []}
+    for _ in range(reps):
+        for name, cvt in (("fp64", S.F64), ("fp32_coarse", S.F32)):
+            st, _ = serving.serve_batched(ctx, specs, arrivals, coarse_val_type=cvt,
+                                          operators=ops)
+            sat, _ = serving.serve_batched(ctx, specs, np.zeros(count), coarse_val_type=cvt,
+                                           operators=ops)
+            runs[name].append((st, sat))
+        plain = serving.serve_plain(ctx, specs, arrivals, operators=ops)
+        plain_sat = serving.serve_plain(ctx, specs, np.zeros(count), operators=ops)
+        runs["plain_fp64"].append((plain, plain_sat))
+
+    def med(xs):
+        return float(np.median(xs))
+    for name, rr in runs.items():
+        res[name] = {"p50_s": med([st["p50_s"] for st, _ in rr]),
+                     "p99_s": med([st["p99_s"] for st, _ in rr]),
+                     "p99_s_each": [st["p99_s"] for st, _ in rr],
+                     "products_per_s": med([st["products_per_s"] for st, _ in rr]),
+                     "products": rr[0][0]["products"],
+                     "saturated_products_per_s": med([sat["products_per_s"] for _, sat in rr]),
+                     "saturated_products_per_s_each": [sat["products_per_s"] for _, sat in rr],
+                     "saturated_p99_s": med([sat["p99_s"] for _, sat in rr])}
+        if name != "plain_fp64":
+            res[name]["peak_active"] = max(st["peak_active"] for st, _ in rr)
+            res[name]["failed"] = sum(st["failed"] + sat["failed"] for st, sat in rr)
     kept = {}
     for name, cvt in (("fp64", S.F64), ("fp32_coarse", S.F32)):
-        st, _ = serving.serve_batched(ctx, specs, arrivals, coarse_val_type=cvt, operators=ops)
-        sat, kept[name] = serving.serve_batched(ctx, specs, np.zeros(count), coarse_val_type=cvt,
-                                                operators=ops, keep=True)
-        res[name] = {"p50_s": st["p50_s"], "p99_s": st["p99_s"],
-                     "products_per_s": st["products_per_s"], "products": st["products"],
-                     "peak_active": st["peak_active"], "failed": st["failed"],
-                     "saturated_products_per_s": sat["products_per_s"],
-                     "saturated_p99_s": sat["p99_s"]}
+        _, kept[name] = serving.serve_batched(ctx, specs, np.zeros(count), coarse_val_type=cvt,
+                                              operators=ops, keep=True)
     # FP32 coarse storage: every request's every level against its FP64
     # hierarchy (which equals the oracle chain bit for bit), on the device.
     per_level = {}
     for a, b in zip(kept["fp32_coarse"], kept["fp64"]):
-        for lvl, (rel, norm) in enumerate(serving.level_errors(a, b)):
-            per_level.setdefault(lvl, []).append((rel, norm))
+        for lvl, e in enumerate(serving.level_errors(a, b)):
+            per_level.setdefault(lvl, []).append(e)
         a.free()
         b.free()
-    res["fp32_level_max_rel_err"] = {str(l): max(r for r, _ in v) for l, v in sorted(per_level.items())}
-    res["fp32_level_median_rel_err"] = {str(l): float(np.median([r for r, _ in v]))
-                                        for l, v in sorted(per_level.items())}
-    res["fp32_level_max_err_over_max"] = {str(l): max(n for _, n in v)
-                                          for l, v in sorted(per_level.items())}
+    lv = sorted(per_level.items())
+    res["fp32_level_max_rel_err"] = {str(l): max(e[0] for e in v) for l, v in lv}
+    res["fp32_level_median_rel_err"] = {str(l): float(np.median([e[0] for e in v]))
+                                        for l, v in lv}
+    res["fp32_level_max_err_over_max"] = {str(l): max(e[1] for e in v) for l, v in lv}
+    # How many entries the large relative errors are (cancellation near zero).
+    res["fp32_level_entries_rel_err_over_1e-3"] = {str(l): sum(e[2] for e in v) for l, v in lv}
+    res["fp32_level_entries"] = {str(l): sum(e[3] for e in v) for l, v in lv}
     res["fp32_error_coverage"] = f"all {count} requests, every level (device comparison)"
-    plain = serving.serve_plain(ctx, specs, arrivals, operators=ops)
-    plain_sat = serving.serve_plain(ctx, specs, np.zeros(count), operators=ops)
-    res["plain_fp64"] = {"p50_s": plain["p50_s"], "p99_s": plain["p99_s"],
-                         "products_per_s": plain["products_per_s"],
-                         "saturated_products_per_s": plain_sat["products_per_s"]}
     res["saturated_speedup_fp64"] = (res["fp64"]["saturated_products_per_s"] /
-                                     plain_sat["products_per_s"])
+                                     res["plain_fp64"]["saturated_products_per_s"])
     return res
 
 
@@ -619,7 +684,8 @@ def main():
         line["hierarchy"] = run_hierarchy(S, torch, ctx, stream, side=args.side)
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         threads = os.cpu_count() or 1
-        kind, run, desc = cpu_reference_runner(prob, threads)
+        kind, run, desc = cpu_reference_runner(
+            prob, threads, "direct" if args.variant == "direct" else "pair")
         rows = calibrated_sample(run, prob.R.M, args.cpu_seconds)
         t = run(rows)
         full = t * prob.R.M / rows

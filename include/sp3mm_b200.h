@@ -157,6 +157,29 @@ SP3MM_API idx_t *spMMSizeUpperboundColParts_0(spmat *A, spmat *B, unsigned short
 SP3MM_API idx_t *spMMSizeUpperboundColParts_1(spmat *A, spmat *B, unsigned short gridCols,
                                     idx_t *bColPartOffsets);
 
+/* 2D column partitioning of a host CSR into gridCols uniform column ranges
+ * (the first N % gridCols ranges one column wider).
+ * colsOffsetsPartitioningUnifRanges_: malloc'd idx_t[A->M*gridCols + 1],
+ * entry [r*gridCols + gc] the 0-based JA/AS position of row r's first entry
+ * in range gc, NZ at the end (the input spMMSizeUpperboundColParts_ takes).
+ * colsPartitioningUnifRanges_ / ...OffsetsAux_: a calloc'd array of gridCols
+ * spmat, range gc as an A->M x width matrix with 0-based IRP and JA/AS
+ * copies (column indices unchanged); free each one's IRP, JA and AS, then
+ * the array, with free() (the reference's freeSpmatInternal + free).  The Aux form also returns the offsets through
+ * *colPartsOffsets when that pointer is not NULL.  NULL plus a message on
+ * stderr on error (including gridCols == 0); an empty range gets NULL JA/AS
+ * where the reference fails the call.
+ * Replace code/src/include/sparseUtilsGeneric.h:43-52
+ * (code/src/commons/sparseUtilsGeneric.c:284-400). */
+SP3MM_API idx_t *colsOffsetsPartitioningUnifRanges_0(spmat *A, unsigned int gridCols);
+SP3MM_API idx_t *colsOffsetsPartitioningUnifRanges_1(spmat *A, unsigned int gridCols);
+SP3MM_API spmat *colsPartitioningUnifRanges_0(spmat *A, unsigned int gridCols);
+SP3MM_API spmat *colsPartitioningUnifRanges_1(spmat *A, unsigned int gridCols);
+SP3MM_API spmat *colsPartitioningUnifRangesOffsetsAux_0(spmat *A, unsigned int gridCols,
+                                                        idx_t **colPartsOffsets);
+SP3MM_API spmat *colsPartitioningUnifRangesOffsetsAux_1(spmat *A, unsigned int gridCols,
+                                                        idx_t **colPartsOffsets);
+
 /* MatrixMarket coordinate file -> host CSR spmat, 0-based, the arrays from
  * malloc/calloc (freeSpmat releases them); NULL plus a message on stderr on
  * error.  Replaces code/src/lib/parser.c:126-330 (MMtoCSR over MMRead,
@@ -310,8 +333,10 @@ SP3MM_API int sp3mm_transpose(sp3mm_ctx *ctx, const sp3mm_dcsr *A, sp3mm_dcsr *A
  * SP3MM_ENOMEM having written only c_row_ptr (call again with larger
  * arrays).  Temporaries live in a fixed 64 MiB device array inside the
  * library (held on every device that uses it until the process exits), which
- * bounds R->M to about 2.7 million rows (SP3MM_ELIMIT beyond) and requires
- * every row's hash tables to fit in shared memory.  The first call on a
+ * bounds R->M to about 3.19 million rows (SP3MM_ELIMIT beyond, with the
+ * exact limit in the message) and requires every row's hash tables to fit
+ * in shared memory; C's nonzero count must stay below 2^31.  Operands whose
+ * max_row is -1 are measured on the device.  The first call on a
  * device looks up that array's address; make it before any stream capture.
  * Calls whose GPU work overlaps share the array and race: serialise them.
  * `stream` is a cudaStream_t (NULL: the legacy default stream). */

@@ -27,14 +27,21 @@ from sp3mm4amg_b200.spmat import (CONFIG, CONFIG_P, SPMAT_P, SPMM_INTERF, HostSp
 HERE = os.path.dirname(os.path.abspath(__file__))
 ORACLE_SO = os.path.join(HERE, "lib", "liboracle_sp3mm.so")
 REF_SO = os.path.join(HERE, "_ref", "libsp3mm_ref.so")
-REF_SRC = "/root/reference/code/src"
+# Root of the reference project's tree, read only by this test
+# infrastructure (building _ref, regenerating the golden fixtures): the
+# SP3MM_REFERENCE_ROOT environment variable, else the read-only checkout the
+# project is developed beside.  Where neither exists, the tests that need the
+# tree itself skip and the committed fixtures under tests/golden stand in.
+REF_ROOT = os.environ.get("SP3MM_REFERENCE_ROOT", "/root/reference")
+REF_SRC = os.path.join(REF_ROOT, "code", "src")
+REF_TEST_DIR = os.path.join(REF_ROOT, "code", "test")
 
 
 def build(ref: bool = True) -> None:
     """Compile the oracle (and the reference library when its tree exists)."""
     targets = ["all"]
     if ref and os.path.isdir(REF_SRC):
-        targets.append("ref")
+        targets += ["ref", f"REF_SRC={REF_SRC}"]
     subprocess.run(["make", "-s", "-C", HERE, *targets], check=True)
 
 

@@ -107,6 +107,12 @@ DEVICE_API = {
 # Host-side MatrixMarket entry points with (restype, argtypes).
 HOST_API = {
     "MMtoCSR": (_c.c_void_p, [_c.c_char_p]),
+    "colsOffsetsPartitioningUnifRanges_0": (_c.c_void_p, [SPMAT_P, _c.c_uint]),
+    "colsOffsetsPartitioningUnifRanges_1": (_c.c_void_p, [SPMAT_P, _c.c_uint]),
+    "colsPartitioningUnifRanges_0": (_c.c_void_p, [SPMAT_P, _c.c_uint]),
+    "colsPartitioningUnifRanges_1": (_c.c_void_p, [SPMAT_P, _c.c_uint]),
+    "colsPartitioningUnifRangesOffsetsAux_0": (_c.c_void_p, [SPMAT_P, _c.c_uint, _c.c_void_p]),
+    "colsPartitioningUnifRangesOffsetsAux_1": (_c.c_void_p, [SPMAT_P, _c.c_uint, _c.c_void_p]),
     "sp3mm_write_mm": (_c.c_int, [SPMAT_P, _c.c_int, _c.c_char_p]),
     "sp3mm_spmat_sort_rows": (_c.c_int, [SPMAT_P, _c.c_int]),
 }

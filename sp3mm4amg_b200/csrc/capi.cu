@@ -199,6 +199,20 @@ struct RowRunner {
     // Longest row of the right operands (first / last; -1: unknown).
     int a_max = -1, b_max = -1;
 
+    // Whether a direct launch runs the register-product kernel: by default
+    // (no lane tuning) when every A and P row holds at most 32 entries
+    // (known longest rows) and the tables fit shared memory; never the retry
+    // launch, which the warp kernels run with proven tables.
+    // Whether a direct launch runs the register-product kernel (rowlanes.cuh):
+    // by default (no lane tuning) when every A and P row holds at most 32
+    // entries (known longest rows) and the tables fit shared memory; never
+    // the retry launch, which the warp kernels run with proven tables.
+    bool use_lanes(const RowParams& p, int G) const {
+        if (ctx->tune_G != 0 || G != 32 || !p.retry_rows) return false;
+        if (a_max < 0 || a_max > 32 || b_max < 0 || b_max > 32) return false;
+        return p.S2 <= p.S1;
+    }
+
     long long operand_nnz() const {
         return direct ? da.R.nnz + da.A.nnz + da.P.nnz : pa.A.nnz + pa.B.nnz;
     }
@@ -215,6 +229,32 @@ struct RowRunner {
                 return set_error(ctx, SP3MM_ECUDA, "dense row kernel launch failed: %s",
                                  cudaGetErrorString(e));
             return SP3MM_OK;
+        }
+        if (direct && use_lanes(p, G)) {
+            const size_t per_warp = lanes_row_bytes(mode, p.S1, p.S2);
+            int warps = static_cast<int>(ctx->smem_budget / per_warp);
+            if (warps > 8) warps = 8;
+            if (warps >= 1) {
+                RowGeom geo{};
+                geo.G = 32;
+                geo.block = 32 * warps;
+                geo.smem = per_warp * warps;
+                const long long grid = (p.nrows + warps - 1) / warps;
+                const long long cap = static_cast<long long>(ctx->num_sms) * 16;
+                geo.grid = static_cast<int>(grid < cap ? grid : cap);
+                p.gtab = nullptr;
+                p.lg1 = ilog2_pow2(next_pow2(static_cast<unsigned>(a_max > 0 ? a_max : 1)));
+                p.lg2 = ilog2_pow2(next_pow2(static_cast<unsigned>(b_max > 0 ? b_max : 1)));
+                static const char* const kLanes[3] = {"direct.lanes.symb", "direct.lanes.num",
+                                                      "direct.lanes.book"};
+                cudaError_t e = cudaSuccess;
+                prof(ctx, kLanes[mode],
+                     [&] { e = launch_direct_lanes(da, p, mode, geo, ctx->stream); });
+                if (e != cudaSuccess)
+                    return set_error(ctx, SP3MM_ECUDA, "lanes row kernel launch failed: %s",
+                                     cudaGetErrorString(e));
+                return SP3MM_OK;
+            }
         }
         const size_t per_group = row_table_bytes(direct, mode, G, p.S1, p.S2);
         const int gpw = 32 / G;
@@ -326,24 +366,36 @@ int finish_matrix(sp3mm_dcsr* C, DevBuf& rp, DevBuf& ci, DevBuf& v) {
     return SP3MM_OK;
 }
 
-// Scan row counts into a fresh row_ptr; returns the total.
+// A result's row_ptr allocation: row_ptr[M+1], the longest row in the slot
+// after it, then (8-byte aligned) the 64-bit total of the row counts, which
+// tells a total past the int32 range from one the 32-bit scan wrapped.
+size_t rp_bytes(int M) { return ((static_cast<size_t>(M) + 2) * 4 + 7) / 8 * 8 + 8; }
+unsigned long long* rp_sum(const DevBuf& rp, int M) {
+    return reinterpret_cast<unsigned long long*>(rp.as<unsigned char>() + rp_bytes(M) - 8);
+}
+
+// Scan row counts into a fresh row_ptr; returns the total (64-bit: a total
+// of 2^31 or more is reported as such, not wrapped).
 int scan_counts(sp3mm_ctx* ctx, int M, const int* row_cnt, DevBuf& rp, long long* total,
                 int* max_row = nullptr) {
-    TRY(rp.alloc(ctx, sizeof(int) * (static_cast<size_t>(M) + 2)));
+    TRY(rp.alloc(ctx, rp_bytes(M)));
     DevBuf tmp;
     const size_t tb = scan_temp_bytes(M);
     TRY(tmp.alloc(ctx, tb));
     prof(ctx, "scan", [&] { launch_scan(M, row_cnt, rp.as<int>(), tmp.p, tb, ctx->stream); });
     CK(ctx, cudaGetLastError());
-    // The longest row rides in the slot after row_ptr[M].
     int* mr = rp.as<int>() + M + 1;
+    unsigned long long* sum = rp_sum(rp, M);
     CK(ctx, cudaMemsetAsync(mr, 0, sizeof(int), ctx->stream));
-    launch_count_max(M, row_cnt, nullptr, mr, ctx->stream);
+    CK(ctx, cudaMemsetAsync(sum, 0, sizeof(unsigned long long), ctx->stream));
+    launch_count_max(M, row_cnt, nullptr, mr, ctx->stream, sum);
     int t[2] = {0, 0};
+    unsigned long long t64 = 0;
     CK(ctx, cudaMemcpyAsync(t, rp.as<int>() + M, 2 * sizeof(int), cudaMemcpyDeviceToHost,
                             ctx->stream));
+    CK(ctx, cudaMemcpyAsync(&t64, sum, sizeof t64, cudaMemcpyDeviceToHost, ctx->stream));
     CK(ctx, cudaStreamSynchronize(ctx->stream));
-    *total = t[0];
+    *total = static_cast<long long>(t64);
     if (max_row) *max_row = t[1];
     return SP3MM_OK;
 }
@@ -362,23 +414,27 @@ struct TailReads {
 int scan_read(sp3mm_ctx* ctx, int M, const int* row_cnt, DevBuf& rp, const int* d_retry,
               TailReads* out) {
     const cudaStream_t st = ctx->stream;
-    if (!rp.p) TRY(rp.alloc(ctx, sizeof(int) * (static_cast<size_t>(M) + 2)));
+    if (!rp.p) TRY(rp.alloc(ctx, rp_bytes(M)));
     DevBuf tmp;
     const size_t tb = scan_temp_bytes(M);
     TRY(tmp.alloc(ctx, tb));
     prof(ctx, "scan", [&] { launch_scan(M, row_cnt, rp.as<int>(), tmp.p, tb, st); });
     CK(ctx, cudaGetLastError());
     int* mr = rp.as<int>() + M + 1;
+    unsigned long long* sum = rp_sum(rp, M);
     CK(ctx, cudaMemsetAsync(mr, 0, sizeof(int), st));
-    launch_count_max(M, row_cnt, nullptr, mr, st);
+    CK(ctx, cudaMemsetAsync(sum, 0, sizeof(unsigned long long), st));
+    launch_count_max(M, row_cnt, nullptr, mr, st, sum);
     unsigned* box = ctx->host_box;
     box[2] = 0;
     CK(ctx, cudaMemcpyAsync(box, rp.as<int>() + M, 2 * sizeof(int), cudaMemcpyDeviceToHost, st));
     if (d_retry)
         CK(ctx, cudaMemcpyAsync(box + 2, d_retry, sizeof(int), cudaMemcpyDeviceToHost, st));
     CK(ctx, cudaMemcpyAsync(box + 3, ctx->d_err, sizeof(unsigned), cudaMemcpyDeviceToHost, st));
+    CK(ctx, cudaMemcpyAsync(box + 4, sum, sizeof(unsigned long long), cudaMemcpyDeviceToHost,
+                            st));
     CK(ctx, cudaStreamSynchronize(st));
-    out->total = static_cast<int>(box[0]);
+    out->total = static_cast<long long>(*reinterpret_cast<unsigned long long*>(box + 4));
     out->max_row = static_cast<int>(box[1]);
     out->retry = static_cast<int>(box[2]);
     out->err = box[3];
@@ -586,8 +642,9 @@ int direct_impl(sp3mm_ctx* ctx, const sp3mm_dcsr& R, const sp3mm_dcsr& A, const 
     const int G = pick_group(ctx, mean);
     const int d1 = ctx->tune_d1 >= 0 ? ctx->tune_d1 : 2;
     const int d2 = ctx->tune_d2 >= 0 ? ctx->tune_d2 : 0;
-    int pmax = 0;
+    int pmax = 0, amax = 0;
     TRY(known_max_row(ctx, P, &pmax));
+    TRY(known_max_row(ctx, A, &amax));
     DevBuf cnt_buf, need, need_opt;
     TRY(cnt_buf.alloc(ctx, sizeof(Counters)));
     TRY(need.alloc(ctx, sizeof(int) * (static_cast<size_t>(M) + 1)));
@@ -598,8 +655,7 @@ int direct_impl(sp3mm_ctx* ctx, const sp3mm_dcsr& R, const sp3mm_dcsr& A, const 
         launch_direct_bounds(view(R), view(A), pmax, need.as<int>(), &dc->total, st,
                              need_opt.as<int>(), d1);
     });
-    RowRunner rr{ctx, true, kSymb, DirectRowArgs{view(R), view(A), view(P)}, {}, A.max_row,
-                 P.max_row};
+    RowRunner rr{ctx, true, kSymb, DirectRowArgs{view(R), view(A), view(P)}, {}, amax, pmax};
     return product_rows(ctx, rr, M, P.N, flavour, out_vt, need, dc, G, d1, d2, A.N, P.N,
                         static_cast<double>(pmax), C, need_opt.as<int>());
 }

@@ -399,18 +399,30 @@ void launch_direct_bounds(const CsrView& R, const CsrView& A, int p_max_row, int
     note_launch();
 }
 
-__global__ void k_count_max(int M, const int* cnt, const int* rp, int* out) {
+__global__ void k_count_max(int M, const int* cnt, const int* rp, int* out,
+                            unsigned long long* sum) {
     int m = 0;
-    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < M; i += gridDim.x * blockDim.x)
-        m = max(m, cnt ? cnt[i] : rp[i + 1] - rp[i]);
+    unsigned long long t = 0;
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < M; i += gridDim.x * blockDim.x) {
+        const int c = cnt ? cnt[i] : rp[i + 1] - rp[i];
+        m = max(m, c);
+        t += static_cast<unsigned long long>(c);
+    }
 #pragma unroll
-    for (int o = 16; o > 0; o >>= 1) m = max(m, __shfl_xor_sync(0xffffffffu, m, o));
-    if ((threadIdx.x & 31) == 0 && m > 0) atomicMax(out, m);
+    for (int o = 16; o > 0; o >>= 1) {
+        m = max(m, __shfl_xor_sync(0xffffffffu, m, o));
+        t += __shfl_xor_sync(0xffffffffu, t, o);
+    }
+    if ((threadIdx.x & 31) == 0) {
+        if (m > 0) atomicMax(out, m);
+        if (sum && t) atomicAdd(sum, t);
+    }
 }
 
-void launch_count_max(int M, const int* cnt, const int* rp, int* out, cudaStream_t st) {
+void launch_count_max(int M, const int* cnt, const int* rp, int* out, cudaStream_t st,
+                      unsigned long long* sum) {
     if (M == 0) return;
-    k_count_max<<<grid_for(M, 256), 256, 0, st>>>(M, cnt, rp, out);
+    k_count_max<<<grid_for(M, 256), 256, 0, st>>>(M, cnt, rp, out, sum);
     note_launch();
 }
 

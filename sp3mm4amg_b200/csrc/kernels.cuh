@@ -54,6 +54,9 @@ struct RowParams {
     // Some row of the first (a_long, direct only) / last (b_long) right
     // operand is longer than the entries the kernel prefetches per step.
     bool a_long, b_long;
+    // Lanes per left-row step (log2) of the register-product direct kernel
+    // (rowlanes.cuh): stage 1 (R*A, A rows) and stage 2 (RA*P, P rows).
+    int lg1, lg2;
 };
 
 // Launch geometry of one row-kernel launch.
@@ -70,6 +73,12 @@ int row_table_limit(int S, int G);
 int row_prefetch_cover(int G);
 cudaError_t launch_direct_rows(const DirectRowArgs& a, const RowParams& p, int mode,
                                const RowGeom& geo, cudaStream_t st);
+// Direct rows with the products formed in registers (rowlanes.cuh): right
+// operands whose rows hold at most 32 entries (p.lg1 / p.lg2 set),
+// shared-memory tables.  lanes_row_bytes: table bytes per warp.
+cudaError_t launch_direct_lanes(const DirectRowArgs& a, const RowParams& p, int mode,
+                                const RowGeom& geo, cudaStream_t st);
+size_t lanes_row_bytes(int mode, int S1, int S2);
 // Tuning value of "lanes per row" that runs every direct row on the
 // CTA-per-row kernel.
 constexpr int kDenseLanes = 512;
@@ -92,8 +101,11 @@ void launch_pair_bounds(const CsrView& A, const CsrView& B, int* need,
 void launch_direct_bounds(const CsrView& R, const CsrView& A, int p_max_row, int* need,
                           unsigned long long* total, cudaStream_t st, int* need_opt = nullptr,
                           int d1 = 0);
-// *out = max(*out, largest cnt[i]) (cnt null: largest row length of rp).
-void launch_count_max(int M, const int* cnt, const int* rp, int* out, cudaStream_t st);
+// *out = max(*out, largest cnt[i]) (cnt null: largest row length of rp) and,
+// when `sum` is given, *sum += the 64-bit total of the row lengths (the
+// caller zeroes both).
+void launch_count_max(int M, const int* cnt, const int* rp, int* out, cudaStream_t st,
+                      unsigned long long* sum = nullptr);
 // need from exact counts: max(cnt[i], cnt1[i]) (cnt1 may be null).
 void launch_need_from_counts(int M, const int* cnt, const int* cnt1, int* need,
                              cudaStream_t st);

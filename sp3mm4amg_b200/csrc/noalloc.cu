@@ -38,8 +38,10 @@ constexpr int kMaxDevices = 64;
 
 static __device__ __align__(256) unsigned char g_noalloc_scratch[kScratchBytes];
 
-// Device address of the scratch array per device (set-up once per device).
+// Device address of the scratch array and SM count per device (set-up once
+// per device).
 unsigned char* g_scratch_addr[kMaxDevices] = {};
+int g_sms[kMaxDevices] = {};
 std::mutex g_setup_mutex;
 
 struct Head {
@@ -49,11 +51,23 @@ struct Head {
     int retry_count;
     unsigned long long total;
     unsigned err;
+    // Filled after the binning passes (run_direct clears the fields above):
+    // longest rows of A and P when the operands do not record them, and
+    // the longest C row with the 64-bit total of C's row counts.
+    int a_max, p_max, c_max;
+    unsigned long long c_total;
 };
 
 int fail(int code, const char* msg) {
     fprintf(stderr, "sp3mm_rap_direct_noalloc: %s\n", msg);
     return code;
+}
+
+// Map a device error word as sp3mm_rap does: malformed input is EINVAL.
+int device_fail(unsigned err, const char* pass) {
+    fprintf(stderr, "sp3mm_rap_direct_noalloc: device error flags 0x%x in the %s pass%s\n", err,
+            pass, (err & kErrInput) ? " (malformed CSR input)" : "");
+    return (err & kErrInput) ? SP3MM_EINVAL : SP3MM_EDEVICE;
 }
 
 #define NA_CK(call)                                                                     \
@@ -66,23 +80,50 @@ int fail(int code, const char* msg) {
         }                                                                               \
     } while (0)
 
-unsigned char* scratch_for(int dev) {
+// The scratch array's device address on `dev` (the current device) and its
+// SM count, looked up on the first call on that device.
+unsigned char* scratch_for(int dev, int* sms) {
     std::lock_guard<std::mutex> lock(g_setup_mutex);
-    if (dev < 0 || dev >= kMaxDevices) return nullptr;
+    if (dev < 0 || dev >= kMaxDevices) {
+        fprintf(stderr, "sp3mm_rap_direct_noalloc: device %d out of range\n", dev);
+        return nullptr;
+    }
     if (!g_scratch_addr[dev]) {
         void* p = nullptr;
-        const cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+        cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+        int n = 0;
+        if (e == cudaSuccess) e = cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev);
         if (e != cudaSuccess) {
-            fprintf(stderr, "sp3mm_rap_direct_noalloc: cudaGetSymbolAddress failed: %s\n",
+            fprintf(stderr, "sp3mm_rap_direct_noalloc: device set-up failed: %s\n",
                     cudaGetErrorString(e));
             return nullptr;
         }
+        g_sms[dev] = n;
         g_scratch_addr[dev] = static_cast<unsigned char*>(p);
     }
+    *sms = g_sms[dev];
     return g_scratch_addr[dev];
 }
 
 size_t align256(size_t x) { return (x + 255) & ~size_t(255); }
+
+// Bytes of the scratch layout for R with M rows (the offsets carve() uses).
+size_t layout_bytes(int M) {
+    const size_t rows = static_cast<size_t>(M) + 1;
+    return align256(sizeof(Head)) + 5 * align256(4 * rows) + align256(rows) +
+           align256(scan_temp_bytes(M));
+}
+
+// Largest row count of R whose layout fits the scratch array.
+int max_rows_fitting() {
+    int lo = 0, hi = INT_MAX - 1;
+    while (lo < hi) {
+        const int mid = lo + (hi - lo + 1) / 2;
+        if (layout_bytes(mid) <= kScratchBytes) lo = mid;
+        else hi = mid - 1;
+    }
+    return lo;
+}
 
 // Carve the per-row arrays out of the scratch array; returns the bytes used.
 struct Layout {
@@ -221,22 +262,19 @@ extern "C" SP3MM_API int sp3mm_rap_direct_noalloc(const sp3mm_dcsr* R, const sp3
     if (c_capacity > 0 && (!c_col || !c_val))
         return fail(SP3MM_EINVAL, "NULL output arrays");
     const int M = R->M;
-    int dev = 0;
+    int dev = 0, sms = 0;
     NA_CK(cudaGetDevice(&dev));
-    unsigned char* base = scratch_for(dev);
+    unsigned char* base = scratch_for(dev, &sms);
     if (!base) return SP3MM_ECUDA;
-    const Layout L = carve(base, M);
-    if (L.total > kScratchBytes) {
+    if (layout_bytes(M) > kScratchBytes) {
         char msg[200];
-        snprintf(msg, sizeof msg,
-                 "R has %d rows; the %zu MiB scratch array holds the work of about %zu rows",
-                 M, kScratchBytes >> 20, kScratchBytes / 24);
+        snprintf(msg, sizeof msg, "R has %d rows; the %zu MiB scratch array holds at most %d",
+                 M, kScratchBytes >> 20, max_rows_fitting());
         return fail(SP3MM_ELIMIT, msg);
     }
+    const Layout L = carve(base, M);
     cudaStream_t st = static_cast<cudaStream_t>(stream);
-    cudaDeviceProp prop;
-    NA_CK(cudaGetDeviceProperties(&prop, dev));
-    const Geo geo{prop.multiProcessorCount, 110 * 1024};
+    const Geo geo{sms, 110 * 1024};
 
     const CsrView vR{R->M, R->N, R->nnz, R->row_ptr, R->col, R->val, R->val_type};
     const CsrView vA{A->M, A->N, A->nnz, A->row_ptr, A->col, A->val, A->val_type};
@@ -246,11 +284,23 @@ extern "C" SP3MM_API int sp3mm_rap_direct_noalloc(const sp3mm_dcsr* R, const sp3
     const double meanP = P->M ? static_cast<double>(P->nnz) / P->M : 1.0;
     const double mean = std::max(meanA, meanP);
     const int G = mean <= 4 ? 4 : mean <= 8 ? 8 : mean <= 16 ? 16 : 32;
-    const double pmax = P->max_row >= 0 ? P->max_row : P->N;
 
     // Start-of-call state: error word and counters cleared.
     NA_CK(cudaMemsetAsync(L.head, 0, sizeof(Head), st));
-    launch_direct_bounds(vR, vA, static_cast<int>(pmax), L.need, &L.head->total, st);
+    // Longest rows the operands do not record are measured (the bounds and
+    // the retry tables need P's; the kernels' prefetch needs both).
+    int a_max = A->max_row, p_max = P->max_row;
+    if (a_max < 0 || p_max < 0) {
+        if (a_max < 0) launch_count_max(A->M, nullptr, A->row_ptr, &L.head->a_max, st);
+        if (p_max < 0) launch_count_max(P->M, nullptr, P->row_ptr, &L.head->p_max, st);
+        Head h{};
+        NA_CK(cudaMemcpyAsync(&h, L.head, sizeof h, cudaMemcpyDeviceToHost, st));
+        NA_CK(cudaStreamSynchronize(st));
+        if (a_max < 0) a_max = h.a_max;
+        if (p_max < 0) p_max = h.p_max;
+    }
+    const double pmax = p_max;
+    launch_direct_bounds(vR, vA, p_max, L.need, &L.head->total, st);
 
     RowParams p{};
     p.nrows = M;
@@ -259,20 +309,28 @@ extern "C" SP3MM_API int sp3mm_rap_direct_noalloc(const sp3mm_dcsr* R, const sp3
     p.err = &L.head->err;
     p.c_vt = SP3MM_F64;
     NA_CK(cudaMemsetAsync(L.row_cnt1, 0, sizeof(int) * (static_cast<size_t>(M) + 1), st));
-    int rc = run_direct(L, da, p, kSymb, G, 1, 1, A->N, P->N, pmax, A->max_row, P->max_row, geo,
-                        st);
+    int rc = run_direct(L, da, p, kSymb, G, 1, 1, A->N, P->N, pmax, a_max, p_max, geo, st);
     if (rc) return rc;
-    launch_scan(M, L.row_cnt, c_row_ptr, L.scan_tmp, L.scan_bytes, st);
-    int nnz = 0;
-    unsigned err = 0;
-    NA_CK(cudaMemcpyAsync(&nnz, c_row_ptr + M, sizeof(int), cudaMemcpyDeviceToHost, st));
-    NA_CK(cudaMemcpyAsync(&err, &L.head->err, sizeof(unsigned), cudaMemcpyDeviceToHost, st));
+    // The 64-bit total of the row counts decides whether C fits int32
+    // offsets before the 32-bit scan result is trusted.
+    launch_count_max(M, L.row_cnt, nullptr, &L.head->c_max, st, &L.head->c_total);
+    Head h{};
+    NA_CK(cudaMemcpyAsync(&h, L.head, sizeof h, cudaMemcpyDeviceToHost, st));
     NA_CK(cudaStreamSynchronize(st));
-    if (err) return fail(SP3MM_EDEVICE, "device error flag set in the symbolic pass");
+    if (h.err) return device_fail(h.err, "symbolic");
+    const long long nnz = static_cast<long long>(h.c_total);
     *c_nnz = nnz;
+    if (nnz >= INT32_MAX) {
+        fprintf(stderr, "sp3mm_rap_direct_noalloc: C has %lld nonzeros, beyond int32 offsets\n",
+                nnz);
+        return SP3MM_ELIMIT;
+    }
+    launch_scan(M, L.row_cnt, c_row_ptr, L.scan_tmp, L.scan_bytes, st);
     if (nnz > c_capacity) {
+        // c_row_ptr is complete on return, so the caller can size C's arrays.
+        NA_CK(cudaStreamSynchronize(st));
         fprintf(stderr,
-                "sp3mm_rap_direct_noalloc: C has %d nonzeros, the output arrays hold %lld\n",
+                "sp3mm_rap_direct_noalloc: C has %lld nonzeros, the output arrays hold %lld\n",
                 nnz, static_cast<long long>(c_capacity));
         return SP3MM_ENOMEM;
     }
@@ -281,11 +339,11 @@ extern "C" SP3MM_API int sp3mm_rap_direct_noalloc(const sp3mm_dcsr* R, const sp3
     p.c_rp = c_row_ptr;
     p.c_ci = c_col;
     p.c_v = c_val;
-    rc = run_direct(L, da, p, kNumExact, G, 0, 0, A->N, P->N, pmax, A->max_row, P->max_row, geo,
-                    st);
+    rc = run_direct(L, da, p, kNumExact, G, 0, 0, A->N, P->N, pmax, a_max, p_max, geo, st);
     if (rc) return rc;
+    unsigned err = 0;
     NA_CK(cudaMemcpyAsync(&err, &L.head->err, sizeof(unsigned), cudaMemcpyDeviceToHost, st));
     NA_CK(cudaStreamSynchronize(st));
-    if (err) return fail(SP3MM_EDEVICE, "device error flag set in the numeric pass");
+    if (err) return device_fail(err, "numeric");
     return SP3MM_OK;
 }

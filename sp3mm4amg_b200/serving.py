@@ -88,8 +88,9 @@ def _device_view(ptr: int, n: int, typestr: str):
 def level_errors(h32, h64):
     """Per level of two hierarchies of the same request (FP32 coarse storage
     and FP64): (max entrywise relative error over nonzero FP64 entries, max
-    error over max |FP64 value|), computed on the device.  Raises if the
-    patterns differ (they must not, in any mode)."""
+    error over max |FP64 value|, entries whose relative error exceeds 1e-3,
+    entries), computed on the device.  Raises if the patterns differ (they
+    must not, in any mode)."""
     import torch
     out = []
     if len(h32) != len(h64):
@@ -100,7 +101,7 @@ def level_errors(h32, h64):
             raise RuntimeError("hierarchies differ in shape or nonzeros")
         n = a.nnz
         if n == 0:
-            out.append((0.0, 0.0))
+            out.append((0.0, 0.0, 0, 0))
             continue
         rows = a.shape[0] + 1
         for pa, pb, m in ((a.d.row_ptr, b.d.row_ptr, rows), (a.d.col, b.d.col, n)):
@@ -111,7 +112,9 @@ def level_errors(h32, h64):
         diff = (va - vb).abs()
         ref = vb.abs()
         nz = ref > 0
-        rel = float((diff[nz] / ref[nz]).max()) if bool(nz.any()) else 0.0
+        rels = diff[nz] / ref[nz]
+        rel = float(rels.max()) if bool(nz.any()) else 0.0
+        over = int((rels > 1e-3).sum()) + int((diff[~nz] > 0).sum())
         norm = float(diff.max() / ref.max()) if float(ref.max()) > 0 else 0.0
-        out.append((rel, norm))
+        out.append((rel, norm, over, n))
     return out

@@ -11,7 +11,8 @@ if ROOT not in sys.path:
 from sp3mm4amg_b200.problems import CSR  # noqa: E402
 
 GOLDEN = os.path.join(ROOT, "tests", "golden", "golden_cases.npz")
-REF_TEST_DIR = "/root/reference/code/test"
+REF_FIXTURE = os.path.join(ROOT, "tests", "golden", "reference_fixture.npz")
+from oracle import REF_TEST_DIR  # noqa: E402
 
 
 def pytest_configure(config):
@@ -47,10 +48,15 @@ def orc():
     return oracle.Oracle()
 
 
+def reference_fixture_arrays():
+    """The reference's bundled quadruple code/test/{r,ac,p,ac_next} (R, AC,
+    P, AC_next), as the committed fixture holds it (tests/golden/
+    make_golden.py reads the files with the reference's own MatrixMarket
+    loader)."""
+    z = np.load(REF_FIXTURE)
+    return tuple(_unpack(z, n) for n in ("r", "ac", "p", "ac_next"))
+
+
 @pytest.fixture(scope="session")
 def reference_fixture():
-    """The reference's bundled 14^3 quadruple (R, AC, P, AC_next), read in place."""
-    if not os.path.isdir(REF_TEST_DIR):
-        pytest.skip("reference tree not present")
-    import oracle
-    return tuple(oracle.load_mm(os.path.join(REF_TEST_DIR, n)) for n in ("r", "ac", "p", "ac_next"))
+    return reference_fixture_arrays()

@@ -17,6 +17,13 @@ of the reference library built from the unmodified reference sources
 
 It also checks that the 1-based (_1) functions on the shifted inputs return
 the same matrices shifted by one, and records that check.
+
+It also writes ``reference_fixture.npz``: the reference's only bundled golden
+quadruple, ``code/test/{r,ac,p,ac_next}`` (R, AC, P and the externally
+computed next-level operator), read with the reference library's own
+MatrixMarket loader (MMtoCSR), plus that library's pair-wise and direct
+results on it (``ref_pair``, ``ref_direct``).  The GPU box has no reference
+tree, so its tests read the quadruple from this file.
 """
 from __future__ import annotations
 
@@ -50,8 +57,36 @@ def pack(prefix, m, out):
     out[f"{prefix}_shape"] = np.array(m.shape, np.int64)
 
 
+def write_reference_fixture(ref):
+    import ctypes
+    from sp3mm4amg_b200.spmat import csr_from_spmat
+    lib = ctypes.CDLL(O.REF_SO)
+    lib.MMtoCSR.restype = ctypes.c_void_p
+    lib.MMtoCSR.argtypes = [ctypes.c_char_p]
+    lib.freeSpmat.argtypes = [ctypes.c_void_p]
+    out, mats = {}, {}
+    for n in ("r", "ac", "p", "ac_next"):
+        p = lib.MMtoCSR(os.fsencode(os.path.join(O.REF_TEST_DIR, n)))
+        assert p, n
+        m = csr_from_spmat(p, 0)
+        lib.freeSpmat(p)
+        # The device CSR contract: strictly ascending columns in every row.
+        for i in range(m.M):
+            c = m.indices[m.indptr[i]:m.indptr[i + 1]]
+            assert np.all(np.diff(c) > 0), (n, i)
+        mats[n] = m
+        pack(n, m, out)
+    R, AC, P = mats["r"], mats["ac"], mats["p"]
+    pack("ref_pair", ref.sp3mm_pair("spmmRowByRow_SymbNum_", R, AC, P, 0), out)
+    pack("ref_direct", ref.sp3mm_direct(R, AC, P, 0), out)
+    path = os.path.join(os.path.dirname(os.path.abspath(__file__)), "reference_fixture.npz")
+    np.savez_compressed(path, **out)
+    print("wrote", path, os.path.getsize(path), "bytes")
+
+
 def main():
     ref = O.Reference()
+    write_reference_fixture(ref)
     out = {}
     names = []
     for name, prob in cases():

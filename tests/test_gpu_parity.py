@@ -272,12 +272,22 @@ def test_elapsed_internal_set():
     assert 0.0 < t < 10.0
 
 
-def test_reference_fixture_on_gpu_if_present(reference_fixture, orc):
+def test_reference_fixture_on_gpu(reference_fixture):
+    """The reference's bundled quadruple code/test/{r,ac,p,ac_next}: every
+    variant within 1e-12 of the external AC_next, and bit for bit equal to the
+    reference library's own pair-wise / direct result on the same inputs."""
+    from conftest import REF_FIXTURE, _unpack
     R, AC, P, ACN = reference_fixture
-    for name, sp in (("sp3mmRowByRowPair_", None), ("sp3mmRowByRowMerged_", None),
-                     ("sp3mmRowByRowPair_", "spmmRowByRow_SymbNum_")):
-        C = S.sp3mm(R, AC, P, name, spmm=sp)
-        assert O.compare(C, ACN, rtol=RTOL)["ok"]
+    z = np.load(REF_FIXTURE)
+    ref_pair, ref_direct = _unpack(z, "ref_pair"), _unpack(z, "ref_direct")
+    for off in (0, 1):
+        for name, sp, want in (("sp3mmRowByRowPair_", None, ref_pair),
+                               ("sp3mmRowByRowMerged_", None, ref_direct),
+                               ("sp3mmRowByRowPair_", "spmmRowByRow_SymbNum_", ref_pair),
+                               ("sp3mmRowByRowMerged_SymbNum_", None, ref_direct)):
+            C = S.sp3mm(R, AC, P, name, spmm=sp, off_f=off)
+            assert O.compare(C, ACN, rtol=RTOL)["ok"], (name, sp, off)
+            assert_same(C, want, what=f"{name} {sp} off={off}")
 
 
 @pytest.mark.parametrize("off", [0, 1])

@@ -156,8 +156,9 @@ def test_serving_level_errors_on_device():
         _, h32 = serving.serve_batched(ctx, specs, np.zeros(2), S.F32, keep=True, min_coarse=30)
         for a, b in zip(h32, h64):
             errs = serving.level_errors(a, b)
-            assert errs[0] == (0.0, 0.0) and len(errs) >= 2
-            for rel, norm in errs[1:]:
+            assert errs[0][:3] == (0.0, 0.0, 0) and errs[0][3] > 0 and len(errs) >= 2
+            for rel, norm, over, n in errs[1:]:
                 assert 0.0 < norm <= 1e-5 and rel < 1e-2
+                assert 0 <= over <= n and n > 0
             a.free()
             b.free()

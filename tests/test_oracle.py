@@ -24,6 +24,31 @@ def test_oracle_matches_reference_fixture(orc, reference_fixture, off):
     assert O.compare(D, ACN, rtol=1e-12)["ok"]
 
 
+def test_oracle_matches_reference_fixture_results(orc, reference_fixture):
+    """Bit for bit against the reference library's own results on its fixture
+    (stored beside the quadruple by tests/golden/make_golden.py)."""
+    from conftest import REF_FIXTURE, _unpack
+    z = np.load(REF_FIXTURE)
+    R, AC, P, _ = reference_fixture
+    for got, key in ((orc.sp3mm_pair(R, AC, P), "ref_pair"),
+                     (orc.sp3mm_direct(R, AC, P), "ref_direct")):
+        want = _unpack(z, key)
+        cmp = O.compare(got, want, rtol=0.0)
+        assert cmp["ok"] and cmp["bitwise_equal"] == want.nnz, (key, cmp)
+
+
+def test_reference_fixture_file_matches_the_tree(reference_fixture):
+    """Where the reference tree is present, the committed quadruple equals its
+    files (read here with scipy, an independent MatrixMarket reader)."""
+    from conftest import REF_TEST_DIR
+    if not os.path.isdir(REF_TEST_DIR):
+        pytest.skip("reference tree not present")
+    for got, n in zip(reference_fixture, ("r", "ac", "p", "ac_next")):
+        want = O.load_mm(os.path.join(REF_TEST_DIR, n))
+        cmp = O.compare(got, want, rtol=0.0)
+        assert cmp["ok"] and cmp["bitwise_equal"] == want.nnz, (n, cmp)
+
+
 def test_oracle_matches_golden(orc, golden):
     for name, g in golden.items():
         for off in (0, 1):
