@@ -436,7 +436,9 @@ SP3MM_API int sp3mm_hierarchy_build_batch(sp3mm_ctx *ctx, int n, const sp3mm_dcs
 
 /* ---- Request server: continuous batching of hierarchy setups ------------
  * Each request is a host CSR operator A0 (0-based int64 row_ptr/col, FP64
- * values; borrowed until the request is done or has failed) on a box grid.
+ * values; borrowed until the request is done or has failed) on a box grid
+ * (sp3mm_server_submit: smoothed block aggregation), or A0 with the
+ * caller's prolongators (sp3mm_server_submit_ops).
  * Every sp3mm_server_step admits queued requests first come first served
  * while fewer than max_active are in flight and the request's device-memory
  * estimate fits both the budget (mem_fraction of the HBM free at creation,
@@ -459,6 +461,23 @@ SP3MM_API int sp3mm_server_submit(sp3mm_server *s, int64_t M, int64_t nnz,
                                   const int32_t *dims, int ndim, int block, double omega,
                                   int64_t min_coarse, int max_levels, int coarse_val_type,
                                   double arrival, int64_t *id);
+/* Submit a request whose prolongators the caller provides (the setup
+ * requests of an AMG caller such as AMG4PSBLAS, which aggregates by its own
+ * rules): host CSRs A0 (M x M) and P_0 .. P_{np-1}, P_l of p_rows[l] x
+ * p_cols[l] with p_rows[0] = M and p_rows[l] = p_cols[l-1] (0-based int64
+ * indices, FP64 values, ascending columns; borrowed until the request is
+ * done or has failed).  The server forms R_l = P_l^T and A_{l+1} =
+ * R_l A_l P_l (direct product) on the device, level by level, batched with
+ * the other requests in flight; coarse levels (l >= 1, their P included)
+ * are stored as coarse_val_type.  The hierarchy's levels and results are
+ * read as for the other requests; its grid sizes are the row counts. */
+SP3MM_API int sp3mm_server_submit_ops(sp3mm_server *s, int64_t M, int64_t nnz,
+                                      const int64_t *row_ptr, const int64_t *col,
+                                      const double *val, int np, const int64_t *p_rows,
+                                      const int64_t *p_cols, const int64_t *p_nnz,
+                                      const int64_t *const *p_row_ptr,
+                                      const int64_t *const *p_col, const double *const *p_val,
+                                      int coarse_val_type, double arrival, int64_t *id);
 SP3MM_API int sp3mm_server_step(sp3mm_server *s, int *pending);
 SP3MM_API int sp3mm_server_poll(const sp3mm_server *s, int64_t id, int *status,
                                 double *latency, double *queued);

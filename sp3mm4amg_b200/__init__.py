@@ -512,6 +512,29 @@ class Server:
         self._inputs[rid.value] = (rp, ci, v)
         return rid.value
 
+    def submit_ops(self, A0: CSR, Ps, coarse_val_type: int = F64, arrival: float = -1.0) -> int:
+        """A request with the caller's prolongators P_0, P_1, ... (host CSR);
+        the server builds R_l = P_l^T and A_{l+1} = R_l A_l P_l."""
+        rp = np.ascontiguousarray(A0.indptr, np.int64)
+        ci = np.ascontiguousarray(A0.indices, np.int64)
+        v = np.ascontiguousarray(A0.data, np.float64)
+        prp = [np.ascontiguousarray(P.indptr, np.int64) for P in Ps]
+        pci = [np.ascontiguousarray(P.indices, np.int64) for P in Ps]
+        pv = [np.ascontiguousarray(P.data, np.float64) for P in Ps]
+        n = len(Ps)
+        rows = (ctypes.c_int64 * n)(*[P.M for P in Ps])
+        cols = (ctypes.c_int64 * n)(*[P.N for P in Ps])
+        nnz = (ctypes.c_int64 * n)(*[P.nnz for P in Ps])
+        a_rp = (ctypes.c_void_p * n)(*[a.ctypes.data for a in prp])
+        a_ci = (ctypes.c_void_p * n)(*[a.ctypes.data for a in pci])
+        a_v = (ctypes.c_void_p * n)(*[a.ctypes.data for a in pv])
+        rid = ctypes.c_int64()
+        self.ctx._check(self.ctx.lib.sp3mm_server_submit_ops(
+            self.h, A0.M, A0.nnz, rp.ctypes.data, ci.ctypes.data, v.ctypes.data, n, rows, cols,
+            nnz, a_rp, a_ci, a_v, coarse_val_type, float(arrival), ctypes.byref(rid)))
+        self._inputs[rid.value] = (rp, ci, v, prp, pci, pv, rows, cols, nnz, a_rp, a_ci, a_v)
+        return rid.value
+
     def step(self) -> int:
         pending = ctypes.c_int()
         self.ctx._check(self.ctx.lib.sp3mm_server_step(self.h, ctypes.byref(pending)))

@@ -92,6 +92,11 @@ DEVICE_API = {
                                        _c.c_void_p, _c.c_void_p, _c.c_void_p, _c.c_int,
                                        _c.c_int, _c.c_double, _c.c_int64, _c.c_int, _c.c_int,
                                        _c.c_double, _c.POINTER(_c.c_int64)]),
+    "sp3mm_server_submit_ops": (_c.c_int, [_c.c_void_p, _c.c_int64, _c.c_int64, _c.c_void_p,
+                                           _c.c_void_p, _c.c_void_p, _c.c_int, _c.c_void_p,
+                                           _c.c_void_p, _c.c_void_p, _c.c_void_p, _c.c_void_p,
+                                           _c.c_void_p, _c.c_int, _c.c_double,
+                                           _c.POINTER(_c.c_int64)]),
     "sp3mm_server_step": (_c.c_int, [_c.c_void_p, _c.POINTER(_c.c_int)]),
     "sp3mm_server_poll": (_c.c_int, [_c.c_void_p, _c.c_int64, _c.POINTER(_c.c_int),
                                      _c.POINTER(_c.c_double), _c.POINTER(_c.c_double)]),

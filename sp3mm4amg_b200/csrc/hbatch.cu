@@ -387,20 +387,70 @@ int step_group(sp3mm_ctx* ctx, const std::vector<sp3mm_hierarchy*>& hs) {
     return SP3MM_OK;
 }
 
+// One step for hierarchies whose prolongators the caller provides (same
+// value types within the group): R = P^T by a device transpose per
+// hierarchy, then one batch of direct R*A*P products for all of them.
+int step_given(sp3mm_ctx* ctx, const std::vector<sp3mm_hierarchy*>& hs) {
+    const int k = static_cast<int>(hs.size());
+    const int cvt = hs[0]->coarse_val_type;
+    ProfSpan whole(ctx, "hstep.given");
+    std::vector<sp3mm_dcsr> X(k), Aop(k), P(k);
+    std::vector<std::shared_ptr<void>> rkeep(k);
+    for (int t = 0; t < k; ++t) {
+        sp3mm_hierarchy* h = hs[t];
+        const sp3mm_dcsr& A = h->A.back();
+        P[t] = h->given_P[h->A.size() - 1];
+        if (P[t].M != A.M || A.M != A.N || P[t].val_type != A.val_type)
+            return set_error(ctx, SP3MM_EINVAL,
+                             "hierarchy step: prolongator %zu does not match its operator",
+                             h->A.size() - 1);
+        auto R = std::shared_ptr<sp3mm_dcsr>(new sp3mm_dcsr{}, [ctx](sp3mm_dcsr* m) {
+            sp3mm_dcsr_free(ctx, m);
+            delete m;
+        });
+        TRY(sp3mm_transpose(ctx, &P[t], R.get()));
+        X[t] = *R;
+        Aop[t] = A;
+        rkeep[t] = R;
+    }
+    std::vector<int> rk(k, SP3MM_BATCH_RAP);
+    sp3mm_batch* raw = nullptr;
+    TRY(sp3mm_batch_create(ctx, k, rk.data(), X.data(), Aop.data(), P.data(), cvt, &raw));
+    auto b = hold(raw);
+    TRY(sp3mm_batch_run(b.get()));
+    batch_trim(b.get());
+    for (int t = 0; t < k; ++t) {
+        sp3mm_hierarchy* h = hs[t];
+        sp3mm_dcsr Ac{};
+        TRY(sp3mm_batch_result(b.get(), t, &Ac));
+        h->P.push_back(P[t]);
+        h->R.push_back(X[t]);
+        h->A.push_back(Ac);
+        h->nx.push_back(Ac.M);
+        h->ny.push_back(1);
+        h->nz.push_back(1);
+        h->nlev = static_cast<int>(h->A.size());
+        h->keep.push_back(rkeep[t]);
+        h->keep.push_back(b);
+    }
+    return SP3MM_OK;
+}
+
 }  // namespace
 
 namespace sp3mm {
 
 int hierarchy_step(sp3mm_ctx* ctx, const std::vector<sp3mm_hierarchy*>& all) {
-    // Group by (operator value type, coarse storage type).
-    std::vector<sp3mm_hierarchy*> groups[4];
+    // Group by (operator value type, coarse storage type), block-aggregation
+    // hierarchies apart from those with given prolongators.
+    std::vector<sp3mm_hierarchy*> groups[8];
     for (sp3mm_hierarchy* h : all)
         if (h->wants_level())
-            groups[(h->A.back().val_type == SP3MM_F32 ? 2 : 0) +
+            groups[(h->given_P.empty() ? 0 : 4) + (h->A.back().val_type == SP3MM_F32 ? 2 : 0) +
                    (h->coarse_val_type == SP3MM_F32 ? 1 : 0)]
                 .push_back(h);
-    for (auto& g : groups)
-        if (!g.empty()) TRY(step_group(ctx, g));
+    for (int g = 0; g < 8; ++g)
+        if (!groups[g].empty()) TRY(g < 4 ? step_group(ctx, groups[g]) : step_given(ctx, groups[g]));
     return SP3MM_OK;
 }
 

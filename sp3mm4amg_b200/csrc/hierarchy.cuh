@@ -21,9 +21,14 @@ struct sp3mm_hierarchy {
     // (kept alive here) instead of owning their arrays.
     bool owns_arrays = true;
     std::vector<std::shared_ptr<void>> keep;
+    // Prolongators the caller provides, one per level to build (device
+    // copies kept alive through `keep`); empty: block aggregation on the
+    // box grid.
+    std::vector<sp3mm_dcsr> given_P;
 
     // Whether another level should be built.
     bool wants_level() const {
+        if (!given_P.empty()) return A.size() <= given_P.size();
         const sp3mm_dcsr& a = A.back();
         return static_cast<int>(A.size()) < max_levels && a.M >= min_coarse && a.M > 1;
     }

@@ -1,8 +1,10 @@
 // server.cu -- a setup-request server with continuous batching.
 //
-// A request is an operator A0 on a box grid (host CSR) whose smoothed-
-// aggregation hierarchy is to be built on the device (the product chain of
-// code/scripts/getLevels3MMmatrixes.py:29-38).  Every engine step
+// A request is an operator A0 (host CSR) whose hierarchy is to be built on
+// the device (the product chain of code/scripts/getLevels3MMmatrixes.py:
+// 29-38): on a box grid by smoothed block aggregation, or with prolongators
+// P_0, P_1, ... that the caller provides (R_l = P_l^T is formed on the
+// device).  Every engine step
 //
 //   1. admits queued requests, first come first served, while a slot is
 //      free and the request's device-memory estimate fits both the server's
@@ -26,6 +28,8 @@
 
 #include <algorithm>
 #include <chrono>
+#include <climits>
+#include <cstdint>
 #include <condition_variable>
 #include <deque>
 #include <memory>
@@ -48,12 +52,22 @@ double now_s(std::chrono::steady_clock::time_point t0) {
 
 enum { kQueued = 0, kActive = 1, kDone = 2, kFailed = 3, kTaken = 4 };
 
+// A borrowed host CSR (0-based int64 indices, FP64 values).
+struct HostCsr {
+    int64_t M = 0, N = 0, nnz = 0;
+    const int64_t* rp = nullptr;
+    const int64_t* ci = nullptr;
+    const double* v = nullptr;
+};
+
 struct Request {
     int64_t id = 0;
     int64_t M = 0, nnz = 0;
     const int64_t* rp = nullptr;
     const int64_t* ci = nullptr;
     const double* v = nullptr;
+    // Caller-provided prolongators (empty: block aggregation on dims).
+    std::vector<HostCsr> P;
     int32_t dims[3] = {1, 1, 1};
     int ndim = 1, block = 2, max_levels = 1, cvt = SP3MM_F64;
     long long min_coarse = 0;
@@ -77,6 +91,15 @@ size_t request_estimate(int64_t M, int64_t nnz) {
     const size_t level0 = a /* A0 */ + 5 * a /* P, R, A*P0, A1, booking */ +
                           static_cast<size_t>(M) * 48 /* work arrays */;
     return 2 * level0;
+}
+
+// A request with given prolongators also holds them and their transposes.
+size_t request_estimate_ops(int64_t M, int64_t nnz, const std::vector<HostCsr>& P) {
+    size_t e = request_estimate(M, nnz);
+    for (const HostCsr& p : P)
+        e += 2 * (static_cast<size_t>(p.M + 1) * 4 + static_cast<size_t>(p.N + 1) * 4 +
+                  static_cast<size_t>(p.nnz) * 12);
+    return e;
 }
 
 size_t free_hbm(sp3mm_ctx* ctx) { return free_device_bytes(ctx); }
@@ -152,6 +175,19 @@ int admit(sp3mm_server* s, sp3mm_ctx* lctx, Request& r) {
     h->nlev = 1;
     h->keep.push_back(A0);
     r.h = h;
+    // Given prolongators: level 0 in FP64, coarser ones in the coarse
+    // storage type (each product's operands share one value type).
+    for (size_t l = 0; l < r.P.size(); ++l) {
+        const HostCsr& hp = r.P[l];
+        auto P = std::shared_ptr<sp3mm_dcsr>(new sp3mm_dcsr{}, [ctx](sp3mm_dcsr* m) {
+            sp3mm_dcsr_free(ctx, m);
+            delete m;
+        });
+        TRY(sp3mm_dcsr_upload_arrays(lctx, hp.M, hp.N, hp.nnz, hp.rp, hp.ci, hp.v,
+                                     l == 0 ? SP3MM_F64 : r.cvt, P.get()));
+        h->given_P.push_back(*P);
+        h->keep.push_back(P);
+    }
     return SP3MM_OK;
 }
 
@@ -252,6 +288,52 @@ int sp3mm_server_submit(sp3mm_server* s, int64_t M, int64_t nnz, const int64_t* 
     return SP3MM_OK;
 }
 
+int sp3mm_server_submit_ops(sp3mm_server* s, int64_t M, int64_t nnz, const int64_t* row_ptr,
+                            const int64_t* col, const double* val, int np,
+                            const int64_t* p_rows, const int64_t* p_cols, const int64_t* p_nnz,
+                            const int64_t* const* p_row_ptr, const int64_t* const* p_col,
+                            const double* const* p_val, int coarse_val_type, double arrival,
+                            int64_t* id) {
+    if (!s || !row_ptr || (nnz > 0 && (!col || !val)) || !id || M < 1 || np < 1 ||
+        !p_rows || !p_cols || !p_nnz || !p_row_ptr || !p_col || !p_val ||
+        (coarse_val_type != SP3MM_F64 && coarse_val_type != SP3MM_F32))
+        return set_error(s ? s->ctx : nullptr, SP3MM_EINVAL, "server: invalid request");
+    Request r;
+    int64_t rows = M;
+    for (int l = 0; l < np; ++l) {
+        if (p_rows[l] != rows || p_cols[l] < 1 || p_nnz[l] < 0 || !p_row_ptr[l] ||
+            (p_nnz[l] > 0 && (!p_col[l] || !p_val[l])))
+            return set_error(s->ctx, SP3MM_EINVAL,
+                             "server: prolongator %d does not follow its level's size", l);
+        HostCsr hp;
+        hp.M = p_rows[l];
+        hp.N = p_cols[l];
+        hp.nnz = p_nnz[l];
+        hp.rp = p_row_ptr[l];
+        hp.ci = p_col[l];
+        hp.v = p_val[l];
+        r.P.push_back(hp);
+        rows = p_cols[l];
+    }
+    r.id = s->next_id++;
+    r.M = M;
+    r.nnz = nnz;
+    r.rp = row_ptr;
+    r.ci = col;
+    r.v = val;
+    r.dims[0] = static_cast<int32_t>(std::min<int64_t>(M, INT32_MAX));
+    r.ndim = 1;
+    r.max_levels = np + 1;
+    r.cvt = coarse_val_type;
+    r.t_arrival = arrival >= 0 ? arrival : now_s(s->t0);
+    r.est = request_estimate_ops(M, nnz, r.P);
+    const int64_t rid = r.id;
+    s->reqs[rid] = std::move(r);
+    s->queue.push_back(rid);
+    *id = rid;
+    return SP3MM_OK;
+}
+
 int sp3mm_server_step(sp3mm_server* s, int* pending) {
     if (!s) return SP3MM_EINVAL;
     sp3mm_ctx* ctx = s->ctx;
@@ -305,6 +387,7 @@ int sp3mm_server_step(sp3mm_server* s, int* pending) {
             r->rp = nullptr;
             r->ci = nullptr;
             r->v = nullptr;
+            r->P.clear();
             if (r->error != SP3MM_OK) {
                 if (r->h) sp3mm_hierarchy_free(ctx, r->h);
                 r->h = nullptr;

@@ -162,3 +162,77 @@ def test_serving_level_errors_on_device():
                 assert 0 <= over <= n and n > 0
             a.free()
             b.free()
+
+
+def _explicit_chain(npoints, seed, orc):
+    """A kNN operator with its caller-side prolongators for two levels (greedy
+    aggregation + one Jacobi step on each level, as an AMG caller with its
+    own aggregation rules would pass them) and the oracle's level chain."""
+    prob = pb.knn_problem(npoints, seed=seed)
+    A0, P0 = prob.A, prob.P
+    A1 = orc.sp3mm_direct(P0.transpose(), A0, P0)
+    P1 = pb.jacobi_smooth(A1, pb.aggregates_from_labels(pb.greedy_aggregation(A1, seed)))
+    A2 = orc.sp3mm_direct(P1.transpose(), A1, P1)
+    return A0, [P0, P1], [A0, A1, A2]
+
+
+def test_server_given_prolongators_alone_and_in_mix(orc):
+    """Requests that carry their own prolongators (irregular, greedy
+    aggregation): every level equals the oracle chain bit for bit, served
+    alone and mixed with block-aggregation requests."""
+    chains = [_explicit_chain(3000, 5, orc), _explicit_chain(7000, 6, orc)]
+    with S.Context() as ctx:
+        for mix in (False, True):
+            srv = S.Server(ctx)
+            ids = []
+            for A0, Ps, _ in chains:
+                ids.append(srv.submit_ops(A0, Ps))
+                if mix:
+                    srv.submit(pb.stencil_operator((20, 20, 20)), (20, 20, 20), min_coarse=30)
+            while srv.step():
+                pass
+            for rid, (_, Ps, want) in zip(ids, chains):
+                assert srv.poll(rid)[0] == S.Server.DONE
+                h = srv.take(rid)
+                assert len(h) == len(Ps) + 1
+                for l, (A, P, R) in enumerate(_levels(h)):
+                    _same(A, want[l])
+                    if l < len(Ps):
+                        _same(P, Ps[l])
+                        _same(R, Ps[l].transpose())
+                h.free()
+            srv.free()
+
+
+def test_server_given_prolongators_fp32_coarse(orc):
+    """FP32 coarse storage with given prolongators: level 0 and the pattern of
+    every level exact, coarse values at FP32 rounding scale."""
+    A0, Ps, want = _explicit_chain(3000, 7, orc)
+    with S.Context() as ctx:
+        srv = S.Server(ctx)
+        rid = srv.submit_ops(A0, Ps, coarse_val_type=S.F32)
+        while srv.step():
+            pass
+        assert srv.poll(rid)[0] == S.Server.DONE
+        h = srv.take(rid)
+        got = _levels(h)
+        _same(got[0][0], want[0])
+        for l in (1, 2):
+            A = got[l][0]
+            assert np.array_equal(A.indptr, want[l].indptr)
+            assert np.array_equal(A.indices, want[l].indices)
+            scale = np.abs(want[l].data).max()
+            assert np.abs(A.data - want[l].data).max() <= 1e-5 * scale
+        h.free()
+        srv.free()
+
+
+def test_server_given_prolongators_rejects_mismatched_sizes():
+    A0 = pb.stencil_operator((6, 6))
+    P = pb.aggregates_from_labels(np.arange(36) // 4)
+    bad = pb.aggregates_from_labels(np.arange(5) % 2)   # 5 rows after 9 coarse columns
+    with S.Context() as ctx:
+        srv = S.Server(ctx)
+        with pytest.raises(S.Sp3mmError):
+            srv.submit_ops(A0, [P, bad])
+        srv.free()
