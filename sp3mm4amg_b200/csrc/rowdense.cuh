@@ -12,10 +12,10 @@
 // then the right row's entries).  Every column therefore still receives its
 // contributions in the reference's order (code/src/include/
 // SpMMUtilsGeneric.h:39-55), and the accumulator of a column range is a
-// dense slice of shared memory indexed by column -- no hashing.  Equal
-// columns within a batch of 32 staged products are resolved as in the warp
-// kernels (__match_any_sync, the group's lowest lane adds the group's
-// products in lane order).
+// dense slice of shared memory indexed by column -- no hashing.  Within a
+// batch of 32 staged products, the products of one right row's segment have
+// distinct columns and are added at once, segment after segment (batches
+// spread over many short segments group equal columns with a match).
 //
 // Stage 1 (the R*A row) walks the row's column span in chunks of kDSpan
 // columns.  Each column's first touch is recorded as the flat position of
@@ -46,11 +46,12 @@ constexpr int kDSamples = 2048;   // columns sampled per stage for that histogra
 // Dynamic shared memory: acc double[kDSpan] | ftq int[kDSpan] (after stage 1:
 // u64 sort keys [kDList]) | lkey int[kDList] | lq int[kDList] |
 // lval double[kDList] | touched u8[kDSpan] | per warp: sk int[kStage],
-// sq int[kStage], sv double[kStage] | hist int[kDHist] | total int.
+// sq int[kStage], sv double[kStage], sst int[kStage] | hist int[kDHist] |
+// total int.
 __host__ __device__ constexpr size_t dense_smem_bytes() {
     return static_cast<size_t>(kDSpan) * 8 + static_cast<size_t>(kDSpan) * 4 +
            static_cast<size_t>(kDList) * 16 + static_cast<size_t>(kDSpan) +
-           static_cast<size_t>(kDWarps) * kStage * 16 + static_cast<size_t>(kDHist) * 4 + 16;
+           static_cast<size_t>(kDWarps) * kStage * 20 + static_cast<size_t>(kDHist) * 4 + 16;
 }
 
 // First index in [b, e) whose column is >= x (columns ascending).
@@ -77,14 +78,45 @@ struct LeftSorted {
     }
 };
 
+// Batches whose products come from at most this many right-row segments
+// are added in rounds by segment; others group equal columns with a match.
+constexpr int kDSegRounds = 3;
+
 // One batch of staged products into the dense slice (slot = column - base).
-// FT: record a new column's first-touch position.
+// FT: record a new column's first-touch position.  sst[i] is the left
+// position (step) a staged product comes from; steps never decrease along
+// the staging, and one step's columns are distinct (a right row's columns
+// are), so the products of one segment of equal steps are added all at
+// once, segment after segment: every column receives its products in the
+// reference's order without grouping equal columns.  Batches spread over
+// many short segments group equal columns with __match_any_sync instead
+// (the lowest lane of a group adds the group's products in lane order).
 template <bool NUM, bool FT>
 __device__ __forceinline__ void dbatch(double* acc, unsigned char* touched, int* ftq, int base,
-                                       const int* sk, const double* sv, const int* sq, int i,
-                                       bool valid) {
+                                       const int* sk, const double* sv, const int* sq,
+                                       const int* sst, int i, bool valid) {
     const int lane = threadIdx.x & 31;
     const unsigned lt = lanemask_lt();
+    const int st = valid ? sst[i] : -1;
+    const int prev = __shfl_up_sync(kFull, st, 1);
+    const unsigned starts = __ballot_sync(kFull, valid && (lane == 0 || prev != st));
+    const int nseg = __popc(starts);
+    if (nseg <= kDSegRounds) {
+        const int seg = __popc(starts & (lt | (1u << lane))) - 1;
+        const int slot = valid ? sk[i] - base : 0;
+        const double v = (NUM && valid) ? sv[i] : 0.0;
+        for (int r = 0; r < nseg; ++r) {
+            if (valid && seg == r) {
+                if (!touched[slot]) {
+                    touched[slot] = 1;
+                    if (FT) ftq[slot] = sq[i];
+                }
+                if (NUM) acc[slot] = __dadd_rn(acc[slot], v);
+            }
+            __syncwarp();
+        }
+        return;
+    }
     const int key = valid ? sk[i] : -2 - lane;
     const unsigned peers = __match_any_sync(kFull, key);
     if (valid && (peers & lt) == 0) {
@@ -116,7 +148,7 @@ __device__ __forceinline__ void daccumulate(const Left& L, int n, const int* __r
                                             const int* __restrict__ b_ci,
                                             const TB* __restrict__ b_v, int wlo, int whi,
                                             int base, double* acc, unsigned char* touched,
-                                            int* ftq, int* sk, int* sq, double* sv) {
+                                            int* ftq, int* sk, int* sq, double* sv, int* sst) {
     if (wlo >= whi) return;
     const int lane = threadIdx.x & 31;
     int qbase = 0;
@@ -178,6 +210,7 @@ __device__ __forceinline__ void daccumulate(const Left& L, int n, const int* __r
                         sk[i] = __ldg(b_ci + e);
                         if (NUM) sv[i] = __dmul_rn(ldv(b_v, e), sj);
                         if (FT) sq[i] = qj + e;
+                        sst[i] = j;
                     }
                 }
             } else {
@@ -190,11 +223,13 @@ __device__ __forceinline__ void daccumulate(const Left& L, int n, const int* __r
                     sk[pos] = __ldg(b_ci + ea);
                     if (NUM) sv[pos] = __dmul_rn(ldv(b_v, ea), s);
                     if (FT) sq[pos] = fo + (ea - ab);
+                    sst[pos] = lane;
                 }
             }
             __syncwarp();
             for (int i0 = 0; i0 < wl; i0 += 32)
-                dbatch<NUM, FT>(acc, touched, ftq, base, sk, sv, sq, i0 + lane, i0 + lane < wl);
+                dbatch<NUM, FT>(acc, touched, ftq, base, sk, sv, sq, sst, i0 + lane,
+                                i0 + lane < wl);
             __syncwarp();
         }
     }
@@ -233,6 +268,7 @@ struct DenseSmem {
     int* sk;
     int* sq;
     double* sv;
+    int* sst;
     int* hist;
     long long* s_tot;
     int* s_n1;
@@ -252,11 +288,12 @@ __device__ __forceinline__ DenseSmem dense_smem(unsigned char* smem, int* s_n1, 
     d.lq = d.lkey + kDList;
     d.lval = reinterpret_cast<double*>(d.lq + kDList);
     d.touched = reinterpret_cast<unsigned char*>(d.lval + kDList);
-    unsigned char* wst = d.touched + kDSpan + static_cast<size_t>(threadIdx.x >> 5) * kStage * 16;
+    unsigned char* wst = d.touched + kDSpan + static_cast<size_t>(threadIdx.x >> 5) * kStage * 20;
     d.sk = reinterpret_cast<int*>(wst);
     d.sq = d.sk + kStage;
     d.sv = reinterpret_cast<double*>(d.sq + kStage);
-    d.hist = reinterpret_cast<int*>(d.touched + kDSpan + static_cast<size_t>(kDWarps) * kStage * 16);
+    d.sst = reinterpret_cast<int*>(d.sv + kStage);
+    d.hist = reinterpret_cast<int*>(d.touched + kDSpan + static_cast<size_t>(kDWarps) * kStage * 20);
     d.s_tot = reinterpret_cast<long long*>(d.hist + kDHist);
     d.s_n1 = s_n1;
     d.s_lo = s_lo;
@@ -386,7 +423,7 @@ __device__ __forceinline__ void dense_row(const DenseSmem& d, const CsrView& R, 
         int wlo, whi;
         balanced_range(d, L1, rlen, A.rp, A.ci, cb, ce, tot1, wlo, whi);
         daccumulate<NUM, true>(L1, rlen, A.rp, A.ci, av, wlo, whi, cb, d.acc, d.touched, d.ftq,
-                               d.sk, d.sq, d.sv);
+                               d.sk, d.sq, d.sv, d.sst);
         __syncthreads();
         // List this warp's touched columns (value and first touch) and
         // clear them.
@@ -480,7 +517,7 @@ __device__ __forceinline__ void dense_row(const DenseSmem& d, const CsrView& R, 
         if (run2) {
             balanced_range(d, L2, n1, P.rp, P.ci, cb, ce, tot2, wlo2, whi2);
             daccumulate<NUM, false>(L2, n1, P.rp, P.ci, pv, wlo2, whi2, cb, d.acc, d.touched,
-                                    nullptr, d.sk, d.sq, d.sv);
+                                    nullptr, d.sk, d.sq, d.sv, d.sst);
         }
         __syncthreads();
         int cnt = 0;
