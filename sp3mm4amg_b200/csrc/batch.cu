@@ -506,11 +506,13 @@ int ensure_numeric(sp3mm_batch* b) {
         launch_need_from_counts(M, b->d_cnt2.as<int>(), b->d_cnt1.as<int>(), b->d_need.as<int>(),
                                 ctx->stream);
     TRY(bin_rows(ctx, M, b->d_need.as<int>(), 0, 32, dc, nullptr, b->nbins));
+    ProfSpan span(ctx, "batch.graph");
     return build_numeric(b);
 }
 
 int batch_plan(sp3mm_batch* b) {
     sp3mm_ctx* ctx = b->ctx;
+    ProfSpan whole(ctx, "batch.plan");
     const cudaStream_t st = ctx->stream;
     const int n = static_cast<int>(b->items.size());
     const long long rows = b->rows;

@@ -204,13 +204,15 @@ struct RowRunner {
     // (known longest rows) and the tables fit shared memory; never the retry
     // launch, which the warp kernels run with proven tables.
     // Whether a direct launch runs the register-product kernel (rowlanes.cuh):
-    // by default (no lane tuning) when every A and P row holds at most 32
-    // entries (known longest rows) and the tables fit shared memory; never
-    // the retry launch, which the warp kernels run with proven tables.
+    // by default (no lane tuning) when every A row holds at most 16 entries
+    // and every P row at most 32 (known longest rows) and the tables fit
+    // shared memory; never the retry launch, which the warp kernels run with
+    // proven tables.  A rows of 17-32 entries (one step per batch) ran 6 %
+    // slower than the warp kernel on the kNN product, so they stay there.
     static constexpr size_t kLanesMaxWarpBytes = 16 * 1024;
     bool use_lanes(const RowParams& p, int G) const {
         if (ctx->tune_G != 0 || G != 32 || !p.retry_rows) return false;
-        if (a_max < 0 || a_max > 32 || b_max < 0 || b_max > 32) return false;
+        if (a_max < 0 || a_max > 16 || b_max < 0 || b_max > 32) return false;
         return p.S2 <= p.S1;
     }
 
