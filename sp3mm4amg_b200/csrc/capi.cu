@@ -199,21 +199,28 @@ struct RowRunner {
     // Longest row of the right operands (first / last; -1: unknown).
     int a_max = -1, b_max = -1;
 
-    // Whether a direct launch runs the register-product kernel: by default
-    // (no lane tuning) when every A and P row holds at most 32 entries
-    // (known longest rows) and the tables fit shared memory; never the retry
-    // launch, which the warp kernels run with proven tables.
     // Whether a direct launch runs the register-product kernel (rowlanes.cuh):
-    // by default (no lane tuning) when every A row holds at most 16 entries
-    // and every P row at most 32 (known longest rows) and the tables fit
-    // shared memory; never the retry launch, which the warp kernels run with
-    // proven tables.  A rows of 17-32 entries (one step per batch) ran 6 %
-    // slower than the warp kernel on the kNN product, so they stay there.
+    // by default (no lane tuning) when the operands' longest rows are known
+    // and the tables fit shared memory; never the retry launch, which the
+    // warp kernels run with proven tables.
     static constexpr size_t kLanesMaxWarpBytes = 16 * 1024;
     bool use_lanes(const RowParams& p, int G) const {
         if (ctx->tune_G != 0 || G != 32 || !p.retry_rows) return false;
-        if (a_max < 0 || a_max > 16 || b_max < 0 || b_max > 32) return false;
+        if (a_max < 0 || b_max < 0) return false;
         return p.S2 <= p.S1;
+    }
+
+    // Batch layout of a lanes stage whose right operand has rows of at most
+    // `mx` entries, `avg` on average: 2^lg lanes per step when the rows
+    // fill at least 3/4 of them (stencil rows: 1.53 ms at 128^3 against
+    // 1.57 packed), else packed (the kNN product's A rows of 16-31 entries:
+    // 8.4 ms against 11.3 on the staged kernel).
+    static int lanes_layout(int mx, const CsrView& B) {
+        if (mx <= 0) return 0;
+        if (mx > 32) return -1;
+        const int lg = ilog2_pow2(next_pow2(static_cast<unsigned>(mx)));
+        const double avg = B.M > 0 ? static_cast<double>(B.nnz) / B.M : 0.0;
+        return avg >= 0.75 * (1 << lg) ? lg : -1;
     }
 
     long long operand_nnz() const {
@@ -252,8 +259,8 @@ struct RowRunner {
                 const long long cap = static_cast<long long>(ctx->num_sms) * 16;
                 geo.grid = static_cast<int>(grid < cap ? grid : cap);
                 p.gtab = nullptr;
-                p.lg1 = ilog2_pow2(next_pow2(static_cast<unsigned>(a_max > 0 ? a_max : 1)));
-                p.lg2 = ilog2_pow2(next_pow2(static_cast<unsigned>(b_max > 0 ? b_max : 1)));
+                p.lg1 = lanes_layout(a_max, da.A);
+                p.lg2 = lanes_layout(b_max, da.P);
                 static const char* const kLanes[3] = {"direct.lanes.symb", "direct.lanes.num",
                                                       "direct.lanes.book"};
                 cudaError_t e = cudaSuccess;

@@ -54,8 +54,10 @@ struct RowParams {
     // Some row of the first (a_long, direct only) / last (b_long) right
     // operand is longer than the entries the kernel prefetches per step.
     bool a_long, b_long;
-    // Lanes per left-row step (log2) of the register-product direct kernel
-    // (rowlanes.cuh): stage 1 (R*A, A rows) and stage 2 (RA*P, P rows).
+    // Layout of the register-product direct kernel's batches (rowlanes.cuh)
+    // in stage 1 (R*A, A rows) and stage 2 (RA*P, P rows): lanes per
+    // left-row step (log2, at most 5, every right row at most that long), or
+    // -1 for packed batches (any row length).
     int lg1, lg2;
 };
 
@@ -73,9 +75,9 @@ int row_table_limit(int S, int G);
 int row_prefetch_cover(int G);
 cudaError_t launch_direct_rows(const DirectRowArgs& a, const RowParams& p, int mode,
                                const RowGeom& geo, cudaStream_t st);
-// Direct rows with the products formed in registers (rowlanes.cuh): right
-// operands whose rows hold at most 32 entries (p.lg1 / p.lg2 set),
-// shared-memory tables.  lanes_row_bytes: table bytes per warp.
+// Direct rows with the products formed in registers (rowlanes.cuh):
+// shared-memory tables, batch layouts p.lg1 / p.lg2.  lanes_row_bytes:
+// table bytes per warp.
 cudaError_t launch_direct_lanes(const DirectRowArgs& a, const RowParams& p, int mode,
                                 const RowGeom& geo, cudaStream_t st);
 size_t lanes_row_bytes(int mode, int S1, int S2);

@@ -42,6 +42,7 @@ constexpr int kDSpan = 8192;   // columns of the dense accumulator slice
 constexpr int kDList = 4096;   // R*A row entries a CTA holds
 constexpr int kDHist = 1024;   // bins of the column histogram that balances the warps
 constexpr int kDSamples = 2048;   // columns sampled per stage for that histogram
+constexpr int kDSearch = 4;    // arity of the segment searches
 
 // Dynamic shared memory: acc double[kDSpan] | ftq int[kDSpan] (after stage 1:
 // u64 sort keys [kDList]) | lkey int[kDList] | lq int[kDList] |
@@ -54,14 +55,55 @@ __host__ __device__ constexpr size_t dense_smem_bytes() {
            static_cast<size_t>(kDWarps) * kStage * 20 + static_cast<size_t>(kDHist) * 4 + 16;
 }
 
-// First index in [b, e) whose column is >= x (columns ascending).
-__device__ __forceinline__ int lbound(const int* __restrict__ ci, int b, int e, int x) {
-    while (b < e) {
-        const int m = b + ((e - b) >> 1);
-        if (__ldg(ci + m) < x) b = m + 1;
-        else e = m;
+// Pivot step of a K-ary lower bound: the answer (first index whose column
+// is >= x) lies in [lo, lo + n]; the K-1 pivots lo + floor(n k / K) were
+// loaded into v, and the step keeps the part between the last pivot below x
+// and the first at or above it.
+template <int K>
+__device__ __forceinline__ void kary_step(const int (&m)[K - 1], const int (&v)[K - 1], int x,
+                                          int& lo, int& n) {
+    int left = lo, right = m[0];
+#pragma unroll
+    for (int k = 1; k < K; ++k) {
+        if (v[k - 1] < x) {
+            left = m[k - 1] + 1;
+            right = k < K - 1 ? m[k < K - 1 ? k : 0] : lo + n;
+        }
     }
-    return b;
+    lo = left;
+    n = right - left;
+}
+
+// The segment [sb, se) of the right row [ab, ae) (columns ascending, first
+// and last given) whose columns fall in [wlo, whi); the row reaches the
+// range (first < whi, last >= wlo).  Both ends are searched together, K-ary:
+// each step loads the K-1 pivots of both searches at once, so the chain of
+// dependent loads is log_K of the row's length instead of twice log_2.
+template <int K>
+__device__ __forceinline__ void segment_bounds(const int* __restrict__ ci, int ab, int ae,
+                                               int first, int last, int wlo, int whi, int& sb,
+                                               int& se) {
+    // The answers lie in [ab + 1, ae - 1] when searched (first < wlo <= last,
+    // or first < whi <= last).
+    int lo0 = first < wlo ? ab + 1 : ab, n0 = first < wlo ? ae - ab - 2 : 0;
+    int lo1 = last >= whi ? ab + 1 : ae, n1 = last >= whi ? ae - ab - 2 : 0;
+    while (n0 > 0 || n1 > 0) {
+        int m0[K - 1], m1[K - 1], v0[K - 1], v1[K - 1];
+#pragma unroll
+        for (int k = 1; k < K; ++k) {
+            m0[k - 1] = lo0 + static_cast<int>((static_cast<long long>(n0) * k) / K);
+            m1[k - 1] = lo1 + static_cast<int>((static_cast<long long>(n1) * k) / K);
+        }
+#pragma unroll
+        for (int k = 0; k < K - 1; ++k) {
+            v0[k] = __ldg(ci + (n0 > 0 ? m0[k] : ab));
+            v1[k] = __ldg(ci + (n1 > 0 ? m1[k] : ab));
+        }
+        if (n0 > 0) kary_step<K>(m0, v0, wlo, lo0, n0);
+        if (n1 > 0) kary_step<K>(m1, v1, whi, lo1, n1);
+    }
+    sb = lo0;
+    se = lo1;
 }
 
 // The stage-1 list in first-touch order: entry t is list index sorted[t]
@@ -170,8 +212,7 @@ __device__ __forceinline__ void daccumulate(const Left& L, int n, const int* __r
                 } else if (first >= whi) {
                     sb = se = ab;
                 } else {
-                    sb = first >= wlo ? ab : lbound(b_ci, ab + 1, ae, wlo);
-                    se = last < whi ? ae : lbound(b_ci, sb, ae - 1, whi);
+                    segment_bounds<kDSearch>(b_ci, ab, ae, first, last, wlo, whi, sb, se);
                 }
             }
         }
@@ -185,45 +226,33 @@ __device__ __forceinline__ void daccumulate(const Left& L, int n, const int* __r
         int total;
         const int off = wscan_excl(len, total);
         if (total == 0) continue;
-        const bool spread = __reduce_max_sync(kFull, static_cast<unsigned>(len)) > 16u;
+        // Staged in product order, lane i of a window holding product
+        // w0 + i: consecutive lanes read consecutive entries of a segment
+        // (the loads coalesce), each lane finding its step by a search over
+        // the steps' offsets.
+        const int sbase = sb - off;   // product p of this step is entry sbase + p
         for (int w0 = 0; w0 < total; w0 += kStage) {
             const int wl = min(kStage, total - w0);
-            if (spread) {
 #pragma unroll
-                for (int r = 0; r < kStage / 32; ++r) {
-                    const int i = lane + 32 * r;
-                    const int pidx = w0 + i;
-                    int j = 0;
+            for (int r = 0; r < kStage / 32; ++r) {
+                const int i = lane + 32 * r;
+                const int pidx = w0 + i;
+                int j = 0;
 #pragma unroll
-                    for (int step = 16; step > 0; step >>= 1) {
-                        const int oc = __shfl_sync(kFull, off, j + step);
-                        if (oc <= pidx) j += step;
-                    }
-                    const int sbj = __shfl_sync(kFull, sb, j);
-                    const int ofj = __shfl_sync(kFull, off, j);
-                    double sj = 0.0;
-                    if (NUM) sj = __shfl_sync(kFull, s, j);
-                    int qj = 0;
-                    if (FT) qj = __shfl_sync(kFull, fo - ab, j);
-                    if (i < wl) {
-                        const int e = sbj + pidx - ofj;
-                        sk[i] = __ldg(b_ci + e);
-                        if (NUM) sv[i] = __dmul_rn(ldv(b_v, e), sj);
-                        if (FT) sq[i] = qj + e;
-                        sst[i] = j;
-                    }
+                for (int step = 16; step > 0; step >>= 1) {
+                    const int oc = __shfl_sync(kFull, off, j + step);
+                    if (oc <= pidx) j += step;
                 }
-            } else {
-                const int e_end = min(len, w0 + kStage - off);
-                int e = max(0, w0 - off);
-#pragma unroll 4
-                for (; e < e_end; ++e) {
-                    const int pos = off + e - w0;
-                    const int ea = sb + e;
-                    sk[pos] = __ldg(b_ci + ea);
-                    if (NUM) sv[pos] = __dmul_rn(ldv(b_v, ea), s);
-                    if (FT) sq[pos] = fo + (ea - ab);
-                    sst[pos] = lane;
+                const int e = __shfl_sync(kFull, sbase, j) + pidx;
+                double sj = 0.0;
+                if (NUM) sj = __shfl_sync(kFull, s, j);
+                int qj = 0;
+                if (FT) qj = __shfl_sync(kFull, fo - ab, j);
+                if (i < wl) {
+                    sk[i] = __ldg(b_ci + e);
+                    if (NUM) sv[i] = __dmul_rn(ldv(b_v, e), sj);
+                    if (FT) sq[i] = qj + e;
+                    sst[i] = j;
                 }
             }
             __syncwarp();

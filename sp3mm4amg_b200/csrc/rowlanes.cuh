@@ -1,17 +1,15 @@
 // rowlanes.cuh -- direct R*A*P rows with the products formed in registers
 // (sm_100a).
 //
-// For right operands with short rows (A and P rows of at most 32 entries:
-// the fine levels of an AMG hierarchy, whose stencil rows hold 5-30
-// entries), one warp owns one output row and covers several left-row steps
-// per batch.  With W = 2^lg lanes per step (W >= the right operand's longest
-// row), lane l of a batch holds the product of step b0 + (l >> lg) and that
-// step's right-row entry (l & (W-1)).  Batch order then lane order is
-// exactly the reference's product order -- left position t ascending, then
-// the right row's entries ascending (code/src/include/SpMMUtilsGeneric.h:
-// 39-55) -- so no staging buffer is needed: the lanes load their entries
-// straight from the right operand (a step's entries are contiguous, so the
-// loads of a step coalesce).
+// One warp owns one output row and forms its products 32 per batch, one per
+// lane, loaded straight from the right operand (no staging buffer).  Batch
+// order then lane order is exactly the reference's product order -- left
+// position t ascending, then the right row's entries ascending
+// (code/src/include/SpMMUtilsGeneric.h:39-55).  Two layouts deal the
+// products out: 2^lg lanes per left step when the right rows nearly fill
+// them (the stencil rows of fine AMG levels), else packed, 32 consecutive
+// products per batch found by a search over the steps' offsets (longer and
+// uneven right rows: coarser levels, kNN graphs).
 //
 // Accumulation of one batch: one __match_any_sync groups equal columns; the
 // lowest lane of each group (its leader) finds or inserts the column in the
@@ -96,48 +94,82 @@ __device__ __forceinline__ void lanes_batch(const WTab& T, int key, double v, bo
 }
 
 // Accumulate sum_{t<n} L.val(t) * B(L.key(t), :) into T in the reference
-// order; every right row has at most 2^lg entries (checked: a longer row
-// flags kErrInput, since its entries past 2^lg would be missed).  n is
-// warp-uniform.  Returns false when the table passed its load limit; nk =
-// distinct columns inserted (listed in T.ord either way).
-template <bool NUM, typename TB, class Left>
+// order.  Steps are taken 32 at a time (lane j holds step t0 + j), and
+// their products, in the reference's order (step, then right-row entry),
+// are dealt out 32 per batch in one of two layouts:
+//
+// * !PACK (every right row has at most 2^lg entries; a longer one flags
+//   kErrInput, since its entries past 2^lg would be missed): 2^lg lanes per
+//   step, lane l of a batch holding entry (l mod 2^lg) of the batch's step
+//   l >> lg.  Lanes past a row's end idle, so this layout is for right rows
+//   that nearly fill their 2^lg lanes.
+// * PACK: lane l of batch q holds product 32 q + l, whatever the rows'
+//   lengths; the lane finds its step by a search over the steps' product
+//   offsets (shuffles), so only the last batch of a chunk idles lanes.
+//
+// n is warp-uniform.  Returns false when the table passed its load limit;
+// nk = distinct columns inserted (listed in T.ord either way).
+template <bool NUM, bool PACK, typename TB, class Left>
 __device__ __forceinline__ bool lanes_accumulate(const Left& L, int n, int lg,
                                                  const int* __restrict__ b_rp,
                                                  const int* __restrict__ b_ci,
                                                  const TB* __restrict__ b_v, const WTab& T,
                                                  unsigned* err, int& nk) {
     const int lane = threadIdx.x & 31;
-    const int spb = 32 >> lg;                  // steps per batch
-    const int sub = lane >> lg;                // this lane's step in a batch
-    const int e = lane & ((1 << lg) - 1);      // and its entry in that step
+    const int lgf = PACK ? 0 : lg;
+    const int spb = 32 >> lgf;                  // fixed layout: steps per batch
+    const int sub = lane >> lgf;                // this lane's step in a batch
+    const int e = lane & ((1 << lgf) - 1);      // and its entry in that step
     nk = 0;
     for (int t0 = 0; t0 < n; t0 += 32) {
-        // Chunk of up to 32 steps: lane j holds step t0 + j.
         const int t = t0 + lane;
-        int rb = 0, re = 0;
+        int rb = 0, len = 0;
         double s = 0.0;
         if (t < n) {
             const int k = L.key(t);
             if (NUM) s = L.val(t);
             rb = __ldg(b_rp + k);
-            re = __ldg(b_rp + k + 1);
-            if (re - rb > (1 << lg)) atomicOr(err, kErrInput);
+            len = __ldg(b_rp + k + 1) - rb;
+            if (!PACK && len > (1 << lgf)) atomicOr(err, kErrInput);
         }
-        const int cn = n - t0 < 32 ? n - t0 : 32;
-        const int nbat = (cn + spb - 1) / spb;
+        int off = 0, total = 0, nbat;
+        if constexpr (PACK) {
+            off = wscan_excl(len, total);
+            nbat = (total + 31) >> 5;
+        } else {
+            const int cn = n - t0 < 32 ? n - t0 : 32;
+            nbat = (cn + spb - 1) / spb;
+        }
+        const int base = rb - off;   // packed: product p of this step is entry base + p
         for (int q0 = 0; q0 < nbat; q0 += kLanesPrefetch) {
             int ck[kLanesPrefetch];
             double cv[kLanesPrefetch];
             bool ok[kLanesPrefetch];
 #pragma unroll
             for (int q = 0; q < kLanesPrefetch; ++q) {
-                // src < 32 always: batches start at multiples of spb.
-                const int src = ((q0 + q) * spb + sub) & 31;
-                const int jb = __shfl_sync(kFull, rb, src);
-                const int je = __shfl_sync(kFull, re, src);
-                const double js = NUM ? __shfl_sync(kFull, s, src) : 0.0;
-                const int ei = jb + e;
-                ok[q] = q0 + q < nbat && ei < je;
+                int ei;
+                double js;
+                if constexpr (PACK) {
+                    const int pidx = ((q0 + q) << 5) + lane;
+                    // The last step whose first product is at or before
+                    // pidx (an empty step shares its offset with the next).
+                    int j = 0;
+#pragma unroll
+                    for (int step = 16; step > 0; step >>= 1) {
+                        const int o = __shfl_sync(kFull, off, j + step);
+                        if (o <= pidx) j += step;
+                    }
+                    ei = __shfl_sync(kFull, base, j) + pidx;
+                    js = NUM ? __shfl_sync(kFull, s, j) : 0.0;
+                    ok[q] = pidx < total;
+                } else {
+                    // src < 32 always: batches start at multiples of spb.
+                    const int src = ((q0 + q) * spb + sub) & 31;
+                    const int jl = __shfl_sync(kFull, len, src);
+                    ei = __shfl_sync(kFull, rb, src) + e;
+                    js = NUM ? __shfl_sync(kFull, s, src) : 0.0;
+                    ok[q] = q0 + q < nbat && e < jl;
+                }
                 ck[q] = 0;
                 cv[q] = 0.0;
                 if (ok[q]) {
@@ -164,7 +196,7 @@ __host__ __device__ __forceinline__ size_t wlanes_bytes(bool num, int S1, int S2
     return static_cast<size_t>(S1 + S2) * (num ? 16 : 8);
 }
 
-template <int MODE, typename TV, typename TO>
+template <int MODE, typename TV, typename TO, bool PACK>
 __global__ void __launch_bounds__(256, 4) k_direct_lanes(DirectRowArgs a, RowParams p) {
     constexpr bool NUM = MODE != kSymb;
     extern __shared__ __align__(16) unsigned char smem[];
@@ -201,10 +233,11 @@ __global__ void __launch_bounds__(256, 4) k_direct_lanes(DirectRowArgs a, RowPar
         const int rlen = __ldg(a.R.rp + row + 1) - rb;
         int n1 = 0, n2 = 0;
         const LeftG<TV> L1{a.R.ci, rv, rb};
-        bool ok = lanes_accumulate<NUM>(L1, rlen, p.lg1, a.A.rp, a.A.ci, av, T1, p.err, n1);
+        bool ok = lanes_accumulate<NUM, PACK>(L1, rlen, p.lg1, a.A.rp, a.A.ci, av, T1, p.err,
+                                              n1);
         if (ok) {
             const LeftT L2{keys1, vals1, ord1};
-            ok = lanes_accumulate<NUM>(L2, n1, p.lg2, a.P.rp, a.P.ci, pv, T2, p.err, n2);
+            ok = lanes_accumulate<NUM, PACK>(L2, n1, p.lg2, a.P.rp, a.P.ci, pv, T2, p.err, n2);
         }
         wclear(T1, n1, NUM);
         __syncwarp();
