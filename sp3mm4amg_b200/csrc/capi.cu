@@ -70,6 +70,17 @@ size_t pool_idle_bytes(sp3mm_ctx* ctx) {
     return reserved > used ? static_cast<size_t>(reserved - used) : 0;
 }
 
+void pool_reserve(sp3mm_ctx* ctx, size_t bytes) {
+    if (bytes == 0 || pool_idle_bytes(ctx) >= bytes) return;
+    void* p = nullptr;
+    if (cudaMallocAsync(&p, bytes, ctx->stream) != cudaSuccess) {
+        cudaGetLastError();   // not fatal: the pool grows on demand instead
+        return;
+    }
+    cudaFreeAsync(p, ctx->stream);
+    if (cudaStreamSynchronize(ctx->stream) != cudaSuccess) cudaGetLastError();
+}
+
 size_t free_device_bytes(sp3mm_ctx* ctx) {
     // The reading is refreshed every 100 ms; in between, the pool's own
     // growth is subtracted from it (other processes' use is seen at the

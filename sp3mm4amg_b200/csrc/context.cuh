@@ -172,6 +172,12 @@ struct Bins {
 size_t free_device_bytes(sp3mm_ctx* ctx);
 // Bytes the device's memory pool holds reserved but unused (a cheap query).
 size_t pool_idle_bytes(sp3mm_ctx* ctx);
+// Map `bytes` into the device's memory pool now (one allocation, freed at
+// once; the pool keeps freed memory), unless it holds that much idle
+// already: later allocations then do not wait for the pool to grow, which
+// takes 0.1-0.3 s per growth step and holds up the process's other threads'
+// CUDA calls meanwhile.  Failure is not an error (the pool grows on demand).
+void pool_reserve(sp3mm_ctx* ctx, size_t bytes);
 int read_err(sp3mm_ctx* ctx, unsigned* out);
 // Read and clear the sticky device error word; map it to a return code.
 int check_device_err(sp3mm_ctx* ctx);

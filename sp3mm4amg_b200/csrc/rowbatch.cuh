@@ -14,24 +14,23 @@
 // what a row touches (every row clears what it inserted, through the
 // insertion-order list), so any prefix of the region is an empty table.
 //
-// Arithmetic and ordering are those of the single-product warp kernels
-// (waccumulate / wbatch): products generated in the reference's order,
-// rounded products added in that order, first-touch forwarding of the
-// R*A row into P (code/src/Sp3MM_CSR_OMP_UB_Generic.c:498-573), rows written
-// sorted.  Results are therefore bit-identical to the single-product path.
+// Rows are accumulated as in the single-product register-product kernel
+// (rowlanes.cuh, packed batches: right rows of any length): products formed
+// in the reference's order, rounded products added in that order,
+// first-touch forwarding of the R*A row into P
+// (code/src/Sp3MM_CSR_OMP_UB_Generic.c:498-573), rows written sorted.
+// Results are therefore bit-identical to the single-product path.
 #pragma once
 
 #include "batch.cuh"
-#include "rowwarp.cuh"
+#include "rowlanes.cuh"
 
 namespace sp3mm {
 
-// Bytes of one warp's region: numeric sv[kStage] vals1[scap] vals2[scap]
-// sk[kStage] keys1[scap] keys2[scap] ord1[scap] ord2[scap]; symbolic sk
-// keys1 keys2 ord1 ord2.
+// Bytes of one warp's region: numeric vals1[scap] vals2[scap] keys1[scap]
+// keys2[scap] ord1[scap] ord2[scap]; symbolic keys1 keys2 ord1 ord2.
 __host__ __device__ __forceinline__ size_t batch_region_bytes(bool num, int scap) {
-    return num ? static_cast<size_t>(kStage) * 12 + static_cast<size_t>(scap) * 32
-               : static_cast<size_t>(kStage) * 4 + static_cast<size_t>(scap) * 16;
+    return static_cast<size_t>(scap) * (num ? 32 : 16);
 }
 
 // Smallest table (power of two >= 32 slots) whose load limit for a warp
@@ -81,6 +80,14 @@ __device__ __forceinline__ long long batch_book(const BatchRowParams& p, int g, 
     return static_cast<long long>(off);
 }
 
+// One row's accumulation into T: packed register-product batches.
+template <bool NUM, typename TB, class Left>
+__device__ __forceinline__ bool batch_acc(const Left& L, int n, const int* b_rp,
+                                          const int* b_ci, const TB* b_v, const WTab& T,
+                                          unsigned* err, int& nk) {
+    return lanes_accumulate<NUM, true>(L, n, -1, b_rp, b_ci, b_v, T, err, nk);
+}
+
 // Accumulate with an optimistic table of S slots, then (on overflow) once
 // more with the proven size Sp when it fits the region.  Returns the size
 // used, or 0 when the row does not fit (the table is left clear).
@@ -88,14 +95,14 @@ template <bool NUM, typename TB, class Left>
 __device__ __forceinline__ int batch_accumulate(const Left& L, int n, const int* b_rp,
                                                 const int* b_ci, const TB* b_v, int* keys,
                                                 double* vals, int* ord, int S, int Sp, int scap,
-                                                int* sk, double* sv, int& nk) {
+                                                unsigned* err, int& nk) {
     WTab T = make_wtab(keys, vals, ord, S);
-    if (waccumulate<NUM, kProbeBySize>(L, n, b_rp, b_ci, b_v, T, sk, sv, nk)) return S;
+    if (batch_acc<NUM>(L, n, b_rp, b_ci, b_v, T, err, nk)) return S;
     wclear(T, nk, NUM);
     __syncwarp();
     if (Sp <= S || Sp > scap) return 0;
     T = make_wtab(keys, vals, ord, Sp);
-    if (waccumulate<NUM, kProbeBySize>(L, n, b_rp, b_ci, b_v, T, sk, sv, nk)) return Sp;
+    if (batch_acc<NUM>(L, n, b_rp, b_ci, b_v, T, err, nk)) return Sp;
     wclear(T, nk, NUM);
     __syncwarp();
     return 0;
@@ -115,11 +122,9 @@ __global__ void __launch_bounds__(256, 4)
     unsigned char* region =
         GT ? p.gtab + (static_cast<long long>(blockIdx.x) * nw + wib) * p.gstride
            : smem + static_cast<size_t>(wib) * bytes;
-    double* sv = reinterpret_cast<double*>(region);
-    double* vals1 = sv + kStage;
+    double* vals1 = reinterpret_cast<double*>(region);
     double* vals2 = vals1 + scap;
-    int* sk = NUM ? reinterpret_cast<int*>(vals2 + scap) : reinterpret_cast<int*>(region);
-    int* keys1 = sk + kStage;
+    int* keys1 = NUM ? reinterpret_cast<int*>(vals2 + scap) : reinterpret_cast<int*>(region);
     int* keys2 = keys1 + scap;
     int* ord1 = keys2 + scap;
     int* ord2 = ord1 + scap;
@@ -154,7 +159,7 @@ __global__ void __launch_bounds__(256, 4)
                 const int opt1 = p.need_opt ? __ldg(p.need_opt + g) : need1 >> p.d1;
                 S1 = batch_accumulate<NUM>(L1, xlen, Y.rp, Y.ci, static_cast<const TV*>(Y.v),
                                            keys1, vals1, ord1, batch_slots(opt1),
-                                           batch_slots(need1), scap, sk, sv, n1);
+                                           batch_slots(need1), scap, p.err, n1);
                 if (S1 == 0) {
                     batch_retry(p, g, need1);
                     continue;
@@ -165,7 +170,7 @@ __global__ void __launch_bounds__(256, 4)
                 S2 = batch_accumulate<NUM>(L2, n1, Z.rp, Z.ci, static_cast<const TV*>(Z.v),
                                            keys2, vals2, ord2,
                                            min(batch_slots(need2 >> p.d2), scap),
-                                           batch_slots(need2), scap, sk, sv, n2);
+                                           batch_slots(need2), scap, p.err, n2);
                 wclear(T1, n1, NUM);
                 __syncwarp();
                 if (S2 == 0) {
@@ -193,14 +198,12 @@ __global__ void __launch_bounds__(256, 4)
                 const WTab T1 = make_wtab(keys1, vals1, ord1, S1);
                 const WTab T2 = make_wtab(keys2, vals2, ord2, S2);
                 bool ok = S1 <= scap && S2 <= scap &&
-                          waccumulate<NUM, kProbeBySize>(L1, xlen, Y.rp, Y.ci,
-                                                         static_cast<const TV*>(Y.v), T1, sk, sv,
-                                                         n1);
+                          batch_acc<NUM>(L1, xlen, Y.rp, Y.ci, static_cast<const TV*>(Y.v), T1,
+                                         p.err, n1);
                 if (ok) {
                     const LeftT L2{keys1, vals1, ord1};
-                    ok = waccumulate<NUM, kProbeBySize>(L2, n1, Z.rp, Z.ci,
-                                                        static_cast<const TV*>(Z.v), T2, sk, sv,
-                                                        n2);
+                    ok = batch_acc<NUM>(L2, n1, Z.rp, Z.ci, static_cast<const TV*>(Z.v), T2,
+                                        p.err, n2);
                 }
                 if (S1 <= scap) wclear(T1, n1, NUM);
                 __syncwarp();
@@ -220,7 +223,7 @@ __global__ void __launch_bounds__(256, 4)
                 const int opt1 = p.need_opt ? __ldg(p.need_opt + g) : need1 >> p.d1;
                 S1 = batch_accumulate<NUM>(L1, xlen, Y.rp, Y.ci, static_cast<const TV*>(Y.v),
                                            keys1, vals1, ord1, batch_slots(opt1),
-                                           batch_slots(need1), scap, sk, sv, n1);
+                                           batch_slots(need1), scap, p.err, n1);
                 if (S1 == 0) {
                     batch_retry(p, g, need1);
                     continue;
@@ -239,9 +242,9 @@ __global__ void __launch_bounds__(256, 4)
                 S1 = batch_slots(e);
                 if (S1 <= scap) S1 = min(S1 << p.slack, scap);
                 const WTab T = make_wtab(keys1, vals1, ord1, S1);
-                const bool ok = S1 <= scap &&
-                                waccumulate<NUM, kProbeBySize>(L1, xlen, Y.rp, Y.ci,
-                                                 static_cast<const TV*>(Y.v), T, sk, sv, n1);
+                const bool ok = S1 <= scap && batch_acc<NUM>(L1, xlen, Y.rp, Y.ci,
+                                                             static_cast<const TV*>(Y.v), T,
+                                                             p.err, n1);
                 if (!ok || n1 != e) {
                     if (S1 <= scap) wclear(T, n1, NUM);
                     if (lane == 0) atomicOr(p.err, kErrCount);

@@ -236,6 +236,10 @@ int sp3mm_server_create(sp3mm_ctx* ctx, int max_active, double mem_fraction,
     s->max_active = max_active;
     s->mem_fraction = mem_fraction;
     s->budget = static_cast<size_t>(mem_fraction * static_cast<double>(free_hbm(ctx)));
+    // The budget is mapped into the memory pool up front, so that admitting
+    // requests never waits for the pool to grow (which stalls the loader
+    // threads' copies too).
+    pool_reserve(ctx, s->budget);
     s->t0 = std::chrono::steady_clock::now();
     for (int k = 0; k < sp3mm_server::kLoaders; ++k) {
         const int rc = sp3mm_ctx_create(ctx->device, &s->loader_ctx[k]);
