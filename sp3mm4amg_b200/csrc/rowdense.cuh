@@ -43,6 +43,8 @@ constexpr int kDList = 4096;   // R*A row entries a CTA holds
 constexpr int kDHist = 1024;   // bins of the column histogram that balances the warps
 constexpr int kDSamples = 2048;   // columns sampled per stage for that histogram
 constexpr int kDSearch = 4;    // arity of the segment searches
+constexpr int kDSteps = kDWarps * 32;   // stage-1 left entries described at a time
+constexpr int kDAhead = 4;     // stage-1 steps whose products a thread loads ahead
 
 // Dynamic shared memory: acc double[kDSpan] | ftq int[kDSpan] (after stage 1:
 // u64 sort keys [kDList]) | lkey int[kDList] | lq int[kDList] |
@@ -298,6 +300,7 @@ struct DenseSmem {
     int* sq;
     double* sv;
     int* sst;
+    int* step;   // stage-1 step descriptions (over the warps' staging)
     int* hist;
     long long* s_tot;
     int* s_n1;
@@ -322,6 +325,7 @@ __device__ __forceinline__ DenseSmem dense_smem(unsigned char* smem, int* s_n1, 
     d.sq = d.sk + kStage;
     d.sv = reinterpret_cast<double*>(d.sq + kStage);
     d.sst = reinterpret_cast<int*>(d.sv + kStage);
+    d.step = reinterpret_cast<int*>(d.touched + kDSpan);
     d.hist = reinterpret_cast<int*>(d.touched + kDSpan + static_cast<size_t>(kDWarps) * kStage * 20);
     d.s_tot = reinterpret_cast<long long*>(d.hist + kDHist);
     d.s_n1 = s_n1;
@@ -402,6 +406,129 @@ __device__ __forceinline__ void balanced_range(const DenseSmem& d, const Left& L
     __syncthreads();
 }
 
+// Stage 1 (the R*A row) over the columns [cb, ce) of the slice starting at
+// cb, one left entry (step) at a time: the whole CTA takes step t's right
+// row (thread i its entries i, i + blockDim, ...), adds the rounded products
+// to the dense slice and records each new column's first touch (the flat
+// position of its product: the full lengths of the right rows before t plus
+// its offset), then synchronises before step t + 1.  A right row's columns
+// are distinct, so a step has no conflicts, and the barrier between steps
+// keeps every column's contributions in the reference's order (left
+// position ascending; code/src/include/SpMMUtilsGeneric.h:39-55).  Steps are
+// described kDSteps at a time in shared memory (bounds, left value, flat
+// position), and every thread loads its products kDAhead steps ahead, so a
+// step costs a few shared-memory operations and one barrier.  Only the
+// first `nw` warps step (enough for the longest right row, at most all):
+// they synchronise among themselves with a named barrier, so warps that
+// would idle add nothing to a step's cost.
+template <bool NUM, typename TV>
+__device__ __forceinline__ void dstage1(const DenseSmem& d, const CsrView& R, const CsrView& A,
+                                        int rb, int rlen, int cb, int ce, int nw) {
+    const int tid = threadIdx.x;
+    const int nt = nw * 32;
+    const int lane = tid & 31;
+    const int wid = tid >> 5;
+    const TV* rv = static_cast<const TV*>(R.v);
+    const TV* av = static_cast<const TV*>(A.v);
+    int* st_ab = d.step;
+    int* st_ae = st_ab + kDSteps;
+    int* st_fo = st_ae + kDSteps;
+    double* st_s = reinterpret_cast<double*>(st_fo + kDSteps);
+    int carry = 0;   // full right-row lengths before this block of steps
+    for (int b0 = 0; b0 < rlen; b0 += kDSteps) {
+        const int nb = min(kDSteps, rlen - b0);
+        int ab = 0, ae = 0;
+        double sv = 0.0;
+        if (tid < nb) {
+            const int k = __ldg(R.ci + rb + b0 + tid);
+            if (NUM) sv = ldv(rv, rb + b0 + tid);
+            ab = __ldg(A.rp + k);
+            ae = __ldg(A.rp + k + 1);
+        }
+        int wt;
+        const int x = wscan_excl(ae - ab, wt);
+        if (lane == 0) d.hist[wid] = wt;
+        __syncthreads();
+        int before = carry, all = 0;
+        for (int w = 0; w < kDWarps; ++w) {
+            const int v = d.hist[w];
+            if (w < wid) before += v;
+            all += v;
+        }
+        carry += all;
+        if (tid < nb) {
+            st_ab[tid] = ab;
+            st_ae[tid] = ae;
+            st_fo[tid] = before + x;
+            st_s[tid] = sv;
+        }
+        __syncthreads();
+        if (wid >= nw) {
+            __syncthreads();
+            continue;
+        }
+        int pc[kDAhead];
+        double pvv[kDAhead];
+#pragma unroll
+        for (int q = 0; q < kDAhead; ++q) {
+            pc[q] = -1;
+            pvv[q] = 0.0;
+            if (q < nb) {
+                const int e = st_ab[q] + tid;
+                if (e < st_ae[q]) {
+                    pc[q] = __ldg(A.ci + e);
+                    if (NUM) pvv[q] = ldv(av, e);
+                }
+            }
+        }
+        for (int t0 = 0; t0 < nb; t0 += kDAhead) {
+#pragma unroll
+            for (int q = 0; q < kDAhead; ++q) {
+                const int t = t0 + q;
+                if (t < nb) {
+                    const int col = pc[q];
+                    const double v = pvv[q];
+                    const int tn = t + kDAhead;
+                    pc[q] = -1;
+                    if (tn < nb) {
+                        const int e = st_ab[tn] + tid;
+                        if (e < st_ae[tn]) {
+                            pc[q] = __ldg(A.ci + e);
+                            if (NUM) pvv[q] = ldv(av, e);
+                        }
+                    }
+                    const int fo = st_fo[t];
+                    const double s = NUM ? st_s[t] : 0.0;
+                    if (col >= cb && col < ce) {
+                        const int slot = col - cb;
+                        if (!d.touched[slot]) {
+                            d.touched[slot] = 1;
+                            d.ftq[slot] = fo + tid;
+                        }
+                        if (NUM) d.acc[slot] = __dadd_rn(d.acc[slot], __dmul_rn(v, s));
+                    }
+                    // Right rows longer than the CTA: their further entries.
+                    const int ab_t = st_ab[t], ae_t = st_ae[t];
+                    for (int e = ab_t + tid + nt; e < ae_t; e += nt) {
+                        const int c2 = __ldg(A.ci + e);
+                        if (c2 >= cb && c2 < ce) {
+                            const int slot = c2 - cb;
+                            if (!d.touched[slot]) {
+                                d.touched[slot] = 1;
+                                d.ftq[slot] = fo + (e - ab_t);
+                            }
+                            if (NUM) d.acc[slot] = __dadd_rn(d.acc[slot], __dmul_rn(ldv(av, e), s));
+                        }
+                    }
+                    // Named barrier 1 over the stepping warps.
+                    asm volatile("bar.sync 1, %0;" ::"r"(nt) : "memory");
+                }
+            }
+        }
+        __syncthreads();
+    }
+}
+
 // One output row of C = R*A*P (row `row` of R) by the whole CTA.  `finish`
 // runs on thread 0 once the counts are known: finish(n1, n2, fail) returns
 // the output offset of the row, or -1 when nothing is to be written (the
@@ -416,8 +543,6 @@ __device__ __forceinline__ void dense_row(const DenseSmem& d, const CsrView& R, 
     const int lane = threadIdx.x & 31;
     const int wid = threadIdx.x >> 5;
     const unsigned lt = lanemask_lt();
-    const TV* rv = static_cast<const TV*>(R.v);
-    const TV* av = static_cast<const TV*>(A.v);
     const TV* pv = static_cast<const TV*>(P.v);
     const int rb = __ldg(R.rp + row);
     const int rlen = __ldg(R.rp + row + 1) - rb;
@@ -426,39 +551,35 @@ __device__ __forceinline__ void dense_row(const DenseSmem& d, const CsrView& R, 
         *d.s_lo = INT_MAX;
         *d.s_hi = -1;
         *d.s_tot = 0;
+        *d.s_cnt = 0;
     }
     __syncthreads();
-    // Stage-1 span: the A rows' first and last columns.
-    int lo = INT_MAX, hi = -1;
-    long long tot = 0;
+    // Stage-1 span (the A rows' first and last columns) and longest A row.
+    int lo = INT_MAX, hi = -1, amax = 0;
     for (int t = threadIdx.x; t < rlen; t += blockDim.x) {
         const int k = __ldg(R.ci + rb + t);
         const int ab = __ldg(A.rp + k), ae = __ldg(A.rp + k + 1);
-        tot += ae - ab;
+        amax = max(amax, ae - ab);
         if (ab < ae) {
             lo = min(lo, __ldg(A.ci + ab));
             hi = max(hi, __ldg(A.ci + ae - 1));
         }
     }
     block_span(lo, hi, d.s_lo, d.s_hi);
-    block_total(tot, d.s_tot);
+    amax = static_cast<int>(__reduce_max_sync(kFull, static_cast<unsigned>(amax)));
+    if (lane == 0) atomicMax(d.s_cnt, amax);
     __syncthreads();
     const int lo1 = *d.s_lo, hi1 = *d.s_hi;
-    const long long tot1 = *d.s_tot;
-    const LeftG<TV> L1{R.ci, rv, rb};
+    const int nw1 = min(kDWarps, max(1, (*d.s_cnt + 31) >> 5));
     for (long long c0 = lo1; c0 <= hi1; c0 += kDSpan) {
         const int cb = static_cast<int>(c0);
         const int ce = static_cast<int>(min(static_cast<long long>(hi1) + 1, c0 + kDSpan));
-        int wlo, whi;
-        balanced_range(d, L1, rlen, A.rp, A.ci, cb, ce, tot1, wlo, whi);
-        daccumulate<NUM, true>(L1, rlen, A.rp, A.ci, av, wlo, whi, cb, d.acc, d.touched, d.ftq,
-                               d.sk, d.sq, d.sv, d.sst);
-        __syncthreads();
-        // List this warp's touched columns (value and first touch) and
+        dstage1<NUM, TV>(d, R, A, rb, rlen, cb, ce, nw1);
+        // List the slice's touched columns (value and first touch) and
         // clear them.
-        for (int s0 = wlo; s0 < whi; s0 += 32) {
+        for (int s0 = cb + 32 * wid; s0 < ce; s0 += 32 * kDWarps) {
             const int col = s0 + lane;
-            const bool hit = col < whi && d.touched[col - cb];
+            const bool hit = col < ce && d.touched[col - cb];
             const unsigned b = __ballot_sync(kFull, hit);
             int pos0 = 0;
             if (lane == 0 && b) pos0 = atomicAdd(d.s_n1, __popc(b));
@@ -514,7 +635,7 @@ __device__ __forceinline__ void dense_row(const DenseSmem& d, const CsrView& R, 
     // Stage-2 span: the P rows' first and last columns.
     lo = INT_MAX;
     hi = -1;
-    tot = 0;
+    long long tot = 0;
     if (!fail) {
         for (int t = threadIdx.x; t < n1; t += blockDim.x) {
             const int c = d.lkey[t];
