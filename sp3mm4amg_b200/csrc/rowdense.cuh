@@ -5,28 +5,33 @@
 // reaches hundreds of A rows of hundreds of entries, the R*A row has
 // thousands of columns, and one warp per row with a hash table large enough
 // for it leaves a handful of warps per SM.  Here a CTA of kDWarps warps owns
-// one row, and the warps split the row's COLUMNS, not its products: warp w
-// owns a contiguous column range, finds in every right row the segment that
-// falls in its range (binary search; right rows are ordered), and processes
-// exactly its products in the reference's order (left position ascending,
-// then the right row's entries).  Every column therefore still receives its
-// contributions in the reference's order (code/src/include/
-// SpMMUtilsGeneric.h:39-55), and the accumulator of a column range is a
-// dense slice of shared memory indexed by column -- no hashing.  Within a
-// batch of 32 staged products, the products of one right row's segment have
-// distinct columns and are added at once, segment after segment (batches
-// spread over many short segments group equal columns with a match).
+// one row, accumulating into a dense slice of shared memory indexed by
+// column (no hashing).  Every column must receive its contributions in the
+// reference's order (left position ascending, then the right row's entries;
+// code/src/include/SpMMUtilsGeneric.h:39-55); the two stages keep it in two
+// ways.
 //
-// Stage 1 (the R*A row) walks the row's column span in chunks of kDSpan
-// columns.  Each column's first touch is recorded as the flat position of
-// the product that made it (left position, then right-row entry), and after
-// each chunk the touched columns are listed with their position and value.
-// Sorting that list by position gives the order in which the reference's
-// index map appends the columns (code/src/include/sparseMatrix.h:85-104), the
-// order in which the direct product forwards the R*A row into P
-// (code/src/Sp3MM_CSR_OMP_UB_Generic.c:542-545).  Stage 2 forwards the list
-// into P over the span of the P columns it reaches (one chunk), and the C row
-// is written in column order straight from the dense slice (no sort).
+// Stage 1 (the R*A row) steps through the left entries: the CTA takes one
+// right row per step (a right row's columns are distinct, so a step has no
+// conflicts) and synchronises between steps (dstage1).  It walks the row's
+// column span in chunks of kDSpan columns.  Each column's first touch is
+// recorded as the flat position of the product that made it (left
+// position, then right-row entry), and after each chunk the touched columns
+// are listed with their position and value.  Sorting that list by position
+// gives the order in which the reference's index map appends the columns
+// (code/src/include/sparseMatrix.h:85-104), the order in which the direct
+// product forwards the R*A row into P (code/src/Sp3MM_CSR_OMP_UB_Generic.c:
+// 542-545).
+//
+// Stage 2 forwards the list into P over the span of the P columns it
+// reaches (one chunk), with the warps splitting the COLUMNS, not the
+// products: warp w owns a contiguous column range, finds in every right row
+// the segment that falls in its range (right rows are ordered), and
+// processes exactly its products in order.  Within a batch of 32 staged
+// products, the products of one right row's segment have distinct columns
+// and are added at once, segment after segment (batches spread over many
+// short segments group equal columns with a match).  The C row is written
+// in column order straight from the dense slice (no sort).
 //
 // A row whose R*A row has more than kDList columns, or whose C row spans more
 // than kDSpan columns, is appended to the retry list (processed by the
