@@ -421,12 +421,14 @@ __device__ __forceinline__ void balanced_range(const DenseSmem& d, const Left& L
 // keeps every column's contributions in the reference's order (left
 // position ascending; code/src/include/SpMMUtilsGeneric.h:39-55).  Steps are
 // described kDSteps at a time in shared memory (bounds, left value, flat
-// position), and every thread loads its products kDAhead steps ahead, so a
-// step costs a few shared-memory operations and one barrier.  Only the
-// first `nw` warps step (enough for the longest right row, at most all):
+// position), and every thread loads its products (PER entries of each
+// right row: 2 when the longest right row is longer than the CTA) kDAhead
+// steps ahead, so a step costs a few shared-memory operations and one
+// barrier.  Only the first `nw` warps step (enough for the longest right
+// row, at most all):
 // they synchronise among themselves with a named barrier, so warps that
 // would idle add nothing to a step's cost.
-template <bool NUM, typename TV>
+template <bool NUM, int PER, typename TV>
 __device__ __forceinline__ void dstage1(const DenseSmem& d, const CsrView& R, const CsrView& A,
                                         int rb, int rlen, int cb, int ce, int nw) {
     const int tid = threadIdx.x;
@@ -472,17 +474,22 @@ __device__ __forceinline__ void dstage1(const DenseSmem& d, const CsrView& R, co
             __syncthreads();
             continue;
         }
-        int pc[kDAhead];
-        double pvv[kDAhead];
+        // pc / pvv[q][j]: the product of entry tid + j * nt of the right row
+        // of step t0 + q (pc = -1: none).
+        int pc[kDAhead][PER];
+        double pvv[kDAhead][PER];
 #pragma unroll
         for (int q = 0; q < kDAhead; ++q) {
-            pc[q] = -1;
-            pvv[q] = 0.0;
-            if (q < nb) {
-                const int e = st_ab[q] + tid;
-                if (e < st_ae[q]) {
-                    pc[q] = __ldg(A.ci + e);
-                    if (NUM) pvv[q] = ldv(av, e);
+#pragma unroll
+            for (int j = 0; j < PER; ++j) {
+                pc[q][j] = -1;
+                pvv[q][j] = 0.0;
+                if (q < nb) {
+                    const int e = st_ab[q] + tid + j * nt;
+                    if (e < st_ae[q]) {
+                        pc[q][j] = __ldg(A.ci + e);
+                        if (NUM) pvv[q][j] = ldv(av, e);
+                    }
                 }
             }
         }
@@ -491,30 +498,38 @@ __device__ __forceinline__ void dstage1(const DenseSmem& d, const CsrView& R, co
             for (int q = 0; q < kDAhead; ++q) {
                 const int t = t0 + q;
                 if (t < nb) {
-                    const int col = pc[q];
-                    const double v = pvv[q];
+                    int col[PER];
+                    double v[PER];
                     const int tn = t + kDAhead;
-                    pc[q] = -1;
-                    if (tn < nb) {
-                        const int e = st_ab[tn] + tid;
-                        if (e < st_ae[tn]) {
-                            pc[q] = __ldg(A.ci + e);
-                            if (NUM) pvv[q] = ldv(av, e);
+#pragma unroll
+                    for (int j = 0; j < PER; ++j) {
+                        col[j] = pc[q][j];
+                        v[j] = pvv[q][j];
+                        pc[q][j] = -1;
+                        if (tn < nb) {
+                            const int e = st_ab[tn] + tid + j * nt;
+                            if (e < st_ae[tn]) {
+                                pc[q][j] = __ldg(A.ci + e);
+                                if (NUM) pvv[q][j] = ldv(av, e);
+                            }
                         }
                     }
                     const int fo = st_fo[t];
                     const double s = NUM ? st_s[t] : 0.0;
-                    if (col >= cb && col < ce) {
-                        const int slot = col - cb;
-                        if (!d.touched[slot]) {
-                            d.touched[slot] = 1;
-                            d.ftq[slot] = fo + tid;
+#pragma unroll
+                    for (int j = 0; j < PER; ++j) {
+                        if (col[j] >= cb && col[j] < ce) {
+                            const int slot = col[j] - cb;
+                            if (!d.touched[slot]) {
+                                d.touched[slot] = 1;
+                                d.ftq[slot] = fo + tid + j * nt;
+                            }
+                            if (NUM) d.acc[slot] = __dadd_rn(d.acc[slot], __dmul_rn(v[j], s));
                         }
-                        if (NUM) d.acc[slot] = __dadd_rn(d.acc[slot], __dmul_rn(v, s));
                     }
-                    // Right rows longer than the CTA: their further entries.
+                    // Right rows longer than PER entries per thread.
                     const int ab_t = st_ab[t], ae_t = st_ae[t];
-                    for (int e = ab_t + tid + nt; e < ae_t; e += nt) {
+                    for (int e = ab_t + tid + PER * nt; e < ae_t; e += nt) {
                         const int c2 = __ldg(A.ci + e);
                         if (c2 >= cb && c2 < ce) {
                             const int slot = c2 - cb;
@@ -575,11 +590,15 @@ __device__ __forceinline__ void dense_row(const DenseSmem& d, const CsrView& R, 
     if (lane == 0) atomicMax(d.s_cnt, amax);
     __syncthreads();
     const int lo1 = *d.s_lo, hi1 = *d.s_hi;
-    const int nw1 = min(kDWarps, max(1, (*d.s_cnt + 31) >> 5));
+    const int amax1 = *d.s_cnt;
+    const int nw1 = min(kDWarps, max(1, (amax1 + 31) >> 5));
     for (long long c0 = lo1; c0 <= hi1; c0 += kDSpan) {
         const int cb = static_cast<int>(c0);
         const int ce = static_cast<int>(min(static_cast<long long>(hi1) + 1, c0 + kDSpan));
-        dstage1<NUM, TV>(d, R, A, rb, rlen, cb, ce, nw1);
+        if (amax1 > 32 * kDWarps)
+            dstage1<NUM, 2, TV>(d, R, A, rb, rlen, cb, ce, nw1);
+        else
+            dstage1<NUM, 1, TV>(d, R, A, rb, rlen, cb, ce, nw1);
         // List the slice's touched columns (value and first touch) and
         // clear them.
         for (int s0 = cb + 32 * wid; s0 < ce; s0 += 32 * kDWarps) {
