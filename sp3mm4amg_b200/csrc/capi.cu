@@ -254,8 +254,15 @@ struct RowRunner {
         if (direct && use_lanes(p, G)) {
             // Tables twice the bin's size (the second half the first):
             // fewer probe steps and retried rows; measured 8 % faster at 128^3.
+            // Where that does not fit, the second table (the C row, which in
+            // a Galerkin product holds fewer columns than the R*A row) is
+            // still half the first unless the caller tuned it: more warps
+            // fit an SM (128^3 level 1: 4.24 -> 3.32 ms); a row whose C row
+            // overflows it is retried with proven tables.
             if (lanes_row_bytes(mode, 2 * p.S1, p.S1) <= kLanesMaxWarpBytes) {
                 p.S1 *= 2;
+                p.S2 = p.S1 / 2;
+            } else if (ctx->tune_d2 < 0 && p.S2 == p.S1 && p.S1 >= 64) {
                 p.S2 = p.S1 / 2;
             }
             const size_t per_warp = lanes_row_bytes(mode, p.S1, p.S2);
