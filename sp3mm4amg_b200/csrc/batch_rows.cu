@@ -4,6 +4,8 @@
 #include "rowdense.cuh"
 
 namespace sp3mm {
+
+using namespace dbig;   // the default CTA-per-row configuration (rowdense.cuh)
 namespace {
 
 using KFn = void (*)(const BItem*, const int*, BatchRowParams);

@@ -242,10 +242,39 @@ struct RowRunner {
         if (direct && use_dense(ctx, p)) {
             static const char* const kDense[3] = {"direct.dense.symb", "direct.dense.num",
                                                   "direct.dense.book"};
+            static const char* const kDense2[3] = {"direct.dense2.symb", "direct.dense2.num",
+                                                   "direct.dense2.book"};
+            // Products whose A has many columns run two CTAs per SM first
+            // (half the slice and list); the rows that outgrow it run again
+            // on the default configuration (its row count stays on the
+            // device), and what that cannot hold joins the retry list.
+            const int per_sm = da.A.N >= kDenseSmallMinCols ? dense_small_ctas_per_sm() : 0;
             cudaError_t e = cudaSuccess;
-            prof(ctx, kDense[mode], [&] {
-                e = launch_direct_dense(da, p, mode, ctx->num_sms, ctx->stream);
-            });
+            if (per_sm >= 2) {
+                DevBuf again;
+                TRY(again.alloc(ctx, sizeof(int) * (static_cast<size_t>(p.nrows) + 1)));
+                int* n_again = again.as<int>() + p.nrows;
+                CK(ctx, cudaMemsetAsync(n_again, 0, sizeof(int), ctx->stream));
+                RowParams ps = p;
+                ps.retry_rows = again.as<int>();
+                ps.retry_count = n_again;
+                prof(ctx, kDense2[mode], [&] {
+                    e = launch_direct_dense_small(da, ps, mode, per_sm * ctx->num_sms,
+                                                  ctx->stream);
+                });
+                if (e == cudaSuccess) {
+                    RowParams pb = p;
+                    pb.rows = again.as<int>();
+                    pb.nrows_dev = n_again;
+                    prof(ctx, kDense[mode], [&] {
+                        e = launch_direct_dense(da, pb, mode, ctx->num_sms, ctx->stream);
+                    });
+                }
+            } else {
+                prof(ctx, kDense[mode], [&] {
+                    e = launch_direct_dense(da, p, mode, ctx->num_sms, ctx->stream);
+                });
+            }
             if (e != cudaSuccess)
                 return set_error(ctx, SP3MM_ECUDA, "dense row kernel launch failed: %s",
                                  cudaGetErrorString(e));

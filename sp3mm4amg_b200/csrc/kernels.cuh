@@ -34,6 +34,7 @@ struct PairRowArgs {
 struct RowParams {
     const int* rows;          // the rows of this launch
     int nrows;
+    const int* nrows_dev;     // CTA-per-row kernel: row count on the device (set: nrows bounds it)
     int S1, S2;               // table slots (powers of two >= 32); S2: direct only
     unsigned char* gtab;      // tables in global memory (nullptr: shared memory)
     long long gstride;        // bytes per group in gtab
@@ -90,6 +91,17 @@ constexpr int kDenseLanes = 512;
 cudaError_t launch_direct_dense(const DirectRowArgs& a, const RowParams& p, int mode, int grid,
                                 cudaStream_t st);
 size_t dense_row_smem();
+// The same kernel in half the shared memory, two CTAs per SM
+// (rows_dense_small.cu), for products whose A has at least
+// kDenseSmallMinCols columns (coarse rows then reach a small fraction of
+// them: 1,227 of 32,768 at 128^3 level 2); rows whose R*A row outgrows its
+// 2,048-column list are run again by the default configuration.
+// dense_small_ctas_per_sm(): its resident CTAs per SM (0 when it cannot
+// run).
+constexpr int kDenseSmallMinCols = 16384;
+cudaError_t launch_direct_dense_small(const DirectRowArgs& a, const RowParams& p, int mode,
+                                      int grid, cudaStream_t st);
+int dense_small_ctas_per_sm();
 cudaError_t launch_pair_rows(const PairRowArgs& a, const RowParams& p, int mode,
                              const RowGeom& geo, cudaStream_t st);
 

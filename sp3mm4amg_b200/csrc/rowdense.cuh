@@ -36,30 +36,48 @@
 // A row whose R*A row has more than kDList columns, or whose C row spans more
 // than kDSpan columns, is appended to the retry list (processed by the
 // retry launch with tables sized from a proven bound).
+//
+// The file is compiled in two configurations, each in a namespace of its
+// own (SP3MM_DENSE_NS): `dbig` (the default: an 8,192-column slice, lists of
+// 4,096 columns, one CTA per SM) and `dsmall` (rows_dense_small.cu: half the
+// slice and list in half the shared memory, two CTAs per SM, for rows whose
+// tables are at most kDenseSmallSlots).
 #pragma once
 
 #include "rowwarp.cuh"
 
+#ifndef SP3MM_DENSE_NS
+#define SP3MM_DENSE_NS dbig
+#define SP3MM_DENSE_SPAN 8192
+#define SP3MM_DENSE_LIST 4096
+#define SP3MM_DENSE_STAGE 128
+#define SP3MM_DENSE_MINB 1
+#endif
+
 namespace sp3mm {
+namespace SP3MM_DENSE_NS {
 
 constexpr int kDWarps = 16;    // warps per CTA (one output row per CTA)
-constexpr int kDSpan = 8192;   // columns of the dense accumulator slice
-constexpr int kDList = 4096;   // R*A row entries a CTA holds
+constexpr int kDSpan = SP3MM_DENSE_SPAN;   // columns of the dense accumulator slice
+constexpr int kDList = SP3MM_DENSE_LIST;   // R*A row entries a CTA holds
+constexpr int kDStage = SP3MM_DENSE_STAGE;   // stage-2 staged products per warp window
 constexpr int kDHist = 1024;   // bins of the column histogram that balances the warps
 constexpr int kDSamples = 2048;   // columns sampled per stage for that histogram
 constexpr int kDSearch = 4;    // arity of the segment searches
 constexpr int kDSteps = kDWarps * 32;   // stage-1 left entries described at a time
 constexpr int kDAhead = 4;     // stage-1 steps whose products a thread loads ahead
+// The stage-1 step descriptions live over the warps' stage-2 staging.
+static_assert(kDSteps * 20 <= kDWarps * kDStage * 20, "step descriptions exceed the staging");
 
 // Dynamic shared memory: acc double[kDSpan] | ftq int[kDSpan] (after stage 1:
 // u64 sort keys [kDList]) | lkey int[kDList] | lq int[kDList] |
-// lval double[kDList] | touched u8[kDSpan] | per warp: sk int[kStage],
-// sq int[kStage], sv double[kStage], sst int[kStage] | hist int[kDHist] |
+// lval double[kDList] | touched u8[kDSpan] | per warp: sk int[kDStage],
+// sq int[kDStage], sv double[kDStage], sst int[kDStage] | hist int[kDHist] |
 // total int.
 __host__ __device__ constexpr size_t dense_smem_bytes() {
     return static_cast<size_t>(kDSpan) * 8 + static_cast<size_t>(kDSpan) * 4 +
            static_cast<size_t>(kDList) * 16 + static_cast<size_t>(kDSpan) +
-           static_cast<size_t>(kDWarps) * kStage * 20 + static_cast<size_t>(kDHist) * 4 + 16;
+           static_cast<size_t>(kDWarps) * kDStage * 20 + static_cast<size_t>(kDHist) * 4 + 16;
 }
 
 // Pivot step of a K-ary lower bound: the answer (first index whose column
@@ -238,10 +256,10 @@ __device__ __forceinline__ void daccumulate(const Left& L, int n, const int* __r
         // (the loads coalesce), each lane finding its step by a search over
         // the steps' offsets.
         const int sbase = sb - off;   // product p of this step is entry sbase + p
-        for (int w0 = 0; w0 < total; w0 += kStage) {
-            const int wl = min(kStage, total - w0);
+        for (int w0 = 0; w0 < total; w0 += kDStage) {
+            const int wl = min(kDStage, total - w0);
 #pragma unroll
-            for (int r = 0; r < kStage / 32; ++r) {
+            for (int r = 0; r < kDStage / 32; ++r) {
                 const int i = lane + 32 * r;
                 const int pidx = w0 + i;
                 int j = 0;
@@ -325,13 +343,13 @@ __device__ __forceinline__ DenseSmem dense_smem(unsigned char* smem, int* s_n1, 
     d.lq = d.lkey + kDList;
     d.lval = reinterpret_cast<double*>(d.lq + kDList);
     d.touched = reinterpret_cast<unsigned char*>(d.lval + kDList);
-    unsigned char* wst = d.touched + kDSpan + static_cast<size_t>(threadIdx.x >> 5) * kStage * 20;
+    unsigned char* wst = d.touched + kDSpan + static_cast<size_t>(threadIdx.x >> 5) * kDStage * 20;
     d.sk = reinterpret_cast<int*>(wst);
-    d.sq = d.sk + kStage;
-    d.sv = reinterpret_cast<double*>(d.sq + kStage);
-    d.sst = reinterpret_cast<int*>(d.sv + kStage);
+    d.sq = d.sk + kDStage;
+    d.sv = reinterpret_cast<double*>(d.sq + kDStage);
+    d.sst = reinterpret_cast<int*>(d.sv + kDStage);
     d.step = reinterpret_cast<int*>(d.touched + kDSpan);
-    d.hist = reinterpret_cast<int*>(d.touched + kDSpan + static_cast<size_t>(kDWarps) * kStage * 20);
+    d.hist = reinterpret_cast<int*>(d.touched + kDSpan + static_cast<size_t>(kDWarps) * kDStage * 20);
     d.s_tot = reinterpret_cast<long long*>(d.hist + kDHist);
     d.s_n1 = s_n1;
     d.s_lo = s_lo;
@@ -740,7 +758,8 @@ __device__ __forceinline__ void dense_row(const DenseSmem& d, const CsrView& R, 
 }
 
 template <int MODE, typename TV, typename TO>
-__global__ void __launch_bounds__(kDWarps * 32, 1) k_direct_dense(DirectRowArgs a, RowParams p) {
+__global__ void __launch_bounds__(kDWarps * 32, SP3MM_DENSE_MINB)
+    k_direct_dense(DirectRowArgs a, RowParams p) {
     extern __shared__ __align__(16) unsigned char smem[];
     __shared__ int s_n1, s_lo, s_hi, s_cnt[kDWarps];
     __shared__ long long s_base;
@@ -748,7 +767,8 @@ __global__ void __launch_bounds__(kDWarps * 32, 1) k_direct_dense(DirectRowArgs 
     dense_clear(d);
     int* oc = MODE == kNumBook ? p.ub_ci : p.c_ci;
     TO* ov = static_cast<TO*>(MODE == kNumBook ? p.ub_v : p.c_v);
-    for (long long it = blockIdx.x; it < p.nrows; it += gridDim.x) {
+    const long long nrows = p.nrows_dev ? *p.nrows_dev : p.nrows;
+    for (long long it = blockIdx.x; it < nrows; it += gridDim.x) {
         const int row = p.rows[it];
         const long long eb = MODE == kNumExact ? p.c_rp[row] : 0;
         const long long ee = MODE == kNumExact ? p.c_rp[row + 1] : 0;
@@ -781,4 +801,5 @@ __global__ void __launch_bounds__(kDWarps * 32, 1) k_direct_dense(DirectRowArgs 
     }
 }
 
+}  // namespace SP3MM_DENSE_NS
 }  // namespace sp3mm

@@ -4,6 +4,8 @@
 
 namespace sp3mm {
 
+using namespace dbig;   // the default CTA-per-row configuration (rowdense.cuh)
+
 template <int MODE, bool GT>
 static cudaError_t direct_warp_typed(const DirectRowArgs& a, const RowParams& p,
                                      const RowGeom& geo, cudaStream_t st) {
