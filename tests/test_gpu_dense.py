@@ -4,7 +4,8 @@ sorting flat product positions.  Its results must be bit-identical to the
 reference's direct product (the oracle) and to the warp-per-row kernels, in
 every flavour and value type, including rows it cannot hold (an R*A row of
 more than 4096 columns, or a C row spanning more than 8192 columns), which go
-to the retry launch."""
+to the retry launch, and in both of its configurations (rows that outgrow
+the smaller one run again on the default one)."""
 import numpy as np
 import pytest
 
@@ -124,5 +125,39 @@ def test_rows_with_more_products_than_columns_run_one_cta_per_row(orc):
             C.free()
             _same(got, want, ("dense rows", fl))
             assert any(k.startswith("direct.dense") for k in prof), prof
+        for m in d:
+            m.free()
+
+
+def test_wide_operands_run_the_small_configuration_then_the_default(orc):
+    # A with 20,000 columns: heavy rows run first on the configuration with
+    # half the slice and list (two CTAs per SM); rows whose R*A row holds
+    # more than its 2,048 columns (rows 0-3: about 2,950) run again on the
+    # default configuration, the others (rows 4-7: about 790) stay.
+    rng = np.random.default_rng(31)
+    import scipy.sparse as sp
+    rows = [np.sort(rng.choice(3000, 80 if i < 4 else 20, replace=False)) for i in range(8)]
+    Rm = sp.csr_matrix((rng.uniform(0.5, 1.5, sum(len(r) for r in rows)),
+                        np.concatenate(rows), np.cumsum([0] + [len(r) for r in rows])),
+                       shape=(8, 3000))
+    R = pb.CSR(Rm.indptr, Rm.indices, Rm.data, Rm.shape)
+    A = pb.random_sparse(3000, 20000, 0.002, seed=32)
+    P = pb.random_sparse(20000, 64, 0.05, seed=33)
+    with S.Context() as ctx:
+        _direct_all_ways(ctx, orc, R, A, P, "small then default")
+        want = orc.sp3mm_direct(R, A, P)
+        d = [ctx.upload(m) for m in (R, A, P)]
+        ctx.set_tuning(DENSE, -1, -1)
+        for fl in (S.UB, S.SYMBNUM):
+            ctx.set_profiling(True)
+            C = ctx.rap(*d, S.DIRECT, fl)
+            got = C.download()
+            prof = ctx.profile()
+            ctx.set_profiling(False)
+            C.free()
+            _same(got, want, ("small then default", fl))
+            assert any(k.startswith("direct.dense2") for k in prof), prof
+            assert any(k.startswith("direct.dense.") for k in prof), prof
+        ctx.set_tuning(0, -1, -1)
         for m in d:
             m.free()
