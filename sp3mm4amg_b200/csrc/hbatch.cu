@@ -168,6 +168,109 @@ __global__ void k_hs_fill(long long n, int* iota, void* ones, int vt) {
     }
 }
 
+// A*P0 for an aggregation P0 (one 1.0 per row: fine point j -> its
+// block agg(j)) on operators whose rows hold at most kAggRow entries (the
+// fine levels' stencils), one thread per row: (A P0)_ic is the sum, over
+// the row's entries j in order, of A_ij * 1.0 with agg(j) = c -- the same
+// rounded products (x * 1.0 = x), added in the same order onto the same
+// 0.0 start as the SpMM row kernels, so the result is bit-identical to the
+// SpMM batch that the coarser levels still take.
+constexpr int kAggRow = 32;
+
+// The row's distinct blocks in first-touch order (lab) and, SUMS, their
+// sums; the row has at most kAggRow entries.
+template <bool SUMS>
+__device__ __forceinline__ int agg_row(const HStep& h, int i, const int* __restrict__ agg,
+                                       int* lab, double* sum) {
+    int n = 0;
+    const int e1 = h.A.rp[i + 1];
+    for (int e = h.A.rp[i]; e < e1; ++e) {
+        const int c = agg[h.row_base + h.A.ci[e]];
+        int q = 0;
+        while (q < n && lab[q] != c) ++q;
+        if (q == n) {
+            lab[n] = c;
+            if (SUMS) sum[n] = 0.0;
+            ++n;
+        }
+        if (SUMS) sum[q] = __dadd_rn(sum[q], __dmul_rn(1.0, vload(h.A.v, h.A.vtype, e)));
+    }
+    return n;
+}
+
+// cnt[g] = distinct blocks of row g; maxrow[t] = the longest of
+// hierarchy t (a longer A row than kAggRow flags kErrInput).
+__global__ void k_hs_ap0_count(const HStep* __restrict__ hs, const long long* __restrict__ bases,
+                               int n, long long rows, const int* __restrict__ agg, int* cnt,
+                               int* maxrow, unsigned* err) {
+    for (long long g = blockIdx.x * (long long)blockDim.x + threadIdx.x; g < rows;
+         g += (long long)gridDim.x * blockDim.x) {
+        const int t = find_base(bases, n, g);
+        const HStep& h = hs[t];
+        const int i = static_cast<int>(g - h.row_base);
+        int c = 0;
+        if (h.A.rp[i + 1] - h.A.rp[i] > kAggRow) {
+            atomicOr(err, kErrInput);
+        } else {
+            int lab[kAggRow];
+            c = agg_row<false>(h, i, agg, lab, nullptr);
+        }
+        cnt[g] = c;
+        const unsigned peers = __match_any_sync(__activemask(), t);
+        const int m = static_cast<int>(__reduce_max_sync(peers, static_cast<unsigned>(c)));
+        if ((peers & ((1u << (threadIdx.x & 31)) - 1u)) == 0) atomicMax(maxrow + t, m);
+    }
+}
+
+// Row g of A*P0 at grp[g]: blocks ascending with their sums.
+__global__ void k_hs_ap0_fill(const HStep* __restrict__ hs, const long long* __restrict__ bases,
+                              int n, long long rows, const int* __restrict__ agg,
+                              const int* __restrict__ grp, int* ci, double* v) {
+    for (long long g = blockIdx.x * (long long)blockDim.x + threadIdx.x; g < rows;
+         g += (long long)gridDim.x * blockDim.x) {
+        const HStep& h = hs[find_base(bases, n, g)];
+        const int i = static_cast<int>(g - h.row_base);
+        if (h.A.rp[i + 1] - h.A.rp[i] > kAggRow) continue;
+        int lab[kAggRow];
+        double sum[kAggRow];
+        const int c = agg_row<true>(h, i, agg, lab, sum);
+        for (int a = 1; a < c; ++a) {
+            const int l = lab[a];
+            const double x = sum[a];
+            int b = a - 1;
+            while (b >= 0 && lab[b] > l) {
+                lab[b + 1] = lab[b];
+                sum[b + 1] = sum[b];
+                --b;
+            }
+            lab[b + 1] = l;
+            sum[b + 1] = x;
+        }
+        const int o = grp[g];
+        for (int q = 0; q < c; ++q) {
+            ci[o + q] = lab[q];
+            v[o + q] = sum[q];
+        }
+    }
+}
+
+// Local row pointers of every hierarchy's A*P0 (hierarchy t's at
+// lrp[bases[t] + t]), and off[t] = its first entry in the step's arrays
+// (off[n] = the total).
+__global__ void k_hs_ap0_rp(const long long* __restrict__ bases, int n, long long rows,
+                            const int* __restrict__ grp, int* lrp, int* off) {
+    for (long long g = blockIdx.x * (long long)blockDim.x + threadIdx.x; g < rows;
+         g += (long long)gridDim.x * blockDim.x) {
+        const int t = find_base(bases, n, g);
+        const long long base = bases[t];
+        const int b0 = grp[base];
+        lrp[g + t] = grp[g] - b0;
+        if (g + 1 == bases[t + 1]) lrp[g + t + 1] = grp[g + 1] - b0;
+        if (g == base) off[t] = b0;
+        if (g + 1 == rows) off[n] = grp[rows];
+    }
+}
+
 int grid_of(long long work) {
     const long long g = (work + 255) / 256;
     return static_cast<int>(std::max<long long>(1, std::min<long long>(g, 148LL * 32)));
@@ -258,39 +361,91 @@ int step_group(sp3mm_ctx* ctx, const std::vector<sp3mm_hierarchy*>& hs) {
     note_launch();
     CK(ctx, cudaGetLastError());
 
-    // A*P0 for every hierarchy: one SpMM batch.
+    // A*P0 for every hierarchy: directly when every operator's rows are
+    // short (the fine levels), else one SpMM batch.
     phase.end();
     ProfSpan phase_ap0(ctx, "hstep.ap0");
-    std::vector<int> kinds(k, SP3MM_BATCH_SPMM);
     std::vector<sp3mm_dcsr> X(k), Y(k), Z(k);
-    for (int t = 0; t < k; ++t) {
-        X[t] = hs[t]->A.back();
-        sp3mm_dcsr& p0 = Y[t];
-        p0.M = static_cast<int>(bases[t + 1] - bases[t]);
-        p0.N = H[t].nc;
-        p0.nnz = p0.M;
-        p0.row_ptr = iota.as<int>();
-        p0.col = agg.as<int>() + bases[t];
-        p0.val = ones.p;
-        p0.val_type = tv;
-        p0.max_row = 1;
-    }
+    std::vector<sp3mm_dcsr> AP0(k), P(k), R(k);
+    auto arena = std::make_shared<Arena>(ctx);
+    std::shared_ptr<sp3mm_batch> b1;
     sp3mm_batch* raw = nullptr;
-    TRY(sp3mm_batch_create(ctx, k, kinds.data(), X.data(), Y.data(), nullptr, SP3MM_F64, &raw));
-    auto b1 = hold(raw);
-    TRY(sp3mm_batch_run(b1.get()));
-    batch_trim(b1.get());
+    bool short_rows = true;
+    for (int t = 0; t < k; ++t) {
+        const int mr = hs[t]->A.back().max_row;
+        short_rows = short_rows && mr >= 0 && mr <= kAggRow;
+    }
+    if (short_rows) {
+        DevBuf acnt, agrp, amax, aoff, arp, aci, av;
+        TRY(acnt.alloc(ctx, sizeof(int) * rows));
+        TRY(agrp.alloc(ctx, sizeof(int) * (rows + 1)));
+        TRY(amax.alloc(ctx, sizeof(int) * k));
+        TRY(aoff.alloc(ctx, sizeof(int) * (k + 1)));
+        TRY(arp.alloc(ctx, sizeof(int) * (rows + k)));
+        CK(ctx, cudaMemsetAsync(amax.p, 0, sizeof(int) * k, st));
+        k_hs_ap0_count<<<grid_of(rows), 256, 0, st>>>(dH.as<HStep>(), dB.as<long long>(), k,
+                                                      rows, agg.as<int>(), acnt.as<int>(),
+                                                      amax.as<int>(), ctx->d_err);
+        note_launch();
+        const size_t atb = scan_temp_bytes(static_cast<int>(rows));
+        TRY(tmp.alloc(ctx, atb));
+        launch_scan(static_cast<int>(rows), acnt.as<int>(), agrp.as<int>(), tmp.p, atb, st);
+        k_hs_ap0_rp<<<grid_of(rows), 256, 0, st>>>(dB.as<long long>(), k, rows, agrp.as<int>(),
+                                                   arp.as<int>(), aoff.as<int>());
+        note_launch();
+        CK(ctx, cudaGetLastError());
+        std::vector<int> hoff(k + 1), hmax(k);
+        CK(ctx, cudaMemcpyAsync(hoff.data(), aoff.p, sizeof(int) * (k + 1),
+                                cudaMemcpyDeviceToHost, st));
+        CK(ctx, cudaMemcpyAsync(hmax.data(), amax.p, sizeof(int) * k, cudaMemcpyDeviceToHost,
+                                st));
+        TRY(check_device_err(ctx));   // synchronises: hoff and hmax are complete
+        const long long total = hoff[k];
+        TRY(aci.alloc(ctx, sizeof(int) * std::max<long long>(total, 1)));
+        TRY(av.alloc(ctx, sizeof(double) * std::max<long long>(total, 1)));
+        k_hs_ap0_fill<<<grid_of(rows), 256, 0, st>>>(dH.as<HStep>(), dB.as<long long>(), k,
+                                                     rows, agg.as<int>(), agrp.as<int>(),
+                                                     aci.as<int>(), av.as<double>());
+        note_launch();
+        CK(ctx, cudaGetLastError());
+        int* a_rp = static_cast<int*>(arena->take(arp));
+        int* a_ci = static_cast<int*>(arena->take(aci));
+        double* a_v = static_cast<double*>(arena->take(av));
+        for (int t = 0; t < k; ++t) {
+            AP0[t] = sp3mm_dcsr{static_cast<int>(bases[t + 1] - bases[t]), H[t].nc,
+                                static_cast<long long>(hoff[t + 1] - hoff[t]),
+                                a_rp + bases[t] + t, a_ci + hoff[t], a_v + hoff[t], SP3MM_F64,
+                                hmax[t]};
+        }
+    } else {
+        std::vector<int> kinds(k, SP3MM_BATCH_SPMM);
+        for (int t = 0; t < k; ++t) {
+            X[t] = hs[t]->A.back();
+            sp3mm_dcsr& p0 = Y[t];
+            p0.M = static_cast<int>(bases[t + 1] - bases[t]);
+            p0.N = H[t].nc;
+            p0.nnz = p0.M;
+            p0.row_ptr = iota.as<int>();
+            p0.col = agg.as<int>() + bases[t];
+            p0.val = ones.p;
+            p0.val_type = tv;
+            p0.max_row = 1;
+        }
+        TRY(sp3mm_batch_create(ctx, k, kinds.data(), X.data(), Y.data(), nullptr, SP3MM_F64,
+                               &raw));
+        b1 = hold(raw);
+        TRY(sp3mm_batch_run(b1.get()));
+        batch_trim(b1.get());
+        for (int t = 0; t < k; ++t) TRY(sp3mm_batch_result(b1.get(), t, &AP0[t]));
+    }
 
     // P values (in place when FP64) and the restriction arrays.
     phase_ap0.end();
     ProfSpan phase_jac(ctx, "hstep.jacobi");
-    auto arena = std::make_shared<Arena>(ctx);
-    std::vector<sp3mm_dcsr> AP0(k), P(k), R(k);
     long long nnz_p = 0;
     std::vector<long long> r_base(k), rrp(k);
     long long rrp_total = 0;
     for (int t = 0; t < k; ++t) {
-        TRY(sp3mm_batch_result(b1.get(), t, &AP0[t]));
         r_base[t] = nnz_p;
         nnz_p += AP0[t].nnz;
         rrp[t] = rrp_total;
