@@ -6,7 +6,9 @@
 // a dozen launches and several host round trips per hierarchy, a step runs
 //
 //   labels + diagonals        one launch over the rows of all hierarchies
-//   A*P0                      one batch (sp3mm_batch, SpMM products)
+//   A*P0                      one thread per row when every operator's rows
+//                             hold at most kAggRow entries (count, scan,
+//                             fill), else one batch (sp3mm_batch, SpMM)
 //   Jacobi combine            one launch
 //   transpose                 column counts, scan, scatter, row sort and
 //                             local row pointers over the block-diagonal
