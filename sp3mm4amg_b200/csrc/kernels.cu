@@ -313,8 +313,64 @@ __global__ void __launch_bounds__(256) k_transpose_scatter(CsrView A, const int*
     }
 }
 
+// Rows of more than 32 and at most kSortSmemRow entries: a warp per row
+// sorts the row in shared memory with a bitonic network (the coarse levels'
+// restrictions hold rows of hundreds of entries; odd-even transposition in
+// global memory took 2.8 ms for the 512 rows of 677 entries of 128^3 level
+// 3).  Columns within a row are distinct, so the order is unique.
+constexpr int kSortSmemRow = 2048;
+constexpr int kSortSmemWarps = 4;
+
+__global__ void __launch_bounds__(kSortSmemWarps * 32) k_sort_rows_smem(int M, const int* rp,
+                                                                        int* ci, void* v, int vt) {
+    extern __shared__ __align__(16) unsigned char sort_smem[];
+    const int lane = threadIdx.x & 31;
+    const int w = threadIdx.x >> 5;
+    double* sv = reinterpret_cast<double*>(sort_smem) + static_cast<size_t>(w) * kSortSmemRow;
+    int* sk = reinterpret_cast<int*>(reinterpret_cast<double*>(sort_smem) +
+                                     static_cast<size_t>(kSortSmemWarps) * kSortSmemRow) +
+              static_cast<size_t>(w) * kSortSmemRow;
+    const int warps = (gridDim.x * blockDim.x) / 32;
+    for (int row = (blockIdx.x * blockDim.x + threadIdx.x) / 32; row < M; row += warps) {
+        const int b = rp[row], e = rp[row + 1];
+        const int n = e - b;
+        if (n <= 32 || n > kSortSmemRow) continue;
+        int P2 = 64;
+        while (P2 < n) P2 <<= 1;
+        for (int i = lane; i < P2; i += 32) {
+            sk[i] = i < n ? ci[b + i] : INT_MAX;
+            sv[i] = i < n ? load_val(v, vt, b + i) : 0.0;
+        }
+        __syncwarp();
+        for (int k = 2; k <= P2; k <<= 1) {
+            for (int j = k >> 1; j > 0; j >>= 1) {
+                for (int i = lane; i < P2; i += 32) {
+                    const int ixj = i ^ j;
+                    if (ixj > i) {
+                        const int a0 = sk[i], a1 = sk[ixj];
+                        if ((a0 > a1) == ((i & k) == 0)) {
+                            sk[i] = a1;
+                            sk[ixj] = a0;
+                            const double x0 = sv[i];
+                            sv[i] = sv[ixj];
+                            sv[ixj] = x0;
+                        }
+                    }
+                }
+                __syncwarp();
+            }
+        }
+        for (int i = lane; i < n; i += 32) {
+            ci[b + i] = sk[i];
+            store_val(v, vt, b + i, sv[i]);
+        }
+        __syncwarp();
+    }
+}
+
 // Sort each row's (col, val) by col.  Warp per row; rows up to 32 entries by
-// rank in registers, longer rows by odd-even transposition in place.
+// rank in registers, rows of k_sort_rows_smem's range there, longer rows by
+// odd-even transposition in place.
 __global__ void __launch_bounds__(256) k_sort_rows(int M, const int* rp, int* ci, void* v,
                                                     int vt) {
     const int lane = threadIdx.x & 31;
@@ -337,6 +393,7 @@ __global__ void __launch_bounds__(256) k_sort_rows(int M, const int* rp, int* ci
             __syncwarp();
             continue;
         }
+        if (n <= kSortSmemRow) continue;   // k_sort_rows_smem
         for (int phase = 0; phase < n; ++phase) {
             for (int i = b + (phase & 1) + 2 * lane; i + 1 < e; i += 64) {
                 const int a0 = ci[i], a1 = ci[i + 1];
@@ -529,6 +586,14 @@ void launch_sort_rows(int M, const int* rp, int* ci, void* v, int vt, int max_ro
     k_sort_rows<<<grid_for(static_cast<long long>(M) * 32, 256), 256, 0, st>>>(M, rp, ci, v,
                                                                               vt);
     note_launch();
+    if (max_row > 32) {
+        const int smem = kSortSmemWarps * kSortSmemRow * 12;
+        cudaFuncSetAttribute(k_sort_rows_smem, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             smem);
+        k_sort_rows_smem<<<grid_for(static_cast<long long>(M) * 32, kSortSmemWarps * 32),
+                           kSortSmemWarps * 32, smem, st>>>(M, rp, ci, v, vt);
+        note_launch();
+    }
 }
 
 void launch_colparts_ub(const CsrView& A, int gridCols, const long long* bColOffsets,
