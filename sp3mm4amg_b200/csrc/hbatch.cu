@@ -672,3 +672,55 @@ int sp3mm_hierarchy_build_batch(sp3mm_ctx* ctx, int n, const sp3mm_dcsr* A0, con
 }
 
 }  // extern "C"
+
+namespace sp3mm {
+
+int agg_product(sp3mm_ctx* ctx, const sp3mm_dcsr& A, const int* agg, int nc, sp3mm_dcsr* AP0) {
+    const cudaStream_t st = ctx->stream;
+    if (A.max_row < 0 || A.max_row > kAggRow || A.M < 1) return SP3MM_EINVAL;
+    const long long rows = A.M;
+    HStep h{};
+    h.A = view(A);
+    h.nc = nc;
+    const long long bases[2] = {0, rows};
+    DevBuf dH, dB, cnt, grp, mx, off, tmp, rp, ci, v;
+    TRY(dH.alloc(ctx, sizeof(HStep)));
+    TRY(dB.alloc(ctx, sizeof(bases)));
+    TRY(cnt.alloc(ctx, sizeof(int) * rows));
+    TRY(grp.alloc(ctx, sizeof(int) * (rows + 1)));
+    TRY(mx.alloc(ctx, sizeof(int)));
+    TRY(off.alloc(ctx, sizeof(int) * 2));
+    TRY(rp.alloc(ctx, sizeof(int) * (rows + 1)));
+    CK(ctx, cudaMemcpyAsync(dH.p, &h, sizeof(HStep), cudaMemcpyHostToDevice, st));
+    CK(ctx, cudaMemcpyAsync(dB.p, bases, sizeof(bases), cudaMemcpyHostToDevice, st));
+    CK(ctx, cudaMemsetAsync(mx.p, 0, sizeof(int), st));
+    k_hs_ap0_count<<<grid_of(rows), 256, 0, st>>>(dH.as<HStep>(), dB.as<long long>(), 1, rows,
+                                                  agg, cnt.as<int>(), mx.as<int>(), ctx->d_err);
+    note_launch();
+    const size_t tb = scan_temp_bytes(static_cast<int>(rows));
+    TRY(tmp.alloc(ctx, tb));
+    launch_scan(static_cast<int>(rows), cnt.as<int>(), grp.as<int>(), tmp.p, tb, st);
+    k_hs_ap0_rp<<<grid_of(rows), 256, 0, st>>>(dB.as<long long>(), 1, rows, grp.as<int>(),
+                                               rp.as<int>(), off.as<int>());
+    note_launch();
+    CK(ctx, cudaGetLastError());
+    int hoff[2] = {0, 0}, hmax = 0;
+    CK(ctx, cudaMemcpyAsync(hoff, off.p, sizeof(hoff), cudaMemcpyDeviceToHost, st));
+    CK(ctx, cudaMemcpyAsync(&hmax, mx.p, sizeof(int), cudaMemcpyDeviceToHost, st));
+    TRY(check_device_err(ctx));   // synchronises: hoff and hmax are complete
+    const long long total = hoff[1];
+    TRY(ci.alloc(ctx, sizeof(int) * std::max<long long>(total, 1)));
+    TRY(v.alloc(ctx, sizeof(double) * std::max<long long>(total, 1)));
+    k_hs_ap0_fill<<<grid_of(rows), 256, 0, st>>>(dH.as<HStep>(), dB.as<long long>(), 1, rows,
+                                                 agg, grp.as<int>(), ci.as<int>(),
+                                                 v.as<double>());
+    note_launch();
+    CK(ctx, cudaGetLastError());
+    *AP0 = sp3mm_dcsr{A.M, nc, total, rp.as<int>(), ci.as<int>(), v.p, SP3MM_F64, hmax};
+    rp.detach();
+    ci.detach();
+    v.detach();
+    return SP3MM_OK;
+}
+
+}  // namespace sp3mm
