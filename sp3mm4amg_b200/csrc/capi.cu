@@ -1620,20 +1620,17 @@ int sp3mm_transpose(sp3mm_ctx* ctx, const sp3mm_dcsr* A, sp3mm_dcsr* AT) {
     TRY(ci.alloc(ctx, sizeof(int) * static_cast<size_t>(A->nnz)));
     TRY(v.alloc(ctx, vbytes(A->val_type) * static_cast<size_t>(A->nnz)));
     launch_transpose_scatter(view(*A), rp.as<int>(), cursor.as<int>(), ci.as<int>(), v.p, st);
-    // Longest transposed row = largest column count.
+    // The scatter order within a row is arbitrary: sort (the sort kernels
+    // skip the rows they do not handle, so they run without knowing the
+    // longest row), then validate, which also finds the longest row.
+    launch_sort_rows(A->N, rp.as<int>(), ci.as<int>(), v.p, A->val_type, INT_MAX, st);
     DevBuf mr;
     TRY(mr.alloc(ctx, sizeof(int)));
     CK(ctx, cudaMemsetAsync(mr.p, 0, sizeof(int), st));
     launch_validate_i32(A->N, A->M, rp.as<int>(), ci.as<int>(), mr.as<int>(), ctx->d_err, st);
     int max_row = 0;
     CK(ctx, cudaMemcpyAsync(&max_row, mr.p, sizeof(int), cudaMemcpyDeviceToHost, st));
-    CK(ctx, cudaStreamSynchronize(st));
-    // The scatter order within a row is arbitrary: sort, then re-validate.
-    CK(ctx, cudaMemsetAsync(ctx->d_err, 0, sizeof(unsigned), st));
-    launch_sort_rows(A->N, rp.as<int>(), ci.as<int>(), v.p, A->val_type, max_row, st);
-    CK(ctx, cudaMemsetAsync(mr.p, 0, sizeof(int), st));
-    launch_validate_i32(A->N, A->M, rp.as<int>(), ci.as<int>(), mr.as<int>(), ctx->d_err, st);
-    TRY(check_device_err(ctx));
+    TRY(check_device_err(ctx));   // synchronises: max_row is complete
     AT->M = A->N;
     AT->N = A->M;
     AT->nnz = A->nnz;

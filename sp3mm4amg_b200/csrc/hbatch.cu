@@ -177,7 +177,7 @@ __global__ void k_hs_fill(long long n, int* iota, void* ones, int vt) {
 // rounded products (x * 1.0 = x), added in the same order onto the same
 // 0.0 start as the SpMM row kernels, so the result is bit-identical to the
 // SpMM batch that the coarser levels still take.
-constexpr int kAggRow = 32;
+constexpr int kAggRow = kAggProductRow;
 
 // The row's distinct blocks in first-touch order (lab) and, SUMS, their
 // sums; the row has at most kAggRow entries.

@@ -201,7 +201,7 @@ int sp3mm_block_prolongator(sp3mm_ctx* ctx, const sp3mm_dcsr* A, const int32_t* 
     P0.val_type = A->val_type;
     P0.max_row = 1;
     sp3mm_dcsr AP0{};
-    if (A->max_row >= 0 && A->max_row <= 32)
+    if (A->max_row >= 0 && A->max_row <= kAggProductRow)
         H_TRY(agg_product(ctx, *A, agg, static_cast<int>(cn), &AP0));
     else
         H_TRY(sp3mm_spmm(ctx, A, &P0, SP3MM_UB, SP3MM_F64, &AP0));

@@ -43,8 +43,9 @@ int hierarchy_step(sp3mm_ctx* ctx, const std::vector<sp3mm_hierarchy*>& hs);
 
 // A*P0 for the aggregation P0 given by agg (fine point -> one of nc blocks,
 // value 1.0) computed directly, one thread per row; A's rows must hold at
-// most 32 entries (A.max_row known).  The result's arrays are the caller's
-// (free with sp3mm_dcsr_free); bit-identical to the SpMM.
+// most kAggProductRow entries (A.max_row known).  The result's arrays are
+// the caller's (free with sp3mm_dcsr_free); bit-identical to the SpMM.
+constexpr int kAggProductRow = 32;
 int agg_product(sp3mm_ctx* ctx, const sp3mm_dcsr& A, const int* agg, int nc, sp3mm_dcsr* AP0);
 
 }  // namespace sp3mm
