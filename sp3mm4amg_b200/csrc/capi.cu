@@ -1624,6 +1624,7 @@ int sp3mm_transpose(sp3mm_ctx* ctx, const sp3mm_dcsr* A, sp3mm_dcsr* AT) {
     // skip the rows they do not handle, so they run without knowing the
     // longest row), then validate, which also finds the longest row.
     launch_sort_rows(A->N, rp.as<int>(), ci.as<int>(), v.p, A->val_type, INT_MAX, st);
+    CK(ctx, cudaGetLastError());
     DevBuf mr;
     TRY(mr.alloc(ctx, sizeof(int)));
     CK(ctx, cudaMemsetAsync(mr.p, 0, sizeof(int), st));

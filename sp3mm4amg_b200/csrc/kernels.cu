@@ -588,6 +588,7 @@ void launch_sort_rows(int M, const int* rp, int* ci, void* v, int vt, int max_ro
     note_launch();
     if (max_row > 32) {
         const int smem = kSortSmemWarps * kSortSmemRow * 12;
+        // A failure here surfaces as the launch's error (callers check it).
         cudaFuncSetAttribute(k_sort_rows_smem, cudaFuncAttributeMaxDynamicSharedMemorySize,
                              smem);
         k_sort_rows_smem<<<grid_for(static_cast<long long>(M) * 32, kSortSmemWarps * 32),
