@@ -67,17 +67,16 @@ constexpr int kDSearch = 4;    // arity of the segment searches
 constexpr int kDSteps = kDWarps * 32;   // stage-1 left entries described at a time
 constexpr int kDAhead = 4;     // stage-1 steps whose products a thread loads ahead
 // The stage-1 step descriptions live over the warps' stage-2 staging.
-static_assert(kDSteps * 20 <= kDWarps * kDStage * 20, "step descriptions exceed the staging");
+static_assert(kDSteps * 20 <= kDWarps * kDStage * 16, "step descriptions exceed the staging");
 
 // Dynamic shared memory: acc double[kDSpan] | ftq int[kDSpan] (after stage 1:
 // u64 sort keys [kDList]) | lkey int[kDList] | lq int[kDList] |
 // lval double[kDList] | touched u8[kDSpan] | per warp: sk int[kDStage],
-// sq int[kDStage], sv double[kDStage], sst int[kDStage] | hist int[kDHist] |
-// total int.
+// sv double[kDStage], sst int[kDStage] | hist int[kDHist] | total int.
 __host__ __device__ constexpr size_t dense_smem_bytes() {
     return static_cast<size_t>(kDSpan) * 8 + static_cast<size_t>(kDSpan) * 4 +
            static_cast<size_t>(kDList) * 16 + static_cast<size_t>(kDSpan) +
-           static_cast<size_t>(kDWarps) * kDStage * 20 + static_cast<size_t>(kDHist) * 4 + 16;
+           static_cast<size_t>(kDWarps) * kDStage * 16 + static_cast<size_t>(kDHist) * 4 + 16;
 }
 
 // Pivot step of a K-ary lower bound: the answer (first index whose column
@@ -149,8 +148,8 @@ struct LeftSorted {
 // are added in rounds by segment; others group equal columns with a match.
 constexpr int kDSegRounds = 3;
 
-// One batch of staged products into the dense slice (slot = column - base).
-// FT: record a new column's first-touch position.  sst[i] is the left
+// One batch of staged products into the dense slice (slot = column - base),
+// marking the columns touched.  sst[i] is the left
 // position (step) a staged product comes from; steps never decrease along
 // the staging, and one step's columns are distinct (a right row's columns
 // are), so the products of one segment of equal steps are added all at
@@ -158,10 +157,10 @@ constexpr int kDSegRounds = 3;
 // reference's order without grouping equal columns.  Batches spread over
 // many short segments group equal columns with __match_any_sync instead
 // (the lowest lane of a group adds the group's products in lane order).
-template <bool NUM, bool FT>
-__device__ __forceinline__ void dbatch(double* acc, unsigned char* touched, int* ftq, int base,
-                                       const int* sk, const double* sv, const int* sq,
-                                       const int* sst, int i, bool valid) {
+template <bool NUM>
+__device__ __forceinline__ void dbatch(double* acc, unsigned char* touched, int base,
+                                       const int* sk, const double* sv, const int* sst, int i,
+                                       bool valid) {
     const int lane = threadIdx.x & 31;
     const unsigned lt = lanemask_lt();
     const int st = valid ? sst[i] : -1;
@@ -174,10 +173,7 @@ __device__ __forceinline__ void dbatch(double* acc, unsigned char* touched, int*
         const double v = (NUM && valid) ? sv[i] : 0.0;
         for (int r = 0; r < nseg; ++r) {
             if (valid && seg == r) {
-                if (!touched[slot]) {
-                    touched[slot] = 1;
-                    if (FT) ftq[slot] = sq[i];
-                }
+                touched[slot] = 1;
                 if (NUM) acc[slot] = __dadd_rn(acc[slot], v);
             }
             __syncwarp();
@@ -188,10 +184,7 @@ __device__ __forceinline__ void dbatch(double* acc, unsigned char* touched, int*
     const unsigned peers = __match_any_sync(kFull, key);
     if (valid && (peers & lt) == 0) {
         const int slot = key - base;
-        if (!touched[slot]) {
-            touched[slot] = 1;
-            if (FT) ftq[slot] = sq[i];
-        }
+        touched[slot] = 1;
         if (NUM) {
             double v = acc[slot];
             const int i0 = i - lane;
@@ -207,18 +200,15 @@ __device__ __forceinline__ void dbatch(double* acc, unsigned char* touched, int*
 }
 
 // sum_{t<n} L.val(t) * B(L.key(t), :) restricted to the columns [wlo, whi)
-// (inside the slice starting at `base`), in the reference's order.  FT: the
-// flat position of a product is the sum of the full lengths of the right
-// rows before its left position plus its offset in its own right row.
-template <bool NUM, bool FT, typename TB, class Left>
+// (inside the slice starting at `base`), in the reference's order (stage 2).
+template <bool NUM, typename TB, class Left>
 __device__ __forceinline__ void daccumulate(const Left& L, int n, const int* __restrict__ b_rp,
                                             const int* __restrict__ b_ci,
                                             const TB* __restrict__ b_v, int wlo, int whi,
                                             int base, double* acc, unsigned char* touched,
-                                            int* ftq, int* sk, int* sq, double* sv, int* sst) {
+                                            int* sk, double* sv, int* sst) {
     if (wlo >= whi) return;
     const int lane = threadIdx.x & 31;
-    int qbase = 0;
     for (int t0 = 0; t0 < n; t0 += 32) {
         const int t = t0 + lane;
         int ab = 0, ae = 0, sb = 0, se = 0;
@@ -240,12 +230,6 @@ __device__ __forceinline__ void daccumulate(const Left& L, int n, const int* __r
                     segment_bounds<kDSearch>(b_ci, ab, ae, first, last, wlo, whi, sb, se);
                 }
             }
-        }
-        int fo = 0;
-        if (FT) {
-            int full;
-            fo = wscan_excl(ae - ab, full) + qbase;
-            qbase += full;
         }
         const int len = se - sb;
         int total;
@@ -271,19 +255,15 @@ __device__ __forceinline__ void daccumulate(const Left& L, int n, const int* __r
                 const int e = __shfl_sync(kFull, sbase, j) + pidx;
                 double sj = 0.0;
                 if (NUM) sj = __shfl_sync(kFull, s, j);
-                int qj = 0;
-                if (FT) qj = __shfl_sync(kFull, fo - ab, j);
                 if (i < wl) {
                     sk[i] = __ldg(b_ci + e);
                     if (NUM) sv[i] = __dmul_rn(ldv(b_v, e), sj);
-                    if (FT) sq[i] = qj + e;
                     sst[i] = j;
                 }
             }
             __syncwarp();
             for (int i0 = 0; i0 < wl; i0 += 32)
-                dbatch<NUM, FT>(acc, touched, ftq, base, sk, sv, sq, sst, i0 + lane,
-                                i0 + lane < wl);
+                dbatch<NUM>(acc, touched, base, sk, sv, sst, i0 + lane, i0 + lane < wl);
             __syncwarp();
         }
     }
@@ -320,7 +300,6 @@ struct DenseSmem {
     double* lval;
     unsigned char* touched;
     int* sk;
-    int* sq;
     double* sv;
     int* sst;
     int* step;   // stage-1 step descriptions (over the warps' staging)
@@ -343,13 +322,12 @@ __device__ __forceinline__ DenseSmem dense_smem(unsigned char* smem, int* s_n1, 
     d.lq = d.lkey + kDList;
     d.lval = reinterpret_cast<double*>(d.lq + kDList);
     d.touched = reinterpret_cast<unsigned char*>(d.lval + kDList);
-    unsigned char* wst = d.touched + kDSpan + static_cast<size_t>(threadIdx.x >> 5) * kDStage * 20;
+    unsigned char* wst = d.touched + kDSpan + static_cast<size_t>(threadIdx.x >> 5) * kDStage * 16;
     d.sk = reinterpret_cast<int*>(wst);
-    d.sq = d.sk + kDStage;
-    d.sv = reinterpret_cast<double*>(d.sq + kDStage);
+    d.sv = reinterpret_cast<double*>(d.sk + kDStage);
     d.sst = reinterpret_cast<int*>(d.sv + kDStage);
     d.step = reinterpret_cast<int*>(d.touched + kDSpan);
-    d.hist = reinterpret_cast<int*>(d.touched + kDSpan + static_cast<size_t>(kDWarps) * kDStage * 20);
+    d.hist = reinterpret_cast<int*>(d.touched + kDSpan + static_cast<size_t>(kDWarps) * kDStage * 16);
     d.s_tot = reinterpret_cast<long long*>(d.hist + kDHist);
     d.s_n1 = s_n1;
     d.s_lo = s_lo;
@@ -708,8 +686,8 @@ __device__ __forceinline__ void dense_row(const DenseSmem& d, const CsrView& R, 
         int wlo2 = 0, whi2 = 0;
         if (run2) {
             balanced_range(d, L2, n1, P.rp, P.ci, cb, ce, tot2, wlo2, whi2);
-            daccumulate<NUM, false>(L2, n1, P.rp, P.ci, pv, wlo2, whi2, cb, d.acc, d.touched,
-                                    nullptr, d.sk, d.sq, d.sv, d.sst);
+            daccumulate<NUM>(L2, n1, P.rp, P.ci, pv, wlo2, whi2, cb, d.acc, d.touched, d.sk,
+                             d.sv, d.sst);
         }
         __syncthreads();
         int cnt = 0;
